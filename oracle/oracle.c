@@ -1,0 +1,499 @@
+/*
+ * oracle.c - CPU restatement of the reference's hot-path arithmetic.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This file is the checker for the CUDA product
+ * path: only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg
+ * load it.  It is never linked into, or called by, the product library.
+ *
+ * Every function restates one piece of the reference (KHRR-NBody) and cites
+ * the file:line it follows.  Operation order matches the reference source
+ * (left-to-right sums, no fused multiply-add: build with -ffp-contract=off)
+ * so that, compiled the same way, results agree bit-for-bit with the
+ * reference's own kernels compiled for the host (oracle/_ref); the tests pin
+ * this restatement against fixtures generated from oracle/_ref.
+ *
+ * Layouts: positions/velocities/accelerations are AoS xyz double triples
+ * (the reference's double3), masses and eps^2 are per body.
+ */
+#include <math.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+#define ORC_PI 3.14159265358979 /* common.cuh:7 */
+#define ORC_BLOCK 512           /* common.cuh:8 (BLOCK_SIZE) */
+
+/* ------------------------------------------------------------------------ */
+/* Analytic halo + bulge field                                               */
+/* ------------------------------------------------------------------------ */
+
+/* Field constants: the DataBlock fields dev_fex reads (common.cuh:39-55),
+ * derived on the host as nbody/src/nbody.cu:1111-1120 derives them. */
+typedef struct {
+    double Mh, a, Rh, Mb, b, Rb;
+    double Rh2, con, const1, Mh_inf, c_phi_h, c_phi_b;
+} orc_field;
+
+void orc_field_init(orc_field* f, double Mh, double a, double Rh, double Mb, double b,
+                    double Rb) {
+    const double Rh2 = 3.0 * Rh;
+    const double rcore1 = Rh / a;
+    const double rbcore1 = 1.0 / b;
+    const double rbcore2 = rbcore1 * rbcore1;
+    const double root1 = sqrt(1.0 + (Rb * Rb) * rbcore2);
+    f->Mh = Mh;
+    f->a = a;
+    f->Rh = Rh;
+    f->Mb = Mb;
+    f->b = b;
+    f->Rb = Rb;
+    f->Rh2 = Rh2;
+    f->con = Mh / (rcore1 - atan(rcore1));
+    f->const1 = Mb / (b * log(Rb * rbcore1 + root1) - Rb / root1);
+    f->c_phi_h = f->con / a * (0.5 * log(Rh2 * Rh2 / a / a + 1.0) + atan(Rh2 / a) * a / Rh2) + Mh / Rh2;
+    f->c_phi_b = Mb / Rb - f->const1 * log(Rb / b + root1) / Rb;
+    f->Mh_inf = Mh * (Rh2 / a - atan(Rh2 / a)) / (rcore1 - atan(rcore1));
+}
+
+/* dev_fex (nbody-kernel.cuh:8-40): external acceleration at p. */
+static void fex_one(const orc_field* F, const double* p, double* out) {
+    const double rr = sqrt(p[0] * p[0] + p[1] * p[1] + p[2] * p[2]);
+    if (rr > 0.0) {
+        const double rr3 = rr * rr * rr;
+        const double rrcore = rr / F->a;
+        const double rrbcore1 = rr / F->b;
+        const double root1 = sqrt(1.0 + rrbcore1 * rrbcore1);
+        double forcehalo, forceblg1;
+        if (rr < F->Rh2) forcehalo = -F->con * (rrcore - atan(rrcore)) / rr3;
+        else forcehalo = -F->Mh_inf / rr3;
+        if (rr < F->Rb) forceblg1 = -F->const1 * (F->b * log(rrbcore1 + root1) - rr / root1) / rr3;
+        else forceblg1 = -F->Mb / rr3;
+        const double forcesph = forceblg1 + forcehalo;
+        out[0] = forcesph * p[0];
+        out[1] = forcesph * p[1];
+        out[2] = forcesph * p[2];
+    } else {
+        out[0] = out[1] = out[2] = 0.0;
+    }
+}
+
+void orc_fex(const orc_field* F, int64_t n, const double* pos, double* out) {
+#pragma omp parallel for
+    for (int64_t i = 0; i < n; ++i) fex_one(F, pos + 3 * i, out + 3 * i);
+}
+
+/* ------------------------------------------------------------------------ */
+/* Direct sums                                                               */
+/* ------------------------------------------------------------------------ */
+
+/* ACCEL_kernel (nbody-kernel.cuh:89-142), FP64: for each target i,
+ * a_i = sum_{j=0..n-1} m_j d / (|d|^2 + (eps2_i + eps2_j)/2)^{3/2}, d = r_j - r_i,
+ * summed in j order.  out (nt x 3) is overwritten (targets NULL = all). */
+void orc_accel_f64(int64_t n, const double* pos, const double* mass, const double* eps2,
+                   int64_t nt, const int64_t* targets, double* out) {
+    const int64_t count = targets ? nt : n;
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int64_t k = 0; k < count; ++k) {
+        const int64_t i = targets ? targets[k] : k;
+        const double xi = pos[3 * i], yi = pos[3 * i + 1], zi = pos[3 * i + 2];
+        const double ei = eps2[i];
+        double fx = 0.0, fy = 0.0, fz = 0.0;
+        for (int64_t j = 0; j < n; ++j) {
+            const double dx = pos[3 * j] - xi;
+            const double dy = pos[3 * j + 1] - yi;
+            const double dz = pos[3 * j + 2] - zi;
+            const double den = sqrt(dx * dx + dy * dy + dz * dz + 0.5 * (ei + eps2[j]));
+            const double kk = mass[j] / (den * den * den);
+            fx += dx * kk;
+            fy += dy * kk;
+            fz += dz * kk;
+        }
+        out[3 * k] = fx;
+        out[3 * k + 1] = fy;
+        out[3 * k + 2] = fz;
+    }
+}
+
+/* ACCEL_kernel with real = float (the "reference FP32 kernel"): float
+ * positions/masses/eps2; the 0.5 literal keeps the softening term in double
+ * before the sqrt, whose result is rounded to float (nbody-kernel.cuh:124-131). */
+void orc_accel_f32(int64_t n, const double* pos, const double* mass, const double* eps2,
+                   int64_t nt, const int64_t* targets, double* out) {
+    float* p = (float*)malloc(sizeof(float) * 3 * (size_t)n);
+    float* m = (float*)malloc(sizeof(float) * (size_t)n);
+    float* e = (float*)malloc(sizeof(float) * (size_t)n);
+    for (int64_t i = 0; i < 3 * n; ++i) p[i] = (float)pos[i];
+    for (int64_t i = 0; i < n; ++i) {
+        m[i] = (float)mass[i];
+        e[i] = (float)eps2[i];
+    }
+    const int64_t count = targets ? nt : n;
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int64_t k = 0; k < count; ++k) {
+        const int64_t i = targets ? targets[k] : k;
+        const float xi = p[3 * i], yi = p[3 * i + 1], zi = p[3 * i + 2];
+        const float ei = e[i];
+        float fx = 0.0f, fy = 0.0f, fz = 0.0f;
+        for (int64_t j = 0; j < n; ++j) {
+            const float dx = p[3 * j] - xi;
+            const float dy = p[3 * j + 1] - yi;
+            const float dz = p[3 * j + 2] - zi;
+            const float d2 = dx * dx + dy * dy + dz * dz;
+            const float den = (float)sqrt((double)d2 + 0.5 * (double)(ei + e[j]));
+            const float kk = m[j] / (den * den * den);
+            fx += dx * kk;
+            fy += dy * kk;
+            fz += dz * kk;
+        }
+        out[3 * k] = fx;
+        out[3 * k + 1] = fy;
+        out[3 * k + 2] = fz;
+    }
+    free(p);
+    free(m);
+    free(e);
+}
+
+/* PHI_kernel (nbody-kernel.cuh:43-86), FP64: phi_i = -sum_j m_j /
+ * sqrt(|d|^2 + (eps2_i + eps2_j)/2), j = i included; out is overwritten. */
+void orc_phi_f64(int64_t n, const double* pos, const double* mass, const double* eps2,
+                 int64_t nt, const int64_t* targets, double* out) {
+    const int64_t count = targets ? nt : n;
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int64_t k = 0; k < count; ++k) {
+        const int64_t i = targets ? targets[k] : k;
+        const double xi = pos[3 * i], yi = pos[3 * i + 1], zi = pos[3 * i + 2];
+        const double ei = eps2[i];
+        double s = 0.0;
+        for (int64_t j = 0; j < n; ++j) {
+            const double dx = pos[3 * j] - xi;
+            const double dy = pos[3 * j + 1] - yi;
+            const double dz = pos[3 * j + 2] - zi;
+            s += mass[j] / sqrt(dx * dx + dy * dy + dz * dz + 0.5 * (ei + eps2[j]));
+        }
+        out[k] = 0.0 - s;
+    }
+}
+
+/* ------------------------------------------------------------------------ */
+/* Predictor-corrector                                                       */
+/* ------------------------------------------------------------------------ */
+
+/* kernelNbody_integTime (nbody-kernel.cuh:144-193), one call = one launch.
+ * istep 0 (predictor): vel_t = v + dt f, pos_t = r + dt/2 (v + vel_t);
+ * istep 1 (corrector): vel_t = (vel_t + v + dt f)/2, pos_t = r, acc0 = acc;
+ * f = acc + fex(r).  field NULL means no external field (all constants 0). */
+void orc_integ(int64_t n, const orc_field* F, const double* acc, double* pos_t, double* vel_t,
+               const double* pos, const double* vel, double dt, int istep, double* acc0) {
+#pragma omp parallel for
+    for (int64_t i = 0; i < n; ++i) {
+        const double* r = pos + 3 * i;
+        const double* v = vel + 3 * i;
+        double fe[3] = {0.0, 0.0, 0.0};
+        if (F) fex_one(F, r, fe);
+        double f[3];
+        for (int c = 0; c < 3; ++c) f[c] = acc[3 * i + c] + fe[c];
+        if (istep == 0) {
+            double vt[3];
+            for (int c = 0; c < 3; ++c) vt[c] = v[c] + dt * f[c];
+            for (int c = 0; c < 3; ++c) pos_t[3 * i + c] = r[c] + 0.5 * dt * (v[c] + vt[c]);
+            for (int c = 0; c < 3; ++c) vel_t[3 * i + c] = vt[c];
+        } else {
+            double vtt[3];
+            for (int c = 0; c < 3; ++c) vtt[c] = 0.5 * (vel_t[3 * i + c] + v[c] + dt * f[c]);
+            for (int c = 0; c < 3; ++c) pos_t[3 * i + c] = r[c];
+            for (int c = 0; c < 3; ++c) vel_t[3 * i + c] = vtt[c];
+            for (int c = 0; c < 3; ++c) acc0[3 * i + c] = acc[3 * i + c];
+        }
+    }
+}
+
+/* The reference time step (nbody/src/nbody.cu:1525-1582): predictor with
+ * acc, force at the predicted positions into acct, corrector.  acc (n x 3)
+ * carries a(t) in and a(t+dt) out; acct is the force workspace.
+ * compat_accumulate != 0 reproduces the reference's missing reset of acct
+ * (the force is added onto the previous step's acct); 0 overwrites. */
+void orc_run_steps(int64_t n, const orc_field* F, double* pos, double* vel, const double* mass,
+                   const double* eps2, double dt, int nsteps, int compat_accumulate, double* acc,
+                   double* acct) {
+    double* post = (double*)malloc(sizeof(double) * 3 * (size_t)n);
+    double* velt = (double*)malloc(sizeof(double) * 3 * (size_t)n);
+    double* tmp = (double*)malloc(sizeof(double) * 3 * (size_t)n);
+    for (int s = 0; s < nsteps; ++s) {
+        orc_integ(n, F, acc, post, velt, pos, vel, dt, 0, acc);
+        orc_accel_f64(n, post, mass, eps2, n, NULL, tmp);
+        if (compat_accumulate) {
+            for (int64_t k = 0; k < 3 * n; ++k) acct[k] += tmp[k];
+        } else {
+            memcpy(acct, tmp, sizeof(double) * 3 * (size_t)n);
+        }
+        orc_integ(n, F, acct, pos, vel, post, velt, dt, 1, acc);
+    }
+    free(post);
+    free(velt);
+    free(tmp);
+}
+
+/* ------------------------------------------------------------------------ */
+/* Conservation diagnostics                                                  */
+/* ------------------------------------------------------------------------ */
+
+/* result() reductions (nbody/src/nbody.cu:797-833).  out[16] =
+ * {Lx, Ly, Lz, Impx, Impy, Impz, Ek, Ep, E, R_max, Z_max, Vr_max, Vfi_max,
+ *  Vz_max, 0, 0}; Ek/Ep are the raw sums (E = (Ek + Ep)/2).  Serial order. */
+void orc_conservation(int64_t n, const double* pos, const double* vel, const double* mass,
+                      const double* psi, double* out) {
+    double Lx = 0, Ly = 0, Lz = 0, Ix = 0, Iy = 0, Iz = 0, Ek = 0, Ep = 0;
+    double Vr_max = 0, Vfi_max = 0, Vz_max = 0, R_max = 0, Z_max = 0;
+    for (int64_t i = 0; i < n; ++i) {
+        const double x = pos[3 * i], y = pos[3 * i + 1], z = pos[3 * i + 2];
+        const double vx = vel[3 * i], vy = vel[3 * i + 1], vz = vel[3 * i + 2];
+        const double r = sqrt(x * x + y * y);
+        double vr = 0.0, vfi = 0.0;
+        if (r > 0.0) {
+            vr = (vx * x + vy * y) / r;
+            vfi = (vy * x - vx * y) / r;
+        }
+        const double m = mass[i];
+        Lx += (vz * y - vy * z) * m;
+        Ly += (vx * z - vz * x) * m;
+        Lz += (vy * x - vx * y) * m;
+        Ix += m * vx;
+        Iy += m * vy;
+        Iz += m * vz;
+        Ek += m * (vx * vx + vy * vy + vz * vz);
+        Ep += m * psi[i];
+        if (fabs(vr) > Vr_max) Vr_max = fabs(vr);
+        if (vfi > Vfi_max) Vfi_max = vfi;
+        if (fabs(vz) > Vz_max) Vz_max = fabs(vz);
+        if (r > R_max) R_max = r;
+        if (fabs(z) > Z_max) Z_max = fabs(z);
+    }
+    out[0] = Lx;
+    out[1] = Ly;
+    out[2] = Lz;
+    out[3] = Ix;
+    out[4] = Iy;
+    out[5] = Iz;
+    out[6] = Ek;
+    out[7] = Ep;
+    out[8] = 0.5 * (Ek + Ep);
+    out[9] = R_max;
+    out[10] = Z_max;
+    out[11] = Vr_max;
+    out[12] = Vfi_max;
+    out[13] = Vz_max;
+    out[14] = 0.0;
+    out[15] = 0.0;
+}
+
+/* ------------------------------------------------------------------------ */
+/* p2mesh binning                                                            */
+/* ------------------------------------------------------------------------ */
+
+/* Cell coordinate of one axis (p2mesh-kernel.cuh:25-36): C truncation toward
+ * zero of (p - min)/cs, clamped to [0, g-1].  Out-of-range quotients follow
+ * the CUDA float->int conversion (saturating, NaN -> 0), which the clamp then
+ * maps to 0 or g-1; inside the int range this is exactly (int) + clamp. */
+static int cell_axis(double p, double lo, double cs, int g) {
+    const double q = (p - lo) / cs;
+    if (q >= (double)(g - 1)) return g - 1;
+    if (q > -1.0) return (int)q;
+    return 0;
+}
+
+/* assignParticlesToCells (p2mesh-kernel.cuh:11-57) in body order, plus the
+ * counts.  Note the reference's index quirks, reproduced: iz is clamped to
+ * gy-1 and the linear id is iz*gx*gy + iy*gz + ix.
+ * cell_id/id_in_cell: n; count: C (zeroed here). */
+void orc_assign(int64_t n, const double* pos, const double* lo, const double* cs, const int* g,
+                int* cell_id, int* id_in_cell, int* count, int64_t ncells) {
+    memset(count, 0, sizeof(int) * (size_t)ncells);
+    for (int64_t i = 0; i < n; ++i) {
+        const int ix = cell_axis(pos[3 * i], lo[0], cs[0], g[0]);
+        const int iy = cell_axis(pos[3 * i + 1], lo[1], cs[1], g[1]);
+        const int iz = cell_axis(pos[3 * i + 2], lo[2], cs[2], g[1]);
+        const int c = iz * g[0] * g[1] + iy * g[2] + ix;
+        cell_id[i] = c;
+        id_in_cell[i] = count[c]++;
+    }
+}
+
+/* Exclusive scan of the counts (the start offsets a correct computePrefixSums
+ * would produce), the reference's own start_id view (p2mesh-kernel.cuh:62-123:
+ * the in-block scan is discarded, so start_id[c] is the total of all earlier
+ * 512-cell blocks), and maxPBC, the inclusive scan of 512-cell block totals
+ * that computePrefixSums leaves in its second argument. */
+void orc_scan(int64_t ncells, const int* count, int* start_true, int* start_ref, int* maxpbc) {
+    const int64_t nb = (ncells + ORC_BLOCK - 1) / ORC_BLOCK;
+    int64_t run = 0;
+    for (int64_t c = 0; c < ncells; ++c) {
+        start_true[c] = (int)run;
+        run += count[c];
+    }
+    int64_t acc = 0;
+    for (int64_t b = 0; b < nb; ++b) {
+        int64_t tot = 0;
+        for (int64_t c = b * ORC_BLOCK; c < (b + 1) * ORC_BLOCK && c < ncells; ++c) tot += count[c];
+        const int64_t before = acc;
+        acc += tot;
+        maxpbc[b] = (int)acc;
+        for (int64_t c = b * ORC_BLOCK; c < (b + 1) * ORC_BLOCK && c < ncells; ++c)
+            start_ref[c] = (int)before;
+    }
+}
+
+/* computeCellMassesUnsorted (p2mesh-kernel.cuh:126-137) in body order. */
+void orc_cell_masses(int64_t n, const double* mass, const int* cell_id, double* cell_mass,
+                     int64_t ncells) {
+    memset(cell_mass, 0, sizeof(double) * (size_t)ncells);
+    for (int64_t i = 0; i < n; ++i) cell_mass[cell_id[i]] += mass[i];
+}
+
+/* computeCellPhiUnsorted (p2mesh-kernel.cuh:152-167) in body order; cell_phi
+ * is accumulated into (the reference does not reset it between saves). */
+void orc_cell_phi(int64_t n, const double* phi, const int* cell_id, const int* count,
+                  double* cell_phi) {
+    for (int64_t i = 0; i < n; ++i) cell_phi[cell_id[i]] += phi[i] / count[cell_id[i]];
+}
+
+/* ------------------------------------------------------------------------ */
+/* Damped-wave Poisson stencil                                               */
+/* ------------------------------------------------------------------------ */
+
+typedef struct {
+    int nx;
+    double dx, dt, c, diss_base, diss_extra, sim_l, bc_l;
+} orc_wave;
+
+#define ORC_AT(x, y, z, NX) ((int64_t)(x) + (int64_t)(y) * (NX) + (int64_t)(z) * (NX) * (NX))
+
+/* Sponge coefficient (wave-kernel.cuh:32-60).  Cell coordinates are
+ * ix*dx (not centred) and the x test compares against -(L - bc), as the
+ * reference does. */
+static double wave_diss(const orc_wave* W, int ix, int iy, int iz) {
+    const double x = ix * W->dx, y = iy * W->dx, z = iz * W->dx;
+    const double L = W->sim_l - W->bc_l;
+    double d = W->diss_base;
+    if (x > -L) d += W->diss_extra * fabs(x - L) * fabs(x - L);
+    else if (x < -L) d += W->diss_extra * fabs(x + L) * fabs(x + L);
+    if (y > L) d += W->diss_extra * fabs(y - L) * fabs(y - L);
+    else if (y < -L) d += W->diss_extra * fabs(y + L) * fabs(y + L);
+    if (z > L) d += W->diss_extra * fabs(z - L) * fabs(z - L);
+    else if (z < -L) d += W->diss_extra * fabs(z + L) * fabs(z + L);
+    return d;
+}
+
+/* wave_diss_iteration (wave-kernel.cuh:5-103), FP64, one full-mesh pass. */
+void orc_wave_iter_f64(const orc_wave* W, double* phi_new, const double* phi,
+                       const double* phi_old, const double* mass) {
+    const int NX = W->nx;
+    const double DX = W->dx, C = W->c, DT = W->dt;
+#pragma omp parallel for collapse(2)
+    for (int iz = 0; iz < NX; ++iz)
+        for (int iy = 0; iy < NX; ++iy)
+            for (int ix = 0; ix < NX; ++ix) {
+                const int64_t at = ORC_AT(ix, iy, iz, NX);
+                if (ix == 0 || ix == NX - 1 || iy == 0 || iy == NX - 1 || iz == 0 || iz == NX - 1) {
+                    phi_new[at] = 0.0;
+                    continue;
+                }
+                const double rho = mass[at] / (DX * DX * DX);
+                const double f = 4 * ORC_PI * 1.0 * rho;
+                const double diss = wave_diss(W, ix, iy, iz);
+                const double Q = diss * C * DT * 0.5;
+                const double Wt = 1 + Q;
+                const double K = C * C * (DT * DT) / (DX * DX);
+                const double KM = K / Wt;
+                const double KF = -(C * C) * (DT * DT) / Wt;
+                const double KA = 2 * (1. - 3 * K) / Wt;
+                const double KO = (Q - 1.) / Wt;
+                phi_new[at] = phi[ORC_AT(ix - 1, iy, iz, NX)] * KM + phi[ORC_AT(ix + 1, iy, iz, NX)] * KM +
+                              phi[ORC_AT(ix, iy - 1, iz, NX)] * KM + phi[ORC_AT(ix, iy + 1, iz, NX)] * KM +
+                              phi[ORC_AT(ix, iy, iz - 1, NX)] * KM + phi[ORC_AT(ix, iy, iz + 1, NX)] * KM +
+                              phi[at] * KA + phi_old[at] * KO + f * KF;
+            }
+}
+
+/* The same update in FP32 storage and arithmetic, with the per-cell
+ * coefficients evaluated in FP64 and rounded once (the product's FP32 form). */
+void orc_wave_iter_f32(const orc_wave* W, float* phi_new, const float* phi, const float* phi_old,
+                       const float* mass) {
+    const int NX = W->nx;
+    const double DX = W->dx, C = W->c, DT = W->dt;
+#pragma omp parallel for collapse(2)
+    for (int iz = 0; iz < NX; ++iz)
+        for (int iy = 0; iy < NX; ++iy)
+            for (int ix = 0; ix < NX; ++ix) {
+                const int64_t at = ORC_AT(ix, iy, iz, NX);
+                if (ix == 0 || ix == NX - 1 || iy == 0 || iy == NX - 1 || iz == 0 || iz == NX - 1) {
+                    phi_new[at] = 0.0f;
+                    continue;
+                }
+                const double diss = wave_diss(W, ix, iy, iz);
+                const double Q = diss * C * DT * 0.5;
+                const double Wt = 1 + Q;
+                const double K = C * C * (DT * DT) / (DX * DX);
+                const float KM = (float)(K / Wt);
+                const float KA = (float)(2 * (1. - 3 * K) / Wt);
+                const float KO = (float)((Q - 1.) / Wt);
+                const float KS = (float)(-(C * C) * (DT * DT) / Wt * (4 * ORC_PI) / (DX * DX * DX));
+                const float nb = ((phi[ORC_AT(ix - 1, iy, iz, NX)] + phi[ORC_AT(ix + 1, iy, iz, NX)]) +
+                                  (phi[ORC_AT(ix, iy - 1, iz, NX)] + phi[ORC_AT(ix, iy + 1, iz, NX)])) +
+                                 (phi[ORC_AT(ix, iy, iz - 1, NX)] + phi[ORC_AT(ix, iy, iz + 1, NX)]);
+                phi_new[at] = nb * KM + phi[at] * KA + phi_old[at] * KO + mass[at] * KS;
+            }
+}
+
+/* acc_field (p2mesh-kernel.cuh:169-225) over the whole mesh: -grad(phi)/dx
+ * by central differences, one-sided on the faces.  cell_acc: C x 3. */
+void orc_acc_field(int NX, double DX, const double* phi, double* cell_acc) {
+#pragma omp parallel for collapse(2)
+    for (int iz = 0; iz < NX; ++iz)
+        for (int iy = 0; iy < NX; ++iy)
+            for (int ix = 0; ix < NX; ++ix) {
+                const int64_t at = ORC_AT(ix, iy, iz, NX);
+                double d[3];
+                if (ix == 0) d[0] = phi[ORC_AT(ix + 1, iy, iz, NX)] - phi[at];
+                else if (ix == NX - 1) d[0] = phi[at] - phi[ORC_AT(ix - 1, iy, iz, NX)];
+                else d[0] = 0.5 * (phi[ORC_AT(ix + 1, iy, iz, NX)] - phi[ORC_AT(ix - 1, iy, iz, NX)]);
+                if (iy == 0) d[1] = phi[ORC_AT(ix, iy + 1, iz, NX)] - phi[at];
+                else if (iy == NX - 1) d[1] = phi[at] - phi[ORC_AT(ix, iy - 1, iz, NX)];
+                else d[1] = 0.5 * (phi[ORC_AT(ix, iy + 1, iz, NX)] - phi[ORC_AT(ix, iy - 1, iz, NX)]);
+                if (iz == 0) d[2] = phi[ORC_AT(ix, iy, iz + 1, NX)] - phi[at];
+                else if (iz == NX - 1) d[2] = phi[at] - phi[ORC_AT(ix, iy, iz - 1, NX)];
+                else d[2] = 0.5 * (phi[ORC_AT(ix, iy, iz + 1, NX)] - phi[ORC_AT(ix, iy, iz - 1, NX)]);
+                const double coef = -1. / DX;
+                cell_acc[3 * at] = d[0] * coef;
+                cell_acc[3 * at + 1] = d[1] * coef;
+                cell_acc[3 * at + 2] = d[2] * coef;
+            }
+}
+
+/* apply_acceleration_to_particles + apply_cell_to_particles
+ * (p2mesh-kernel.cuh:227-254): NGP gather of cell values to bodies. */
+void orc_gather(int64_t n, const int* cell_id, const double* cell_acc, const double* cell_phi,
+                double* acc, double* phi) {
+#pragma omp parallel for
+    for (int64_t i = 0; i < n; ++i) {
+        const int64_t c = cell_id[i];
+        if (acc) {
+            acc[3 * i] = cell_acc[3 * c];
+            acc[3 * i + 1] = cell_acc[3 * c + 1];
+            acc[3 * i + 2] = cell_acc[3 * c + 2];
+        }
+        if (phi) phi[i] = cell_phi[c];
+    }
+}
+
+int orc_max_threads(void) {
+#ifdef _OPENMP
+    return omp_get_max_threads();
+#else
+    return 1;
+#endif
+}

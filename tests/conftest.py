@@ -1,0 +1,32 @@
+"""Shared pytest setup: the `gpu` marker and paths to the package and oracle."""
+import pathlib
+import sys
+
+import pytest
+
+ROOT = pathlib.Path(__file__).resolve().parents[1]
+PKG = ROOT / "khrr-nbody_b200"
+ORACLE = ROOT / "oracle"
+GOLDEN = ROOT / "tests" / "golden"
+for p in (PKG, ORACLE):
+    if str(p) not in sys.path:
+        sys.path.insert(0, str(p))
+
+
+def pytest_configure(config):
+    config.addinivalue_line("markers", "gpu: needs a CUDA device (B200, sm_100a)")
+
+
+@pytest.fixture(scope="session")
+def oracle():
+    from pyoracle import Oracle
+    return Oracle()
+
+
+@pytest.fixture(scope="session")
+def golden():
+    import numpy as np
+
+    def load(name):
+        return dict(np.load(GOLDEN / name))
+    return load
