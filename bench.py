@@ -1,0 +1,400 @@
+#!/usr/bin/env python3
+"""Benchmark of the direct-sum gravity time step on B200.
+
+Workload (one "step"): predictor -> FP32 direct-sum force pass -> corrector
+over one 786,432-body disk galaxy (262,144 stars + 524,288 dark-matter bodies,
+masses 1.0 / 6.699356, eps 0.004, dt 0.002), generated from a seed (the
+reference's own start_DM0.txt is not shipped).  The metric is pair
+interactions per second (n^2 per force pass, j = i counted as the reference
+does); the roofline of the force kernel is FP32-pipe issue at the 20-flop-per-
+interaction convention.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl khrr|reference]
+
+N > 1 (under torchrun) runs N independent replicas (the path is pinned to one
+GPU per galaxy; there is no data-path collective), timed as the max over ranks.
+--impl reference times the reference's own ACCEL_kernel compiled for the host
+(oracle/_ref, OpenMP over all host threads) on a bounded target sample.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import pathlib
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = pathlib.Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT / "khrr-nbody_b200"))
+
+METRIC = "G interactions/s & %FP32 peak at 786k bodies; batched vs plain; err vs FP64"
+UNIT = "G interactions/s"
+N_STARS, N_DM = 262144, 524288
+DT = 0.002
+SEED = 1000
+FLOPS_PER_PAIR = 20
+SMS, FP32_LANES = 148, 128
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["khrr", "reference"], default="khrr")
+    ap.add_argument("--no-ensemble", action="store_true", help="skip the 64-galaxy batched-vs-plain leg")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--n-stars", type=int, default=N_STARS)
+    ap.add_argument("--n-dm", type=int, default=N_DM)
+    return ap.parse_args()
+
+
+def measured_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        try:
+            return json.loads(p.read_text())
+        except Exception:
+            return {}
+    return {}
+
+
+def workload(ns, nd):
+    from khrr.galaxy import make_galaxy
+    pos, vel, mass, eps = make_galaxy(ns, nd, SEED).arrays()
+    return pos, vel, mass, eps * eps
+
+
+def config(args, extra=None):
+    c = {"workload": f"disk galaxy N={args.n_stars + args.n_dm} ({args.n_stars} stars + {args.n_dm} DM), "
+                     f"eps 0.004, dt {DT}, predictor-force-corrector step",
+         "n_bodies": args.n_stars + args.n_dm, "dt": DT, "seed": SEED,
+         "l2": "256 MB buffer written between timed steps (inside the timed region)",
+         "parallelism": f"replicas x{args.gpus}" if args.gpus > 1 else "single GPU"}
+    if extra:
+        c.update(extra)
+    return c
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_id):
+        self.proc = None
+        self.gpu_id = gpu_id
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200",
+                 "-i", str(self.gpu_id)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        self.lines = []
+        if self.proc:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except Exception:
+                self.proc.kill()
+                out = ""
+            self.lines = [l for l in out.splitlines() if l.strip()]
+
+    def summary(self):
+        if not getattr(self, "lines", None):
+            return None
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in self.lines:
+            f = [x.strip() for x in l.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+            except ValueError:
+                continue
+            for k, name in enumerate(names):
+                if f[5 + k].lower().startswith("active"):
+                    reasons.add(name)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "samples": len(sm),
+                "reasons": sorted(reasons)}
+
+
+# ---------------------------------------------------------------------------
+# reference arm: the reference's ACCEL_kernel compiled for the host
+# ---------------------------------------------------------------------------
+def cpu_reference_sample(pos, mass, eps2, seconds, rng):
+    """Times the host-compiled reference (or the oracle port when _ref is
+    absent) on a seeded target subset; returns (pairs/s, cores, kind, sample)."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import pyoracle
+    n = len(mass)
+    try:
+        ref = pyoracle.Reference()
+        run = ref.accel
+        cores = ref.max_threads()
+        kind = "reference"
+        what = "ACCEL_kernel (nbody-kernel.cuh:89-142) FP64, host build of the reference (oracle/_ref)"
+    except FileNotFoundError:
+        orc = pyoracle.Oracle()
+        run = orc.accel_f64
+        cores = orc.max_threads()
+        kind = "port"
+        what = "FP64 direct sum, oracle restatement (oracle/oracle.c)"
+    t_cal = max(2 * cores, 16)
+    tg = rng.choice(n, t_cal, replace=False)
+    t0 = time.perf_counter()
+    run(pos, mass, eps2, tg)
+    rate = t_cal * n / (time.perf_counter() - t0)
+    nt = int(min(n, max(t_cal, rate * seconds / n)))
+    tg = rng.choice(n, nt, replace=False)
+    t0 = time.perf_counter()
+    run(pos, mass, eps2, tg)
+    dt = time.perf_counter() - t0
+    return nt * n / dt, cores, kind, f"{nt} seeded targets x {n} sources, {what}", dt
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    pos, vel, mass, eps2 = workload(args.n_stars, args.n_dm)
+    rng = np.random.default_rng(7)
+    rates, total_t, pairs = [], 0.0, 0.0
+    for k in range(args.warmup + args.steps):
+        rate, cores, kind, sample, dt = cpu_reference_sample(pos, mass, eps2, 6.0, rng)
+        if k >= args.warmup:
+            rates.append(rate)
+            total_t += dt
+            pairs += rate * dt
+    value = pairs / total_t / 1e9
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": (len(mass) ** 2) / (value * 1e9) * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator)",
+            "config": config(args),
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": kind,
+                             "sample": sample + "; ms_per_step extrapolates one full n^2 force pass"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ---------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------
+def ensemble_leg(khrr, ctx_device, torch, steps=8):
+    """Configs' 64-galaxy uneven ensemble: one batched step launch vs one
+    force launch per system (the plain path), in galaxy-steps/s."""
+    from khrr.galaxy import ensemble_sizes, make_galaxy
+    sizes = ensemble_sizes(64, seed=77)
+    parts = [make_galaxy(ns, nd, 2000 + k).arrays() for k, (ns, nd) in enumerate(sizes)]
+    pos = np.concatenate([p[0] for p in parts])
+    vel = np.concatenate([p[1] for p in parts])
+    mass = np.concatenate([p[2] for p in parts])
+    eps2 = np.concatenate([p[3] ** 2 for p in parts])
+    off = np.cumsum([0] + [len(p[2]) for p in parts])
+    out = {"galaxies": 64, "bodies": int(off[-1]), "pairs_per_step": float(sum(len(p[2]) ** 2 for p in parts))}
+    ctx = khrr.Context(ctx_device)
+    try:
+        for label, flags in (("batched", 0), ("plain", khrr.PLAIN)):
+            ctx.upload(pos, vel, mass, eps2, offsets=off)
+            ctx.forces(khrr.ACC | (flags & khrr.PLAIN))
+            ctx.step(DT, 2, flags)
+            s = torch.cuda.ExternalStream(ctx.stream)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            ctx.synchronize()
+            e0.record(s)
+            ctx.step(DT, steps, flags)
+            e1.record(s)
+            e1.synchronize()
+            ms = e0.elapsed_time(e1)
+            out[label + "_galaxy_steps_per_s"] = 64 * steps / (ms * 1e-3)
+            out[label + "_ms_per_step"] = ms / steps
+        # accuracy of the batched pass vs FP64 on sampled bodies of every galaxy
+        ctx.upload(pos, vel, mass, eps2, offsets=off)
+        ctx.forces(khrr.ACC)
+        acc = ctx.download(pos=False, vel=False, phi=False)["acc"]
+        rng = np.random.default_rng(3)
+        tg = np.sort(rng.choice(len(mass), 4096, replace=False))
+        ref, _ = ctx.accel_fp64_sample(tg)
+        out["acc_rel_rms_vs_fp64"] = float(np.sqrt(((acc[tg] - ref) ** 2).sum() / (ref ** 2).sum()))
+    finally:
+        ctx.close()
+    out["batched_over_plain"] = out["batched_galaxy_steps_per_s"] / out["plain_galaxy_steps_per_s"]
+    return out
+
+
+def run_khrr(args):
+    import torch
+    import khrr
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+
+    def barrier():
+        if dist:
+            dist.barrier()
+
+    pos, vel, mass, eps2 = workload(args.n_stars, args.n_dm)
+    n = len(mass)
+    ctx = khrr.Context(local)
+    ctx.upload(pos, vel, mass, eps2)
+    ctx.forces(khrr.ACC)
+
+    # accuracy vs FP64 on 4096 seeded targets (GPU FP64 direct sum)
+    acc0 = ctx.download(pos=False, vel=False, phi=False)["acc"]
+    rng = np.random.default_rng(11)
+    tg = np.sort(rng.choice(n, min(4096, n), replace=False))
+    ref, _ = ctx.accel_fp64_sample(tg)
+    err = float(np.sqrt(((acc0[tg] - ref) ** 2).sum() / (ref ** 2).sum()))
+    err_max = float(np.max(np.linalg.norm(acc0[tg] - ref, axis=1) / np.linalg.norm(ref, axis=1)))
+
+    stream = torch.cuda.ExternalStream(ctx.stream)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
+    torch.cuda.synchronize()
+    for _ in range(args.warmup):
+        ctx.step(DT, 1)
+        with torch.cuda.stream(stream):
+            flush.zero_()
+    ctx.synchronize()
+    barrier()
+    torch.cuda.synchronize()
+    ctx.enable_timing(True)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    gpu_id = local
+    try:
+        gpu_id = "GPU-" + str(torch.cuda.get_device_properties(local).uuid)
+    except Exception:
+        pass
+    with ClockSampler(gpu_id) as clk:
+        ev0.record(stream)
+        for _ in range(args.steps):
+            ctx.step(DT, 1)
+            with torch.cuda.stream(stream):
+                flush.zero_()
+        ev1.record(stream)
+        ev1.synchronize()
+    ms = ev0.elapsed_time(ev1)
+    force_ms, launches, pairs_timed = ctx.force_timing()
+    ctx.enable_timing(False)
+    barrier()
+    ms_max = ms
+    if dist:
+        t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_max = float(t.item())
+    pairs_step = float(n) * n
+    value = world * pairs_step * args.steps / (ms_max * 1e-3) / 1e9
+
+    # end to end through the C ABI: pinned host inputs -> step -> host outputs
+    pin = lambda shape: torch.empty(shape, dtype=torch.float64, pin_memory=True).numpy()
+    h_pos, h_vel, h_mass, h_eps2, h_acc = pin((n, 3)), pin((n, 3)), pin(n), pin(n), pin((n, 3))
+    o_pos, o_vel, o_acc = pin((n, 3)), pin((n, 3)), pin((n, 3))
+    h_pos[:], h_vel[:], h_mass[:], h_eps2[:], h_acc[:] = pos, vel, mass, eps2, acc0
+    ptr = lambda a: a.ctypes.data
+    e2e_ms = []
+    for k in range(args.warmup + args.steps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        ctx.upload_ptrs(n, ptr(h_pos), ptr(h_vel), ptr(h_mass), ptr(h_eps2))
+        ctx.set_accelerations_ptr(ptr(h_acc))
+        ctx.step(DT, 1)
+        ctx.download_into(o_pos.ctypes.data, o_vel.ctypes.data, o_acc.ctypes.data, None)
+        e1.record(stream)
+        e1.synchronize()
+        if k >= args.warmup:
+            e2e_ms.append(e0.elapsed_time(e1))
+    e2e_total = sum(e2e_ms)
+    if dist:
+        t = torch.tensor([e2e_total], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_total = float(t.item())
+    e2e_value = world * pairs_step * args.steps / (e2e_total * 1e-3) / 1e9
+
+    peaks = measured_peaks()
+    sm_max = float(peaks.get("sm_max_mhz", 1965.0))
+    peak_tflops = SMS * FP32_LANES * 2 * sm_max * 1e6 / 1e12
+    avg_launch_s = force_ms / max(launches, 1) * 1e-3
+    achieved = FLOPS_PER_PAIR * (pairs_timed / max(launches, 1)) / avg_launch_s / 1e12
+    probe = ctx.fp32_probe()
+
+    ens = None
+    if not args.no_ensemble and rank == 0:
+        ens = ensemble_leg(khrr, local, torch)
+    ctx.close()
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        rate, cores, kind, sample, _ = cpu_reference_sample(pos, mass, eps2, 15.0, np.random.default_rng(5))
+        cpu = {"value": rate / 1e9, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample}
+
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return 0
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32 pair terms (compensated sums), f64 integrator",
+        "data": "synthetic (seeded disk-galaxy generator)",
+        "config": config(args, {"tuning": None}),
+        "pct_fp32_peak": 100.0 * achieved / peak_tflops,
+        "acc_rel_rms_vs_fp64": err, "acc_rel_max_vs_fp64": err_max, "acc_err_targets": int(len(tg)),
+        "roofline": {"bound": "fp32", "kernel": "force_kernel", "achieved": achieved, "peak": peak_tflops,
+                     "unit": "TFLOP/s", "frac": achieved / peak_tflops, "traffic": None,
+                     "flops_per_pair": FLOPS_PER_PAIR, "pairs_per_launch": pairs_timed / max(launches, 1),
+                     "avg_launch_ms": avg_launch_s * 1e3,
+                     "peak_basis": f"nominal FP32: {SMS} SMs x {FP32_LANES} lanes x 2 flops x {sm_max:.0f} MHz "
+                                   "(sm_max_mhz of MEASURED_PEAKS.json)",
+                     "fp32_fma_probe_tflops": probe},
+        "cpu_baseline": cpu,
+        "e2e": {"value": e2e_value, "unit": UNIT,
+                "h2d_bytes_per_step": int(n * (24 + 24 + 8 + 8 + 24)),
+                "d2h_bytes_per_step": int(n * (24 + 24 + 24)),
+                "what": "khrr_upload_state + khrr_set_accelerations (pinned host) + khrr_step(1) + "
+                        "khrr_download_state(pos, vel, acc)"},
+        "gpu_launches": 2 * args.steps,
+        "clocks": clk.summary(),
+        "ensemble": ens,
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_khrr(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,171 @@
+/*
+ * khrr.h - C ABI of the B200 (sm_100a) KHRR-NBody hot path.
+ *
+ * The reference (KHRR-NBody) has no plugin layer: its driver nbody/src/nbody.cu
+ * calls __global__ kernels directly through its RR helper
+ * (CuCall(kernel, grid, block)(args...)), passing raw device pointers in the
+ * reference's layouts (double3 AoS positions, double masses/eps^2,
+ * CellInfo/ParticleCellInfo int pairs) and scalars through __constant__
+ * DataBlock / WaveEqData.  This header is the drop-in boundary for that path:
+ *
+ *  - kernel-level entry points (khrr_accel, khrr_phi, khrr_integ_time, ...)
+ *    take the same device pointers, layouts and accumulate semantics as the
+ *    reference kernel each one replaces (cited per function);
+ *  - a simulation-level API (khrr_upload_state / khrr_step / ...) owns the
+ *    device state for the reference's time loop, in one or many systems;
+ *  - host-only I/O functions read and write the reference's files.
+ *
+ * Conventions: every function returns khrr_status (no exceptions cross the
+ * ABI); khrr_last_error() describes the last failure on a context.  Device
+ * work is enqueued on the context's stream (khrr_set_stream to use another);
+ * host pointers are borrowed for the duration of the call.  One context per
+ * host thread.  Plain C types only.
+ */
+#ifndef KHRR_H
+#define KHRR_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define KHRR_ABI_VERSION 1
+
+typedef enum khrr_status {
+    KHRR_OK = 0,
+    KHRR_ERR_INVALID_ARG = 1,  /* bad pointer, size or parameter            */
+    KHRR_ERR_NOT_MULTIPLE = 2, /* size violates a documented multiple        */
+    KHRR_ERR_CUDA = 3,         /* CUDA runtime error (see khrr_last_error)   */
+    KHRR_ERR_IO = 4,           /* file missing, unreadable or malformed      */
+    KHRR_ERR_TIMEOUT = 5,      /* a bounded device wait gave up              */
+    KHRR_ERR_STATE = 6,        /* call out of order (e.g. step before upload)*/
+    KHRR_ERR_OOM = 7,          /* device allocation failed                   */
+    KHRR_ERR_UNSUPPORTED = 8   /* no device / wrong architecture             */
+} khrr_status;
+
+typedef struct khrr_ctx khrr_ctx;
+
+/* Force-evaluation flags. */
+enum {
+    KHRR_ACC = 1,               /* accelerations (ACCEL_kernel)                   */
+    KHRR_PHI = 2,               /* potentials (PHI_kernel), fused in the same pass */
+    KHRR_COMPAT_ACCUMULATE = 4, /* reference time loop: the step force is added to
+                                   the previous step's (nbody.cu:1559-1566 never
+                                   zeroes acct_); default overwrites             */
+    KHRR_PLAIN = 8,             /* one system per launch, no j-split (baseline)   */
+    KHRR_OVERWRITE = 16         /* kernel-level calls: overwrite instead of +=    */
+};
+
+/* Analytic halo + bulge parameters (__gr_par.ini lines 1-6); the derived
+ * constants are computed as nbody/src/nbody.cu:1111-1120 does. */
+typedef struct khrr_field_params {
+    double Mh, a, Rh, Mb, b, Rb;
+} khrr_field_params;
+
+/* Conservation diagnostics of result() (nbody/src/nbody.cu:797-833), reduced
+ * on the GPU in FP64.  Ek and Ep are the raw sums; E = (Ek + Ep) / 2. */
+typedef struct khrr_lie {
+    double L[3];
+    double Imp[3];
+    double Ek, Ep, E;
+    double R_max, Z_max, Vr_max, Vfi_max, Vz_max;
+} khrr_lie;
+
+/* Force-kernel shape: threads per CTA, i bodies per thread, j-tile size,
+ * and j_split = number of j chunks per system (0 = chosen automatically). */
+typedef struct khrr_tuning {
+    int threads;
+    int i_per_thread;
+    int j_tile;
+    int j_split;
+} khrr_tuning;
+
+/* ---- library / context ---------------------------------------------------- */
+int khrr_abi_version(void);
+const char* khrr_status_name(khrr_status s);
+/* Creates a context on CUDA device `device` (a B200, sm_100). */
+khrr_status khrr_create(int device, khrr_ctx** out);
+void khrr_destroy(khrr_ctx* ctx);
+const char* khrr_last_error(const khrr_ctx* ctx);
+/* The context's stream (cudaStream_t) and a way to replace it (NULL restores
+ * the context's own stream). */
+void* khrr_get_stream(khrr_ctx* ctx);
+khrr_status khrr_set_stream(khrr_ctx* ctx, void* stream);
+khrr_status khrr_synchronize(khrr_ctx* ctx);
+
+/* ---- kernel-level entry points (device pointers) ------------------------ */
+/* ACCEL_kernel (nbody-kernel.cuh:89-142): acc[i] += sum_j m_j d/(d^2 +
+ * (eps2_i + eps2_j)/2)^{3/2}, d = pos_j[j] - pos_i[i], over i, j < n
+ * (KHRR_OVERWRITE: acc = sum).  pos_*, acc: n double3 (AoS xyz); mass_j,
+ * eps2_j: n doubles.  Pair terms in FP32 with compensated sums; any n >= 1
+ * (the reference needs n % 512 == 0). */
+khrr_status khrr_accel(khrr_ctx* ctx, double* acc, const double* pos_i, const double* pos_j,
+                       const double* mass_j, const double* eps2_j, int64_t n, int flags);
+/* PHI_kernel (nbody-kernel.cuh:43-86): phi[i] -= sum_j m_j/sqrt(d^2 +
+ * (eps2_i + eps2_j)/2), j = i included (KHRR_OVERWRITE: phi = -sum). */
+khrr_status khrr_phi(khrr_ctx* ctx, double* phi, const double* pos_i, const double* pos_j,
+                     const double* mass_j, const double* eps2_j, int64_t n, int flags);
+/* kernelNbody_integTime (nbody-kernel.cuh:144-193), FP64, with the context's
+ * external field: istep 0 = predictor, 1 = corrector; same argument roles. */
+khrr_status khrr_integ_time(khrr_ctx* ctx, const double* acc, double* pos_t, double* vel_t,
+                            const double* pos, const double* vel, double dt, int istep,
+                            double t, double* acc0, int64_t n);
+
+/* ---- simulation-level API (context-owned device state) ------------------ */
+/* External field for all later integration; NULL disables it. */
+khrr_status khrr_set_external_field(khrr_ctx* ctx, const khrr_field_params* p);
+/* Uploads n bodies: pos, vel (n x 3, AoS), mass and eps2 (n).  Systems are
+ * independent (no mutual gravity): nsys >= 1 ranges given by sys_offsets
+ * (nsys + 1 increasing offsets, first 0, last n); sys_offsets NULL = one
+ * system.  Resets acc/phi to zero (call khrr_forces for a(t0)). */
+khrr_status khrr_upload_state(khrr_ctx* ctx, int64_t n, const double* pos, const double* vel,
+                              const double* mass, const double* eps2, int nsys,
+                              const int64_t* sys_offsets);
+/* Copies the state back; any pointer may be NULL.  acc excludes the external
+ * field (the reference's acc0); phi is from the last KHRR_PHI evaluation. */
+khrr_status khrr_download_state(khrr_ctx* ctx, double* pos, double* vel, double* acc,
+                                double* phi);
+/* Sets a(t) (n x 3, without the external field) after an upload, e.g. when a
+ * run resumes with known accelerations; the next khrr_step uses it. */
+khrr_status khrr_set_accelerations(khrr_ctx* ctx, const double* acc);
+/* FP64 direct sum on the GPU for nt sampled bodies (indices into the uploaded
+ * order) over their own system, at the current positions: the accuracy
+ * reference each run reports against.  acc: nt x 3, phi: nt (either NULL). */
+khrr_status khrr_accel_fp64_sample(khrr_ctx* ctx, const int64_t* targets, int64_t nt, double* acc,
+                                   double* phi);
+/* Forces at the current positions (KHRR_ACC and/or KHRR_PHI; KHRR_PLAIN). */
+khrr_status khrr_forces(khrr_ctx* ctx, int flags);
+/* nsteps predictor -> force -> corrector steps of size dt (nbody.cu:1525-1582),
+ * replayed from a CUDA graph.  flags: KHRR_PHI evaluates the potential at the
+ * new positions in the last step's force pass; KHRR_COMPAT_ACCUMULATE;
+ * KHRR_PLAIN (per-system launches). */
+khrr_status khrr_step(khrr_ctx* ctx, double dt, int nsteps, int flags);
+/* L, Imp, Ek, Ep, E and maxima over all bodies (uses the last phi). */
+khrr_status khrr_conservation(khrr_ctx* ctx, khrr_lie* out);
+
+/* Force-kernel shape; khrr_autotune times the candidates on the current
+ * state and caches the winner per body count in cache_path (NULL = no cache). */
+khrr_status khrr_set_tuning(khrr_ctx* ctx, const khrr_tuning* t);
+khrr_status khrr_get_tuning(khrr_ctx* ctx, khrr_tuning* t);
+khrr_status khrr_autotune(khrr_ctx* ctx, const char* cache_path);
+
+/* Device timing of the force kernel: when enabled, every force launch is
+ * bracketed by CUDA events on the launching stream; khrr_force_timing returns
+ * (after a synchronize) the summed milliseconds and the launch count since the
+ * last call, and the pair interactions those launches computed. */
+khrr_status khrr_enable_timing(khrr_ctx* ctx, int enable);
+khrr_status khrr_force_timing(khrr_ctx* ctx, double* ms, int64_t* launches,
+                              double* interactions);
+/* Pair interactions one force pass computes on the uploaded state
+ * (sum over systems of n_k^2, j = i counted as the reference does). */
+khrr_status khrr_pair_count(khrr_ctx* ctx, double* pairs);
+/* FP32 FMA throughput probe: a dependent-chain FMA kernel on all SMs;
+ * returns TFLOP/s (2 flops per FMA) measured with CUDA events. */
+khrr_status khrr_fp32_probe(khrr_ctx* ctx, double* tflops);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* KHRR_H */

@@ -1,0 +1,115 @@
+// Internal declarations shared by the CUDA kernels (*.cu) and the host
+// runtime (*.cpp) of libkhrr.  Not part of the public ABI (include/khrr.h).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+namespace khrr {
+
+// Bodies of each system are padded on the device to a multiple of this with
+// zero-mass "ghost" bodies, so every j tile is whole and 16-byte aligned.
+constexpr int kPad = 128;
+// Error codes a kernel can raise through the context's device flag word.
+constexpr unsigned kErrTimeout = 1u;
+
+// One unit of force work: a tile of i bodies against a chunk of j bodies of
+// the same system.  Indices are padded device indices.
+struct WorkItem {
+    int i_begin;  // first i body of the tile
+    int i_end;    // end of the system's real bodies (tile entries past it are skipped)
+    int j_begin;  // first j body of the chunk (multiple of the j tile)
+    int j_end;    // end of the chunk (multiple of the j tile)
+    int slot;     // partial-sum slot this chunk writes
+    int sys;      // system index
+    int pad0, pad1;
+};
+
+// Arguments of one force-kernel launch.
+struct ForceArgs {
+    const float4* body;      // padded FP32 shadow of the j bodies: x, y, z, m
+    const float* hsoft;      // padded 0.5 * eps2 (FP32) of the j bodies
+    const float4* ibody;     // i bodies (x, y, z; equal to body unless the i and j sets differ)
+    const float* ihsoft;     // 0.5 * eps2 of the i bodies
+    const WorkItem* items;   // work queue
+    int n_items;
+    unsigned* queue;         // next-item counter (zeroed before each launch)
+    double4* part;           // partial sums [slot][npad]: ax, ay, az, sum m/r
+    long long npad;          // slot stride
+    float h_uniform;         // 0.5 * eps2 when every body shares it
+    unsigned* err;           // device error flag word
+};
+
+// One compiled force-kernel instance.
+struct ForceVariant {
+    int threads, i_per_thread, j_tile, stages;
+    bool uniform_eps, acc, phi;
+    const void* fn;
+    size_t smem;
+};
+
+// Derived constants of the analytic halo/bulge field (dev_fex operands).
+struct FieldConsts {
+    double a, b, Rb, Mb, Rh2, con, const1, Mh_inf;
+    int enabled;
+};
+
+FieldConsts make_field(double Mh, double a, double Rh, double Mb, double b, double Rb);
+
+// ---- force.cu ---------------------------------------------------------------
+int force_variant_count();
+const ForceVariant* force_variant(int idx);
+const ForceVariant* find_force_variant(int threads, int ipt, int jt, bool unif, bool acc,
+                                       bool phi);
+cudaError_t launch_force(const ForceVariant* v, const ForceArgs& a, int grid, cudaStream_t s);
+// FP64 AoS positions -> padded FP32 shadow (x, y, z, m) and 0.5 * eps2.
+cudaError_t launch_pack(const double* pos, const double* mass, const double* eps2, int64_t n,
+                        int64_t npad, float4* body, float* hsoft, cudaStream_t s);
+// Partials -> out[i] (+)= sum_s part[s][i] (xyz) and/or phi[i] (-)= ...
+cudaError_t launch_reduce_partials(const double4* part, long long npad, int nslots, int64_t n,
+                                   double* acc, double* phi, bool overwrite, cudaStream_t s);
+cudaError_t launch_fp32_probe(float* out, int iters, int grid, int block, cudaStream_t s);
+// FP64 direct sum for sampled targets: tgt[k] is a padded index, [jb[k], je[k])
+// its system's padded body range; out4[k] = (ax, ay, az, phi).
+cudaError_t launch_fp64_sample(const double* pos, const double* mass, const double* eps2,
+                               const int64_t* tgt, const int64_t* jb, const int64_t* je, int64_t nt,
+                               double* out4, cudaStream_t s);
+
+// ---- integrate.cu -----------------------------------------------------------
+struct StepArgs {
+    double* pos;          // x(t)           [npad] double3
+    double* vel;          // v(t)
+    double* acc;          // a(t) without the external field (acc0)
+    double* post;         // predicted x*
+    double* velt;         // predicted v*
+    double* acct;         // force workspace of the literal reference loop
+    const double* mass;   // [npad]
+    double* phi;          // [npad] potential (written when want_phi)
+    float4* body;         // FP32 shadow written with the predicted positions
+    const double4* part;  // force partials [slot][npad]
+    long long npad;
+    const unsigned char* nsplit;  // partial slots per body
+    int64_t n;            // padded count
+    double dt;
+    FieldConsts field;
+    int compat_accumulate;
+    int want_phi;
+    int predict_next;
+};
+cudaError_t launch_predictor(const StepArgs& a, cudaStream_t s);
+cudaError_t launch_corrector(const StepArgs& a, cudaStream_t s);
+// Reduce partials into acc/phi of the state (khrr_forces).
+cudaError_t launch_collect(const StepArgs& a, bool want_acc, bool accumulate, cudaStream_t s);
+// The reference kernel-level integrator (kernelNbody_integTime semantics).
+cudaError_t launch_integ_time(const double* acc, double* pos_t, double* vel_t, const double* pos,
+                              const double* vel, double dt, int istep, double* acc0, int64_t n,
+                              const FieldConsts& f, cudaStream_t s);
+// FP64 conservation sums over bodies (ghosts have zero mass and contribute
+// nothing to the sums; they sit at the origin with zero velocity).
+cudaError_t launch_conservation(const double* pos, const double* vel, const double* mass,
+                                const double* phi, int64_t n, double* block_out, int nblocks,
+                                double* out16, cudaStream_t s);
+int conservation_blocks(int64_t n);
+
+}  // namespace khrr

@@ -1,0 +1,127 @@
+// Host-side context of libkhrr (the object behind the opaque khrr_ctx*).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <map>
+#include <string>
+#include <tuple>
+#include <utility>
+#include <vector>
+
+#include "khrr.h"
+#include "khrr_internal.h"
+
+namespace khrr {
+
+// Grow-only device allocation.
+template <class T>
+struct DevBuf {
+    T* p = nullptr;
+    size_t n = 0;
+    DevBuf() = default;
+    DevBuf(const DevBuf&) = delete;
+    DevBuf& operator=(const DevBuf&) = delete;
+    ~DevBuf() { release(); }
+    cudaError_t ensure(size_t count) {
+        if (count <= n && p) return cudaSuccess;
+        release();
+        cudaError_t e = cudaMalloc(reinterpret_cast<void**>(&p), (count ? count : 1) * sizeof(T));
+        if (e != cudaSuccess) {
+            p = nullptr;
+            n = 0;
+            return e;
+        }
+        n = count;
+        return cudaSuccess;
+    }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+};
+
+// The force-pass work queue for one layout of systems and one kernel shape.
+struct ForcePlan {
+    bool valid = false;
+    int threads = 0, ipt = 0, jt = 0, split_req = -1, ctas = 0;
+    std::vector<WorkItem> items;
+    std::vector<int> sys_item_begin;  // plain plans: items of system k
+    std::vector<int> sys_split;       // j chunks per system
+    int nslots = 1;
+    DevBuf<WorkItem> d_items;
+    DevBuf<unsigned char> d_nsplit;
+    ForcePlan() = default;
+    ForcePlan(const ForcePlan&) = delete;
+    ForcePlan& operator=(const ForcePlan&) = delete;
+};
+
+void plan_force_items(const std::vector<int64_t>& poff, const std::vector<int64_t>& cnt, int itile,
+                      int jt, int ctas, int forced_split, bool plain, ForcePlan& out);
+
+struct StepGraph {
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    cudaGraphNode_t ev0 = nullptr, ev1 = nullptr;  // event-record nodes around the force pass
+};
+
+}  // namespace khrr
+
+struct khrr_ctx {
+    int device = 0;
+    int sm_count = 0;
+    cudaStream_t own = nullptr, stream = nullptr;
+    std::string err;
+
+    // State layout.
+    bool has_state = false;
+    int64_t n = 0, npad = 0;
+    std::vector<int64_t> off, poff, cnt;  // real offsets, padded offsets, counts per system
+    khrr::DevBuf<double> pos, vel, acc, post, velt, acct, mass, eps2, phi;
+    khrr::DevBuf<float4> body;
+    khrr::DevBuf<float> hsoft;
+    khrr::DevBuf<double4> part;
+    khrr::DevBuf<unsigned> queue, errflag;
+    khrr::DevBuf<double> cons_blocks, scratch;
+    bool uniform = false;
+    float h_uniform = 0.0f;
+    khrr::FieldConsts field{};
+    khrr_tuning tuning{128, 8, 128, 0};
+    khrr::ForcePlan plan_batched, plan_plain;
+    bool predicted = false;
+    double pred_dt = 0.0;
+    std::map<std::tuple<uint64_t, bool, bool, bool>, khrr::StepGraph> graphs;
+
+    // Kernel-level entry points: their own shadow, partials and plan.
+    khrr::DevBuf<float4> kbody, kibody;
+    khrr::DevBuf<float> khsoft, kihsoft;
+    khrr::DevBuf<double4> kpart;
+    khrr::ForcePlan kplan;
+    int64_t kplan_n = -1;
+
+    // Timing.
+    bool timing = false;
+    cudaEvent_t ph0 = nullptr, ph1 = nullptr;  // placeholders captured in graphs
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev_pool;
+    size_t ev_used = 0;
+    int64_t timed_launches = 0;
+    double timed_pairs = 0.0;
+    std::map<const void*, int> occupancy;
+
+    khrr_status fail(khrr_status s, const char* fmt, ...);
+    khrr_status cuda(cudaError_t e, const char* what);
+    khrr_status check_device_flag();
+    int resident_ctas(const khrr::ForceVariant* v);
+    const khrr::ForceVariant* variant(bool unif, bool acc, bool phi) const;
+    khrr_status ensure_plan(bool plain);
+    void drop_graphs();
+    khrr::ForceArgs force_args(const khrr::ForcePlan& p, int item_begin, int item_end);
+    khrr_status enqueue_force(bool plain, bool acc, bool phi, bool events);
+    khrr::StepArgs step_args(const khrr::ForcePlan& p, double dt);
+    khrr_status enqueue_step(double dt, bool plain, bool phi_now, bool compat);
+    khrr_status get_step_graph(double dt, bool plain, bool phi_now, bool compat, khrr::StepGraph** out);
+    khrr_status timing_pair(cudaEvent_t* e0, cudaEvent_t* e1);
+    double pairs_per_pass() const;
+};

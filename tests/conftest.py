@@ -18,6 +18,18 @@ def pytest_configure(config):
 
 
 @pytest.fixture(scope="session")
+def libkhrr():
+    """The in-tree libkhrr.so, built with its Makefile if it is missing."""
+    import ctypes
+    import subprocess
+    so = PKG / "build" / "libkhrr.so"
+    if not so.exists():
+        r = subprocess.run(["make", "-C", str(PKG)], capture_output=True, text=True)
+        assert r.returncode == 0, r.stdout + r.stderr
+    return ctypes.CDLL(str(so))
+
+
+@pytest.fixture(scope="session")
 def oracle():
     from pyoracle import Oracle
     return Oracle()

@@ -1,0 +1,269 @@
+"""GPU parity of the force, potential and integrator path against the oracle.
+
+Every call goes through the C ABI (libkhrr.so).  Tolerances:
+  * accelerations: relative RMS <= 1e-6 vs the FP64 oracle (the precision
+    target) and <= 1e-5 vs the reference's own FP32 kernel;
+  * potentials: relative RMS <= 1e-6 vs FP64;
+  * FP64 integrator: bit-exact vs the oracle without the external field,
+    <= 1e-13 relative with it (atan/log may differ by an ulp between libms);
+  * trajectories: max |dx| <= 1e-7 after 10 steps, <= 1e-4 after 100 steps,
+    and the energy drift within 10% (+2e-7) of the FP64 oracle run's.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def rel_rms(a, b):
+    a = np.asarray(a, np.float64).reshape(-1)
+    b = np.asarray(b, np.float64).reshape(-1)
+    return float(np.sqrt(np.sum((a - b) ** 2) / np.sum(b ** 2)))
+
+
+@pytest.fixture(scope="module")
+def torch_cuda():
+    torch = pytest.importorskip("torch")
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    return torch
+
+
+@pytest.fixture(scope="module")
+def ctx(libkhrr, torch_cuda):
+    import khrr
+    c = khrr.Context(0)
+    yield c
+    c.close()
+
+
+def dev(torch, a):
+    return torch.as_tensor(np.ascontiguousarray(a, np.float64), device="cuda")
+
+
+def galaxy(ns, nd, seed, eps_s=0.004, eps_d=0.004):
+    from khrr.galaxy import make_galaxy
+    pos, vel, mass, eps = make_galaxy(ns, nd, seed, eps_stars=eps_s, eps_dm=eps_d).arrays()
+    return pos, vel, mass, eps * eps
+
+
+def kernel_accel(ctx, torch, pos, mass, eps2, acc0=None, pos_i=None, flags=None):
+    import khrr
+    n = len(mass)
+    P, M, E = dev(torch, pos), dev(torch, mass), dev(torch, eps2)
+    Pi = dev(torch, pos_i) if pos_i is not None else P
+    A = dev(torch, acc0) if acc0 is not None else torch.zeros((n, 3), dtype=torch.float64, device="cuda")
+    torch.cuda.synchronize()
+    ctx.accel(A.data_ptr(), Pi.data_ptr(), P.data_ptr(), M.data_ptr(), E.data_ptr(), n,
+              (khrr.OVERWRITE if acc0 is None else 0) if flags is None else flags)
+    ctx.synchronize()
+    return A.cpu().numpy()
+
+
+def test_accel_matches_fp64_and_reference_fp32(ctx, torch_cuda, golden):
+    g = golden("forces_n1536.npz")
+    a = kernel_accel(ctx, torch_cuda, g["pos"], g["mass"], g["eps2"])
+    assert rel_rms(a, g["acc_f64"]) <= 1e-6
+    assert rel_rms(a, g["acc_f32"]) <= 1e-5
+
+
+def test_accel_accumulates_like_the_reference(ctx, torch_cuda, golden):
+    g = golden("forces_n1536.npz")
+    base = np.full((len(g["mass"]), 3), 0.25)
+    a = kernel_accel(ctx, torch_cuda, g["pos"], g["mass"], g["eps2"], acc0=base)
+    assert rel_rms(a - base, g["acc_f64"]) <= 1e-6
+
+
+def test_phi_matches_fp64(ctx, torch_cuda, golden):
+    import khrr
+    torch = torch_cuda
+    g = golden("forces_n1536.npz")
+    n = len(g["mass"])
+    P, M, E = dev(torch, g["pos"]), dev(torch, g["mass"]), dev(torch, g["eps2"])
+    F = torch.full((n,), 2.0, dtype=torch.float64, device="cuda")
+    torch.cuda.synchronize()
+    ctx.phi(F.data_ptr(), P.data_ptr(), P.data_ptr(), M.data_ptr(), E.data_ptr(), n, 0)
+    ctx.synchronize()
+    assert rel_rms(F.cpu().numpy() - 2.0, g["phi"]) <= 1e-6
+    ctx.phi(F.data_ptr(), P.data_ptr(), P.data_ptr(), M.data_ptr(), E.data_ptr(), n, khrr.OVERWRITE)
+    ctx.synchronize()
+    assert rel_rms(F.cpu().numpy(), g["phi"]) <= 1e-6
+
+
+@pytest.mark.parametrize("n_s,n_d", [(300, 700), (1, 0), (5, 122), (4096, 8192)])
+def test_accel_ragged_sizes(ctx, torch_cuda, oracle, n_s, n_d):
+    pos, vel, mass, eps2 = galaxy(max(n_s, 1), n_d, seed=3)
+    a = kernel_accel(ctx, torch_cuda, pos, mass, eps2)
+    ref = oracle.accel_f64(pos, mass, eps2)
+    if len(mass) == 1:
+        assert np.all(a == 0.0)
+    else:
+        assert rel_rms(a, ref) <= 1e-6
+
+
+def test_accel_distinct_target_set(ctx, torch_cuda):
+    pos, vel, mass, eps2 = galaxy(256, 512, seed=4)
+    rng = np.random.default_rng(9)
+    pos_i = rng.uniform(-1, 1, pos.shape)
+    a = kernel_accel(ctx, torch_cuda, pos, mass, eps2, pos_i=pos_i)
+    d = pos[None, :, :] - pos_i[:, None, :]
+    r2 = (d ** 2).sum(-1) + 0.5 * (eps2[:, None] + eps2[None, :])
+    ref = (d * (mass[None, :] / r2 ** 1.5)[:, :, None]).sum(1)
+    assert rel_rms(a, ref) <= 1e-6
+
+
+@pytest.mark.parametrize("threads,ipt", [(128, 4), (128, 8), (256, 4), (256, 8)])
+@pytest.mark.parametrize("split", [0, 1, 3, 7])
+def test_every_kernel_shape_and_split(ctx, torch_cuda, golden, threads, ipt, split):
+    g = golden("forces_n1536.npz")
+    ctx.set_tuning(threads, ipt, 128, split)
+    try:
+        a = kernel_accel(ctx, torch_cuda, g["pos"], g["mass"], g["eps2"])
+    finally:
+        ctx.set_tuning(128, 8, 128, 0)
+    assert rel_rms(a, g["acc_f64"]) <= 1e-6
+
+
+def test_integ_time_matches_reference(ctx, torch_cuda, golden, oracle):
+    torch = torch_cuda
+    f = golden("forces_n1536.npz")
+    g = golden("integ_n1536.npz")
+    n = len(f["mass"])
+    acc = oracle.accel_f64(f["pos"], f["mass"], f["eps2"]).reshape(-1)
+    for with_field in (False, True):
+        if with_field:
+            ctx.set_external_field(Mh=1.0, Mb=0.5)
+        else:
+            ctx.set_external_field(enable=False)
+        A, P, V = dev(torch, acc), dev(torch, f["pos"].reshape(-1)), dev(torch, f["vel"].reshape(-1))
+        PT = torch.zeros(3 * n, dtype=torch.float64, device="cuda")
+        VT = torch.zeros_like(PT)
+        torch.cuda.synchronize()
+        ctx.integ_time(A.data_ptr(), PT.data_ptr(), VT.data_ptr(), P.data_ptr(), V.data_ptr(),
+                       0.002, 0, 0.0, A.data_ptr(), n)
+        ctx.synchronize()
+        F = oracle.field(Mh=1.0, Mb=0.5) if with_field else None
+        post, velt, a0 = np.zeros(3 * n), np.zeros(3 * n), acc.copy()
+        oracle.integ(F, acc, post, velt, f["pos"].reshape(-1).copy(), f["vel"].reshape(-1).copy(),
+                     0.002, 0, a0)
+        got_p, got_v = PT.cpu().numpy(), VT.cpu().numpy()
+        if with_field:
+            assert np.allclose(got_p, g["post"], rtol=1e-13, atol=0)
+            assert np.allclose(got_v, g["velt"], rtol=1e-13, atol=1e-15)
+        else:
+            assert np.array_equal(got_p, post) and np.array_equal(got_v, velt)
+        # corrector
+        acct = oracle.accel_f64(post, f["mass"], f["eps2"]).reshape(-1)
+        AT = dev(torch, acct)
+        P2, V2, A0 = dev(torch, f["pos"].reshape(-1)), dev(torch, f["vel"].reshape(-1)), dev(torch, acc)
+        torch.cuda.synchronize()
+        ctx.integ_time(AT.data_ptr(), P2.data_ptr(), V2.data_ptr(), PT.data_ptr(), VT.data_ptr(),
+                       0.002, 1, 0.002, A0.data_ptr(), n)
+        ctx.synchronize()
+        if with_field:
+            assert np.allclose(P2.cpu().numpy(), g["pos1"], rtol=1e-13, atol=0)
+            assert np.allclose(V2.cpu().numpy(), g["vel1"], rtol=1e-13, atol=1e-15)
+            assert np.array_equal(A0.cpu().numpy(), g["acc1"])
+    ctx.set_external_field(enable=False)
+
+
+def test_state_forces_and_potential(ctx, oracle):
+    import khrr
+    pos, vel, mass, eps2 = galaxy(1000, 2000, seed=5, eps_d=0.006)
+    ctx.upload(pos, vel, mass, eps2)
+    ctx.forces(khrr.ACC | khrr.PHI)
+    out = ctx.download()
+    assert rel_rms(out["acc"], oracle.accel_f64(pos, mass, eps2)) <= 1e-6
+    assert rel_rms(out["phi"], oracle.phi_f64(pos, mass, eps2)) <= 1e-6
+    assert np.array_equal(out["pos"], pos) and np.array_equal(out["vel"], vel)
+
+
+@pytest.mark.parametrize("label,flags", [("corrected", 0), ("literal", 4)])
+def test_ten_reference_steps(ctx, golden, label, flags):
+    import khrr
+    g = golden("steps_n1024.npz")
+    ctx.upload(g["pos"], g["vel"], g["mass"], g["eps2"])
+    ctx.forces(khrr.ACC)
+    ctx.step(float(g["dt"]), int(g["nsteps"]), flags)
+    out = ctx.download()
+    assert np.abs(out["pos"].reshape(-1) - g[label + "_pos"]).max() <= 1e-7
+    assert np.abs(out["vel"].reshape(-1) - g[label + "_vel"]).max() <= 1e-5
+    assert rel_rms(out["acc"], g[label + "_acc"]) <= 1e-5
+
+
+def test_hundred_steps_and_energy_drift(ctx, oracle):
+    import khrr
+    pos, vel, mass, eps2 = galaxy(1024, 2048, seed=6)
+    dt, nsteps = 0.002, 100
+    ctx.upload(pos, vel, mass, eps2)
+    ctx.forces(khrr.ACC | khrr.PHI)
+    e0 = ctx.conservation()
+    ctx.step(dt, nsteps, khrr.PHI)
+    e1 = ctx.conservation()
+    out = ctx.download()
+    p_or, v_or, _, _ = oracle.run_steps(pos, vel, mass, eps2, dt, nsteps)
+    assert np.abs(out["pos"] - p_or).max() <= 1e-4
+    phi0 = oracle.phi_f64(pos, mass, eps2)
+    phi1 = oracle.phi_f64(p_or, mass, eps2)
+    c0 = oracle.conservation(pos, vel, mass, phi0)
+    c1 = oracle.conservation(p_or, v_or, mass, phi1)
+    d_or = c1["E"] / c0["E"] - 1.0
+    d_gpu = e1["E"] / e0["E"] - 1.0
+    assert abs(d_gpu - d_or) <= 0.1 * abs(d_or) + 2e-7
+    assert abs(e0["E"] / c0["E"] - 1.0) <= 1e-6
+
+
+def test_batched_systems_match_separate_oracle(ctx, oracle):
+    import khrr
+    parts = [galaxy(200, 500, seed=7), galaxy(512, 1024, seed=8), galaxy(700, 1500, seed=9, eps_d=0.008)]
+    pos = np.concatenate([p[0] for p in parts])
+    vel = np.concatenate([p[1] for p in parts])
+    mass = np.concatenate([p[2] for p in parts])
+    eps2 = np.concatenate([p[3] for p in parts])
+    off = np.cumsum([0] + [len(p[2]) for p in parts])
+    ctx.upload(pos, vel, mass, eps2, offsets=off)
+    assert ctx.pair_count() == float(sum(len(p[2]) ** 2 for p in parts))
+    ctx.forces(khrr.ACC | khrr.PHI)
+    b = ctx.download()
+    ctx.forces(khrr.ACC | khrr.PHI | khrr.PLAIN)
+    p = ctx.download()
+    for k, (ps, vs, ms, es) in enumerate(parts):
+        s = slice(off[k], off[k + 1])
+        assert rel_rms(b["acc"][s], oracle.accel_f64(ps, ms, es)) <= 1e-6
+        assert rel_rms(b["phi"][s], oracle.phi_f64(ps, ms, es)) <= 1e-6
+        assert rel_rms(p["acc"][s], b["acc"][s]) <= 1e-6
+    # Batched and plain time steps agree.
+    ctx.upload(pos, vel, mass, eps2, offsets=off)
+    ctx.forces(khrr.ACC)
+    ctx.step(0.002, 5, 0)
+    sb = ctx.download()
+    ctx.upload(pos, vel, mass, eps2, offsets=off)
+    ctx.forces(khrr.ACC)
+    ctx.step(0.002, 5, khrr.PLAIN)
+    sp = ctx.download()
+    assert np.abs(sb["pos"] - sp["pos"]).max() <= 1e-8
+
+
+def test_conservation_matches_oracle(ctx, oracle):
+    import khrr
+    pos, vel, mass, eps2 = galaxy(600, 1200, seed=10)
+    ctx.upload(pos, vel, mass, eps2)
+    ctx.forces(khrr.ACC | khrr.PHI)
+    got = ctx.conservation()
+    phi = ctx.download()["phi"]
+    ref = oracle.conservation(pos, vel, mass, phi)
+    for k, v in ref.items():
+        assert got[k] == pytest.approx(v, rel=1e-12, abs=1e-14), k
+
+
+def test_timing_counts_force_launches(ctx):
+    import khrr
+    pos, vel, mass, eps2 = galaxy(1024, 2048, seed=11)
+    ctx.upload(pos, vel, mass, eps2)
+    ctx.enable_timing(True)
+    ctx.forces(khrr.ACC)
+    ctx.step(0.002, 3, 0)
+    ms, launches, pairs = ctx.force_timing()
+    ctx.enable_timing(False)
+    assert launches == 4 and ms > 0.0
+    assert pairs == 4 * float(len(mass)) ** 2
