@@ -304,6 +304,9 @@ def run_khrr(args):
     ms = ev0.elapsed_time(ev1)
     force_ms, launches, pairs_timed = ctx.force_timing()
     ctx.enable_timing(False)
+    tuning = ctx.get_tuning()
+    if launches < 1 or force_ms <= 0.0:
+        raise RuntimeError("force-kernel timing events recorded nothing")
     barrier()
     ms_max = ms
     if dist:
@@ -365,7 +368,7 @@ def run_khrr(args):
         "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32 pair terms (compensated sums), f64 integrator",
         "data": "synthetic (seeded disk-galaxy generator)",
-        "config": config(args, {"tuning": None}),
+        "config": config(args, {"tuning": tuning}),
         "pct_fp32_peak": 100.0 * achieved / peak_tflops,
         "acc_rel_rms_vs_fp64": err, "acc_rel_max_vs_fp64": err_max, "acc_err_targets": int(len(tg)),
         "roofline": {"bound": "fp32", "kernel": "force_kernel", "achieved": achieved, "peak": peak_tflops,

@@ -239,7 +239,10 @@ khrr_status khrr_ctx::enqueue_force(bool plain, bool acc, bool phi, bool events)
     if (st != KHRR_OK) return st;
     ForcePlan& p = plain ? plan_plain : plan_batched;
     const int ctas = resident_ctas(v);
-    if (events && (st = cuda(cudaEventRecord(ph0, stream), "event")) != KHRR_OK) return st;
+    // External records become event-record nodes when captured into a graph;
+    // khrr_step points them at fresh timing events before each replay.
+    if (events && (st = cuda(cudaEventRecordWithFlags(ph0, stream, cudaEventRecordExternal), "event")) != KHRR_OK)
+        return st;
     const size_t nsys = plain ? cnt.size() : 1;
     for (size_t k = 0; k < nsys; ++k) {
         const int b = plain ? p.sys_item_begin[k] : 0;
@@ -251,7 +254,8 @@ khrr_status khrr_ctx::enqueue_force(bool plain, bool acc, bool phi, bool events)
         if ((st = cuda(launch_force(v, force_args(p, b, e), grid, stream), "force kernel")) != KHRR_OK)
             return st;
     }
-    if (events && (st = cuda(cudaEventRecord(ph1, stream), "event")) != KHRR_OK) return st;
+    if (events && (st = cuda(cudaEventRecordWithFlags(ph1, stream, cudaEventRecordExternal), "event")) != KHRR_OK)
+        return st;
     return KHRR_OK;
 }
 
@@ -686,12 +690,12 @@ khrr_status khrr_step(khrr_ctx* c, double dt, int nsteps, int flags) {
         const bool phi_now = phi_last && k == nsteps - 1;
         StepGraph* g = nullptr;
         if ((st = c->get_step_graph(dt, plain, phi_now, compat, &g)) != KHRR_OK) return st;
-        if (g->ev0 && g->ev1) {
-            cudaEvent_t e0 = c->ph0, e1 = c->ph1;
-            if (c->timing && (st = c->timing_pair(&e0, &e1)) != KHRR_OK) return st;
-            cudaGraphExecEventRecordNodeSetEvent(g->exec, g->ev0, e0);
-            cudaGraphExecEventRecordNodeSetEvent(g->exec, g->ev1, e1);
-        }
+        if (!g->ev0 || !g->ev1) return c->fail(KHRR_ERR_CUDA, "step graph lacks its timing event nodes");
+        cudaEvent_t e0 = c->ph0, e1 = c->ph1;
+        if (c->timing && (st = c->timing_pair(&e0, &e1)) != KHRR_OK) return st;
+        if ((st = c->cuda(cudaGraphExecEventRecordNodeSetEvent(g->exec, g->ev0, e0), "graph event")) != KHRR_OK ||
+            (st = c->cuda(cudaGraphExecEventRecordNodeSetEvent(g->exec, g->ev1, e1), "graph event")) != KHRR_OK)
+            return st;
         if ((st = c->cuda(cudaGraphLaunch(g->exec, s), "graph launch")) != KHRR_OK) return st;
         if (c->timing) {
             c->timed_launches += plain ? static_cast<int64_t>(c->cnt.size()) : 1;

@@ -108,7 +108,12 @@ def _f64(a, shape_last=None):
 
 
 def _ptr(a):
-    return a.ctypes.data_as(C.c_void_p) if a is not None else None
+    """numpy array -> its data pointer; raw integer addresses pass through."""
+    if a is None:
+        return None
+    if isinstance(a, int):
+        return C.c_void_p(a)
+    return a.ctypes.data_as(C.c_void_p)
 
 
 class Context:
