@@ -42,7 +42,8 @@ typedef enum khrr_status {
     KHRR_ERR_TIMEOUT = 5,      /* a bounded device wait gave up              */
     KHRR_ERR_STATE = 6,        /* call out of order (e.g. step before upload)*/
     KHRR_ERR_OOM = 7,          /* device allocation failed                   */
-    KHRR_ERR_UNSUPPORTED = 8   /* no device / wrong architecture             */
+    KHRR_ERR_UNSUPPORTED = 8,  /* no device / wrong architecture             */
+    KHRR_ERR_TOO_LARGE = 9     /* n exceeds the fixed scratch of khrr_accel_noalloc */
 } khrr_status;
 
 typedef struct khrr_ctx khrr_ctx;
@@ -112,6 +113,31 @@ khrr_status khrr_phi(khrr_ctx* ctx, double* phi, const double* pos_i, const doub
 khrr_status khrr_integ_time(khrr_ctx* ctx, const double* acc, double* pos_t, double* vel_t,
                             const double* pos, const double* vel, double dt, int istep,
                             double t, double* acc0, int64_t n);
+
+/* Largest n khrr_accel_noalloc accepts. */
+#define KHRR_NOALLOC_MAX_BODIES 32768
+/* khrr_accel without any device allocation.  This entry point has no
+ * counterpart in the reference.  It exists for callers that cannot allocate
+ * device memory on their call path: a host program that fixes its device
+ * memory budget at start-up (cudaMalloc can synchronize the device and can
+ * fail under memory pressure mid-run), or a plugin host that only hands out
+ * device pointers it already owns.  It needs no context: the caller passes
+ * the inputs, the output and a stream (cudaStream_t, NULL = legacy default).
+ * Same arguments and semantics as khrr_accel (acc += sum, or acc = sum with
+ * KHRR_OVERWRITE), for 1 <= n <= KHRR_NOALLOC_MAX_BODIES; larger n returns
+ * KHRR_ERR_TOO_LARGE before any device work.
+ * Scratch: one file-scope device array of about 9.3 MiB (shadow positions,
+ * work items, partial sums, a queue counter), which every GPU that loads the
+ * library holds until the process exits.  The first call on a device looks up
+ * that array's device address (with the device current) and sets the kernel's
+ * attributes, so make the first call before any stream capture.  All calls
+ * share the array and the counter is cleared on every call, so calls whose
+ * GPU work overlaps (on different streams or host threads) race: serialize
+ * them on one stream.  The call only enqueues work; it returns without
+ * synchronizing. */
+khrr_status khrr_accel_noalloc(double* acc, const double* pos_i, const double* pos_j,
+                               const double* mass_j, const double* eps2_j, int64_t n,
+                               int flags, void* stream);
 
 /* ---- simulation-level API (context-owned device state) ------------------ */
 /* External field for all later integration; NULL disables it. */

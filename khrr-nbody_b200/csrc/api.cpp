@@ -393,6 +393,7 @@ const char* khrr_status_name(khrr_status s) {
         case KHRR_ERR_STATE: return "KHRR_ERR_STATE";
         case KHRR_ERR_OOM: return "KHRR_ERR_OOM";
         case KHRR_ERR_UNSUPPORTED: return "KHRR_ERR_UNSUPPORTED";
+        case KHRR_ERR_TOO_LARGE: return "KHRR_ERR_TOO_LARGE";
     }
     return "KHRR_ERR_UNKNOWN";
 }

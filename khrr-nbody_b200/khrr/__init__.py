@@ -24,7 +24,7 @@ OVERWRITE = 16
 
 STATUS = {0: "KHRR_OK", 1: "KHRR_ERR_INVALID_ARG", 2: "KHRR_ERR_NOT_MULTIPLE", 3: "KHRR_ERR_CUDA",
           4: "KHRR_ERR_IO", 5: "KHRR_ERR_TIMEOUT", 6: "KHRR_ERR_STATE", 7: "KHRR_ERR_OOM",
-          8: "KHRR_ERR_UNSUPPORTED"}
+          8: "KHRR_ERR_UNSUPPORTED", 9: "KHRR_ERR_TOO_LARGE"}
 
 
 class KhrrError(RuntimeError):
