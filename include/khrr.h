@@ -75,12 +75,15 @@ typedef struct khrr_lie {
 } khrr_lie;
 
 /* Force-kernel shape: threads per CTA, i bodies per thread, j-tile size,
- * and j_split = number of j chunks per system (0 = chosen automatically). */
+ * j_split = number of j chunks per system (0 = chosen automatically), and
+ * packed = 1 for the packed-FP32 (f32x2, two j bodies per instruction) inner
+ * loop, 0 for the scalar one. */
 typedef struct khrr_tuning {
     int threads;
     int i_per_thread;
     int j_tile;
     int j_split;
+    int packed;
 } khrr_tuning;
 
 /* ---- library / context ---------------------------------------------------- */

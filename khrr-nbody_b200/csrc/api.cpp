@@ -7,8 +7,8 @@
 // reference's layout, so uploads and downloads are straight copies): pos,
 // vel, acc (a(t) without the external field), post/velt (predicted), acct
 // (force workspace of the literal reference loop), mass, eps2, phi.  The force
-// kernel reads the FP32 shadow body[] = (x, y, z, m) and hsoft[] = eps2 / 2,
-// and writes FP64 partials part[slot][body].
+// kernel reads the FP32 structure-of-arrays shadow (x, y, z, m, eps2 / 2) and
+// writes FP64 partials part[slot][body].
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -77,7 +77,8 @@ int khrr_ctx::resident_ctas(const ForceVariant* v) {
 }
 
 const ForceVariant* khrr_ctx::variant(bool unif, bool acc, bool phi) const {
-    return find_force_variant(tuning.threads, tuning.i_per_thread, tuning.j_tile, unif, acc, phi);
+    return find_force_variant(tuning.threads, tuning.i_per_thread, tuning.j_tile, tuning.packed != 0, unif, acc,
+                              phi);
 }
 
 // ---------------------------------------------------------------------------
@@ -150,6 +151,7 @@ void plan_force_items(const std::vector<int64_t>& poff, const std::vector<int64_
                 w.j_end = static_cast<int>(poff[k] + static_cast<int64_t>(c + 1) * tiles / s * jt);
                 w.slot = c;
                 w.sys = static_cast<int>(k);
+                w.pad0 = static_cast<int>(std::min<int64_t>(itile, cnt[k] - ib));  // i bodies in the tile
                 out.items.push_back(w);
             }
         }
@@ -157,8 +159,8 @@ void plan_force_items(const std::vector<int64_t>& poff, const std::vector<int64_
     out.sys_item_begin[nsys] = static_cast<int>(out.items.size());
     if (!plain && nsys > 1) {
         std::stable_sort(out.items.begin(), out.items.end(), [](const WorkItem& a, const WorkItem& b) {
-            const int64_t ca = static_cast<int64_t>(std::min(a.i_end - a.i_begin, 1 << 30)) * (a.j_end - a.j_begin);
-            const int64_t cb = static_cast<int64_t>(std::min(b.i_end - b.i_begin, 1 << 30)) * (b.j_end - b.j_begin);
+            const int64_t ca = static_cast<int64_t>(a.pad0) * (a.j_end - a.j_begin);
+            const int64_t cb = static_cast<int64_t>(b.pad0) * (b.j_end - b.j_begin);
             return ca > cb;
         });
     }
@@ -218,10 +220,8 @@ void khrr_ctx::drop_graphs() {
 // ---------------------------------------------------------------------------
 ForceArgs khrr_ctx::force_args(const ForcePlan& p, int item_begin, int item_end) {
     ForceArgs a{};
-    a.body = body.p;
-    a.hsoft = hsoft.p;
-    a.ibody = body.p;
-    a.ihsoft = hsoft.p;
+    a.j = shadow();
+    a.i = a.j;
     a.items = p.d_items.p + item_begin;
     a.n_items = item_end - item_begin;
     a.queue = queue.p;
@@ -269,7 +269,7 @@ StepArgs khrr_ctx::step_args(const ForcePlan& p, double dt) {
     a.acct = acct.p;
     a.mass = mass.p;
     a.phi = phi.p;
-    a.body = body.p;
+    a.shadow = shadow();
     a.part = part.p;
     a.npad = npad;
     a.nsplit = p.d_nsplit.p;
@@ -300,7 +300,12 @@ khrr_status khrr_ctx::enqueue_step(double dt, bool plain, bool phi_now, bool com
         s.acct += 3 * o;
         s.mass += o;
         s.phi += o;
-        s.body += o;
+        s.shadow = shadow_at(shadow_buf.p, npad);
+        s.shadow.x += o;
+        s.shadow.y += o;
+        s.shadow.z += o;
+        s.shadow.m += o;
+        s.shadow.h += o;
         s.part += o;
         s.nsplit += o;
         s.n = round_up(cnt[k], kPad);
@@ -533,8 +538,7 @@ khrr_status khrr_upload_state(khrr_ctx* c, int64_t n, const double* pos, const d
         if ((st = c->cuda(b->ensure(3 * np), "alloc state")) != KHRR_OK) return st;
     for (DevBuf<double>* b : {&c->mass, &c->eps2, &c->phi})
         if ((st = c->cuda(b->ensure(np), "alloc state")) != KHRR_OK) return st;
-    if ((st = c->cuda(c->body.ensure(np), "alloc shadow")) != KHRR_OK) return st;
-    if ((st = c->cuda(c->hsoft.ensure(np), "alloc shadow")) != KHRR_OK) return st;
+    if ((st = c->cuda(c->shadow_buf.ensure(5 * np), "alloc shadow")) != KHRR_OK) return st;
     cudaStream_t s = c->stream;
     for (DevBuf<double>* b : {&c->pos, &c->vel, &c->acc, &c->post, &c->velt, &c->acct})
         cudaMemsetAsync(b->p, 0, 3 * np * sizeof(double), s);
@@ -558,7 +562,7 @@ khrr_status khrr_upload_state(khrr_ctx* c, int64_t n, const double* pos, const d
             st = c->cuda(cudaMemcpyAsync(c->mass.p + q, mass + o, m * sizeof(double), cudaMemcpyHostToDevice, s), "upload");
     }
     if (st != KHRR_OK) return st;
-    if ((st = c->cuda(launch_pack(c->pos.p, c->mass.p, c->eps2.p, c->npad, c->npad, c->body.p, c->hsoft.p, s),
+    if ((st = c->cuda(launch_pack(c->pos.p, c->mass.p, c->eps2.p, c->npad, c->npad, c->shadow(), s),
                       "pack")) != KHRR_OK)
         return st;
     if ((st = c->cuda(cudaStreamSynchronize(s), "upload sync")) != KHRR_OK) return st;
@@ -651,7 +655,7 @@ khrr_status khrr_forces(khrr_ctx* c, int flags) {
     cudaStream_t s = c->stream;
     khrr_status st;
     // Shadow of the current positions (a previous step leaves the predicted ones).
-    if ((st = c->cuda(launch_pack(c->pos.p, c->mass.p, c->eps2.p, c->npad, c->npad, c->body.p, c->hsoft.p, s),
+    if ((st = c->cuda(launch_pack(c->pos.p, c->mass.p, c->eps2.p, c->npad, c->npad, c->shadow(), s),
                       "pack")) != KHRR_OK)
         return st;
     cudaEvent_t e0 = nullptr, e1 = nullptr;
@@ -742,9 +746,10 @@ khrr_status khrr_set_tuning(khrr_ctx* c, const khrr_tuning* t) {
     if (!c || !t) return KHRR_ERR_INVALID_ARG;
     khrr_tuning n = *t;
     if (n.j_tile == 0) n.j_tile = 128;
-    if (!find_force_variant(n.threads, n.i_per_thread, n.j_tile, false, true, false))
-        return c->fail(KHRR_ERR_INVALID_ARG, "no compiled force kernel with threads=%d i_per_thread=%d j_tile=%d",
-                       n.threads, n.i_per_thread, n.j_tile);
+    if (!find_force_variant(n.threads, n.i_per_thread, n.j_tile, n.packed != 0, false, true, false))
+        return c->fail(KHRR_ERR_INVALID_ARG,
+                       "no compiled force kernel with threads=%d i_per_thread=%d j_tile=%d packed=%d", n.threads,
+                       n.i_per_thread, n.j_tile, n.packed);
     if (n.j_split < 0 || n.j_split > 255) return c->fail(KHRR_ERR_INVALID_ARG, "j_split must be in [0, 255]");
     c->tuning = n;
     c->plan_batched.valid = false;

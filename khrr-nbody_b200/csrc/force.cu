@@ -8,17 +8,23 @@
 // its FP64 partial sums to slot `slot` of a [slot][body] buffer; the
 // integrator (or khrr_accel's reduce) sums the slots in FP64.
 //
-// Per item.  Each of the NT threads holds K i bodies (x, y, z, eps term) in
-// registers.  The item's j bodies (FP32 SoA-of-float4 shadow x, y, z, m plus
-// 0.5*eps^2) stream through a STAGES-deep ring of shared-memory tiles filled
-// by cp.async.bulk (TMA bulk copies, no multicast) that complete on
-// mbarriers; one elected thread issues the copies.  Every j in a tile is a
-// broadcast shared-memory read reused for K interactions.
+// Per item.  Each of the NT threads holds K i bodies in registers.  The item's
+// j bodies (FP32 SoA shadow: x, y, z, m and h = eps^2/2) stream through a
+// STAGES-deep ring of shared-memory tiles filled by cp.async.bulk (TMA bulk
+// copies, no multicast) completing on mbarriers; one elected thread issues
+// the copies.  A 16-byte shared load brings four consecutive j values of one
+// component, reused for all K i bodies.
 //
-// Arithmetic per pair: 3 FADD (d), [1 FADD eps term], 3 FFMA (r^2),
-// MUFU.RSQ (rsqrt.approx.ftz), 3 FMUL (m r^-3), 3 FFMA (accumulate), and one
-// FADD for the potential when requested.  The self pair (j = i) contributes
+// Inner loop (PACKED, the sm_100 form): the packed FP32 instructions
+// (add/mul/fma .f32x2) evaluate two j bodies against one i body per
+// instruction, so a pair costs 6 issue slots of FP32 work (+0.5 for distinct
+// softenings) plus one MUFU.RSQ, and the FP32 datapath, not instruction issue,
+// bounds the kernel.  The scalar form (one pair per instruction) is kept as a
+// tuning alternative.  Per pair: d = x_j - x_i (3 add), r^2 = h_i + h_j + d.d
+// (1 add + 3 fma), rsqrt.approx.ftz (MUFU), m r^-3 (3 mul), acc += d m r^-3
+// (3 fma), and one add for the potential.  The self pair (j = i) contributes
 // zero to the acceleration and m/eps to the potential, as in the reference.
+//
 // Accuracy: tile partials (JT terms, FP32) are folded into per-thread
 // compensated running sums (two-sum, hi + lo) held in shared memory, so the
 // long sum over j stays at FP32-rounding level per tile.
@@ -106,28 +112,62 @@ __device__ __forceinline__ void two_sum_into(float& hi, float& lo, float p) {
     lo += e;
 }
 
+__device__ __forceinline__ float2 f2(float a, float b) { return make_float2(a, b); }
+
 constexpr int kBarBytes = 128;  // mbarriers live in the first 128 bytes
 
 template <int NT, int K, int JT, int STAGES, bool UNIF, bool ACC, bool PHI>
 struct ForceShape {
     static constexpr int NC = (ACC ? 3 : 0) + (PHI ? 1 : 0);
-    static constexpr unsigned kTileBytes = JT * 16u + (UNIF ? 0u : JT * 4u);
-    static constexpr size_t kSmem = kBarBytes + (size_t)STAGES * JT * 16 +
-                                    (UNIF ? 0 : (size_t)STAGES * JT * 4) + (size_t)K * NC * 2 * NT * 4;
+    static constexpr int NCOMP = UNIF ? 4 : 5;  // shadow arrays copied per tile
+    static constexpr unsigned kTileBytes = NCOMP * JT * 4u;
+    static constexpr size_t kSmem = kBarBytes + (size_t)STAGES * kTileBytes + (size_t)K * NC * 2 * NT * 4;
 };
 
-template <int NT, int K, int JT, int STAGES, bool UNIF, bool ACC, bool PHI>
+// Per-thread accumulators of one tile for K i bodies.  The packed form keeps
+// (even j, odd j) partials in the two lanes of a float2.
+template <int K, bool PACKED>
+struct TileAcc;
+
+template <int K>
+struct TileAcc<K, true> {
+    float2 ax[K], ay[K], az[K], pp[K];
+    __device__ __forceinline__ void zero() {
+#pragma unroll
+        for (int k = 0; k < K; ++k) ax[k] = ay[k] = az[k] = pp[k] = f2(0.f, 0.f);
+    }
+    __device__ __forceinline__ float x(int k) const { return ax[k].x + ax[k].y; }
+    __device__ __forceinline__ float y(int k) const { return ay[k].x + ay[k].y; }
+    __device__ __forceinline__ float z(int k) const { return az[k].x + az[k].y; }
+    __device__ __forceinline__ float p(int k) const { return pp[k].x + pp[k].y; }
+};
+
+template <int K>
+struct TileAcc<K, false> {
+    float ax[K], ay[K], az[K], pp[K];
+    __device__ __forceinline__ void zero() {
+#pragma unroll
+        for (int k = 0; k < K; ++k) ax[k] = ay[k] = az[k] = pp[k] = 0.f;
+    }
+    __device__ __forceinline__ float x(int k) const { return ax[k]; }
+    __device__ __forceinline__ float y(int k) const { return ay[k]; }
+    __device__ __forceinline__ float z(int k) const { return az[k]; }
+    __device__ __forceinline__ float p(int k) const { return pp[k]; }
+};
+
+template <int NT, int K, int JT, int STAGES, bool UNIF, bool ACC, bool PHI, bool PACKED>
 __global__ void __launch_bounds__(NT) force_kernel(const ForceArgs a) {
     using S = ForceShape<NT, K, JT, STAGES, UNIF, ACC, PHI>;
     constexpr int NC = S::NC;
+    constexpr int NCOMP = S::NCOMP;
     static_assert(NC > 0, "nothing to accumulate");
     static_assert(STAGES >= 2 && STAGES * 8 <= kBarBytes, "bad stage count");
+    static_assert(JT % 4 == 0, "j tile must be a multiple of 4");
 
     extern __shared__ __align__(128) unsigned char smem_raw[];
     uint64_t* full = reinterpret_cast<uint64_t*>(smem_raw);
-    float4* sbody = reinterpret_cast<float4*>(smem_raw + kBarBytes);
-    float* sh = reinterpret_cast<float*>(sbody + STAGES * JT);
-    float* run = sh + (UNIF ? 0 : STAGES * JT);  // [K][NC][hi|lo][NT]
+    float* ring = reinterpret_cast<float*>(smem_raw + kBarBytes);  // [STAGES][NCOMP][JT]
+    float* run = ring + STAGES * NCOMP * JT;                        // [K][NC][hi|lo][NT]
     __shared__ int s_item;
 
     const int tid = threadIdx.x;
@@ -139,9 +179,13 @@ __global__ void __launch_bounds__(NT) force_kernel(const ForceArgs a) {
     __syncthreads();
 
     auto issue = [&](int stage, int jstart) {  // elected thread only
+        float* dst = ring + stage * NCOMP * JT;
         mbar_arrive_expect_tx(&full[stage], S::kTileBytes);
-        bulk_copy_g2s(sbody + stage * JT, a.body + jstart, JT * 16u, &full[stage]);
-        if (!UNIF) bulk_copy_g2s(sh + stage * JT, a.hsoft + jstart, JT * 4u, &full[stage]);
+        bulk_copy_g2s(dst, a.j.x + jstart, JT * 4u, &full[stage]);
+        bulk_copy_g2s(dst + JT, a.j.y + jstart, JT * 4u, &full[stage]);
+        bulk_copy_g2s(dst + 2 * JT, a.j.z + jstart, JT * 4u, &full[stage]);
+        bulk_copy_g2s(dst + 3 * JT, a.j.m + jstart, JT * 4u, &full[stage]);
+        if (!UNIF) bulk_copy_g2s(dst + 4 * JT, a.j.h + jstart, JT * 4u, &full[stage]);
     };
 
     unsigned consumed = 0;  // tiles this CTA has consumed, over all its items
@@ -158,19 +202,20 @@ __global__ void __launch_bounds__(NT) force_kernel(const ForceArgs a) {
                 issue((consumed + s) % STAGES, w.j_begin + s * JT);
         }
 
-        float xi[K], yi[K], zi[K], hi[K];
+        // i bodies: negated coordinates (d = x_j + (-x_i) rounds like x_j - x_i)
+        // and the eps term, duplicated into both lanes for the packed form.
+        float nx[K], ny[K], nz[K], hh[K];
 #pragma unroll
         for (int k = 0; k < K; ++k) {
             const int i = w.i_begin + k * NT + tid;
             if (i < w.i_end) {
-                const float4 b = a.ibody[i];
-                xi[k] = b.x;
-                yi[k] = b.y;
-                zi[k] = b.z;
-                hi[k] = UNIF ? (a.h_uniform + a.h_uniform) : a.ihsoft[i];
+                nx[k] = -a.i.x[i];
+                ny[k] = -a.i.y[i];
+                nz[k] = -a.i.z[i];
+                hh[k] = UNIF ? (a.h_uniform + a.h_uniform) : a.i.h[i];
             } else {
-                xi[k] = yi[k] = zi[k] = 0.0f;
-                hi[k] = 1.0f;
+                nx[k] = ny[k] = nz[k] = 0.0f;
+                hh[k] = 1.0f;
             }
 #pragma unroll
             for (int c = 0; c < 2 * NC; ++c) run[((k * NC * 2) + c) * NT + tid] = 0.0f;
@@ -181,31 +226,69 @@ __global__ void __launch_bounds__(NT) force_kernel(const ForceArgs a) {
             const int stage = static_cast<int>(q % STAGES);
             const bool ok = mbar_wait_bounded(&full[stage], (q / STAGES) & 1u);
 
-            float px[K], py[K], pz[K], pp[K];
-#pragma unroll
-            for (int k = 0; k < K; ++k) px[k] = py[k] = pz[k] = pp[k] = 0.0f;
+            TileAcc<K, PACKED> acc;
+            acc.zero();
             if (ok) {
-                const float4* tb = sbody + stage * JT;
-                const float* th = sh + stage * JT;
-#pragma unroll 2
-                for (int j = 0; j < JT; ++j) {
-                    const float4 b = tb[j];
-                    const float hj = UNIF ? 0.0f : th[j];
+                const float4* tx = reinterpret_cast<const float4*>(ring + stage * NCOMP * JT);
+                const float4* ty = tx + JT / 4;
+                const float4* tz = tx + 2 * (JT / 4);
+                const float4* tm = tx + 3 * (JT / 4);
+                const float4* th = tx + 4 * (JT / 4);
+#pragma unroll 1
+                for (int q4 = 0; q4 < JT / 4; ++q4) {
+                    const float4 X = tx[q4], Y = ty[q4], Z = tz[q4], M = tm[q4];
+                    const float4 H = UNIF ? make_float4(0.f, 0.f, 0.f, 0.f) : th[q4];
+                    if constexpr (PACKED) {
 #pragma unroll
-                    for (int k = 0; k < K; ++k) {
-                        const float dx = b.x - xi[k];
-                        const float dy = b.y - yi[k];
-                        const float dz = b.z - zi[k];
-                        const float r2 = fmaf(dz, dz, fmaf(dy, dy, fmaf(dx, dx, UNIF ? hi[k] : hi[k] + hj)));
-                        const float inv = rsqrt_approx(r2);
-                        const float minv = b.w * inv;
-                        if (ACC) {
-                            const float f = minv * (inv * inv);
-                            px[k] = fmaf(dx, f, px[k]);
-                            py[k] = fmaf(dy, f, py[k]);
-                            pz[k] = fmaf(dz, f, pz[k]);
+                        for (int half = 0; half < 2; ++half) {
+                            const float2 xj = half ? f2(X.z, X.w) : f2(X.x, X.y);
+                            const float2 yj = half ? f2(Y.z, Y.w) : f2(Y.x, Y.y);
+                            const float2 zj = half ? f2(Z.z, Z.w) : f2(Z.x, Z.y);
+                            const float2 mj = half ? f2(M.z, M.w) : f2(M.x, M.y);
+                            const float2 hj = half ? f2(H.z, H.w) : f2(H.x, H.y);
+#pragma unroll
+                            for (int k = 0; k < K; ++k) {
+                                const float2 dx = __fadd2_rn(xj, f2(nx[k], nx[k]));
+                                const float2 dy = __fadd2_rn(yj, f2(ny[k], ny[k]));
+                                const float2 dz = __fadd2_rn(zj, f2(nz[k], nz[k]));
+                                float2 r2 = UNIF ? f2(hh[k], hh[k]) : __fadd2_rn(hj, f2(hh[k], hh[k]));
+                                r2 = __ffma2_rn(dx, dx, r2);
+                                r2 = __ffma2_rn(dy, dy, r2);
+                                r2 = __ffma2_rn(dz, dz, r2);
+                                const float2 inv = f2(rsqrt_approx(r2.x), rsqrt_approx(r2.y));
+                                const float2 minv = __fmul2_rn(mj, inv);
+                                if (ACC) {
+                                    const float2 f = __fmul2_rn(minv, __fmul2_rn(inv, inv));
+                                    acc.ax[k] = __ffma2_rn(dx, f, acc.ax[k]);
+                                    acc.ay[k] = __ffma2_rn(dy, f, acc.ay[k]);
+                                    acc.az[k] = __ffma2_rn(dz, f, acc.az[k]);
+                                }
+                                if (PHI) acc.pp[k] = __fadd2_rn(acc.pp[k], minv);
+                            }
                         }
-                        if (PHI) pp[k] += minv;
+                    } else {
+                        const float xs[4] = {X.x, X.y, X.z, X.w}, ys[4] = {Y.x, Y.y, Y.z, Y.w};
+                        const float zs[4] = {Z.x, Z.y, Z.z, Z.w}, ms[4] = {M.x, M.y, M.z, M.w};
+                        const float hs[4] = {H.x, H.y, H.z, H.w};
+#pragma unroll
+                        for (int u = 0; u < 4; ++u) {
+#pragma unroll
+                            for (int k = 0; k < K; ++k) {
+                                const float dx = xs[u] + nx[k];
+                                const float dy = ys[u] + ny[k];
+                                const float dz = zs[u] + nz[k];
+                                const float r2 = fmaf(dz, dz, fmaf(dy, dy, fmaf(dx, dx, UNIF ? hh[k] : hh[k] + hs[u])));
+                                const float inv = rsqrt_approx(r2);
+                                const float minv = ms[u] * inv;
+                                if (ACC) {
+                                    const float f = minv * (inv * inv);
+                                    acc.ax[k] = fmaf(dx, f, acc.ax[k]);
+                                    acc.ay[k] = fmaf(dy, f, acc.ay[k]);
+                                    acc.az[k] = fmaf(dz, f, acc.az[k]);
+                                }
+                                if (PHI) acc.pp[k] += minv;
+                            }
+                        }
                     }
                 }
             }
@@ -216,22 +299,22 @@ __global__ void __launch_bounds__(NT) force_kernel(const ForceArgs a) {
                 int c = 0;
                 if (ACC) {
                     float h0 = r[0], l0 = r[NT];
-                    two_sum_into(h0, l0, px[k]);
+                    two_sum_into(h0, l0, acc.x(k));
                     r[0] = h0;
                     r[NT] = l0;
                     float h1 = r[2 * NT], l1 = r[3 * NT];
-                    two_sum_into(h1, l1, py[k]);
+                    two_sum_into(h1, l1, acc.y(k));
                     r[2 * NT] = h1;
                     r[3 * NT] = l1;
                     float h2 = r[4 * NT], l2 = r[5 * NT];
-                    two_sum_into(h2, l2, pz[k]);
+                    two_sum_into(h2, l2, acc.z(k));
                     r[4 * NT] = h2;
                     r[5 * NT] = l2;
                     c = 3;
                 }
                 if (PHI) {
                     float h3 = r[(2 * c) * NT], l3 = r[(2 * c + 1) * NT];
-                    two_sum_into(h3, l3, pp[k]);
+                    two_sum_into(h3, l3, acc.p(k));
                     r[(2 * c) * NT] = h3;
                     r[(2 * c + 1) * NT] = l3;
                 }
@@ -277,32 +360,43 @@ __global__ void __launch_bounds__(NT) force_kernel(const ForceArgs a) {
     }
 }
 
-template <int NT, int K, int JT, int STAGES, bool UNIF, bool ACC, bool PHI>
+template <int NT, int K, bool PACKED, int JT, int STAGES, bool UNIF, bool ACC, bool PHI>
 ForceVariant make_variant() {
     using S = ForceShape<NT, K, JT, STAGES, UNIF, ACC, PHI>;
-    return ForceVariant{NT, K, JT, STAGES, UNIF, ACC, PHI,
-                        reinterpret_cast<const void*>(&force_kernel<NT, K, JT, STAGES, UNIF, ACC, PHI>),
+    return ForceVariant{NT,
+                        K,
+                        JT,
+                        STAGES,
+                        PACKED,
+                        UNIF,
+                        ACC,
+                        PHI,
+                        reinterpret_cast<const void*>(&force_kernel<NT, K, JT, STAGES, UNIF, ACC, PHI, PACKED>),
                         S::kSmem};
 }
 
-template <int NT, int K>
+template <int NT, int K, bool PACKED>
 void add_shape(ForceVariant* v, int& n) {
-    v[n++] = make_variant<NT, K, 128, 3, false, true, false>();
-    v[n++] = make_variant<NT, K, 128, 3, false, true, true>();
-    v[n++] = make_variant<NT, K, 128, 3, false, false, true>();
-    v[n++] = make_variant<NT, K, 128, 3, true, true, false>();
-    v[n++] = make_variant<NT, K, 128, 3, true, true, true>();
-    v[n++] = make_variant<NT, K, 128, 3, true, false, true>();
+    v[n++] = make_variant<NT, K, PACKED, 128, 3, false, true, false>();
+    v[n++] = make_variant<NT, K, PACKED, 128, 3, false, true, true>();
+    v[n++] = make_variant<NT, K, PACKED, 128, 3, false, false, true>();
+    v[n++] = make_variant<NT, K, PACKED, 128, 3, true, true, false>();
+    v[n++] = make_variant<NT, K, PACKED, 128, 3, true, true, true>();
+    v[n++] = make_variant<NT, K, PACKED, 128, 3, true, false, true>();
 }
 
 struct VariantTable {
-    ForceVariant v[32];
+    ForceVariant v[64];
     int n = 0;
     VariantTable() {
-        add_shape<128, 4>(v, n);
-        add_shape<128, 8>(v, n);
-        add_shape<256, 4>(v, n);
-        add_shape<256, 8>(v, n);
+        add_shape<128, 2, true>(v, n);
+        add_shape<128, 4, true>(v, n);
+        add_shape<256, 2, true>(v, n);
+        add_shape<256, 4, true>(v, n);
+        add_shape<128, 4, false>(v, n);
+        add_shape<128, 8, false>(v, n);
+        add_shape<256, 4, false>(v, n);
+        add_shape<256, 8, false>(v, n);
     }
 };
 
@@ -313,18 +407,21 @@ const VariantTable& table() {
 
 // ---- helpers around the force pass -----------------------------------------
 
+// FP64 AoS state -> SoA FP32 shadow; ghosts (i >= n) get zero mass at the
+// origin and body 0's softening term.
 __global__ void pack_kernel(const double* __restrict__ pos, const double* __restrict__ mass,
-                            const double* __restrict__ eps2, int64_t n, int64_t npad,
-                            float4* __restrict__ body, float* __restrict__ hsoft, float ghost_h) {
+                            const double* __restrict__ eps2, int64_t n, int64_t npad, Shadow sh) {
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < npad;
          i += (int64_t)gridDim.x * blockDim.x) {
         if (i < n) {
-            body[i] = make_float4(static_cast<float>(pos[3 * i]), static_cast<float>(pos[3 * i + 1]),
-                                  static_cast<float>(pos[3 * i + 2]), static_cast<float>(mass[i]));
-            hsoft[i] = static_cast<float>(0.5 * eps2[i]);
+            sh.x[i] = static_cast<float>(pos[3 * i]);
+            sh.y[i] = static_cast<float>(pos[3 * i + 1]);
+            sh.z[i] = static_cast<float>(pos[3 * i + 2]);
+            sh.m[i] = static_cast<float>(mass[i]);
+            sh.h[i] = static_cast<float>(0.5 * eps2[i]);
         } else {
-            body[i] = make_float4(0.f, 0.f, 0.f, 0.f);
-            hsoft[i] = ghost_h >= 0.0f ? ghost_h : static_cast<float>(0.5 * eps2[0]);
+            sh.x[i] = sh.y[i] = sh.z[i] = sh.m[i] = 0.0f;
+            sh.h[i] = static_cast<float>(0.5 * eps2[0]);
         }
     }
 }
@@ -428,12 +525,13 @@ const ForceVariant* force_variant(int idx) {
     return (idx >= 0 && idx < table().n) ? &table().v[idx] : nullptr;
 }
 
-const ForceVariant* find_force_variant(int threads, int ipt, int jt, bool unif, bool acc, bool phi) {
+const ForceVariant* find_force_variant(int threads, int ipt, int jt, bool packed, bool unif, bool acc,
+                                       bool phi) {
     const VariantTable& t = table();
     for (int i = 0; i < t.n; ++i) {
         const ForceVariant& v = t.v[i];
-        if (v.threads == threads && v.i_per_thread == ipt && v.j_tile == jt && v.uniform_eps == unif &&
-            v.acc == acc && v.phi == phi)
+        if (v.threads == threads && v.i_per_thread == ipt && v.j_tile == jt && v.packed == packed &&
+            v.uniform_eps == unif && v.acc == acc && v.phi == phi)
             return &v;
     }
     return nullptr;
@@ -448,10 +546,8 @@ cudaError_t launch_force(const ForceVariant* v, const ForceArgs& a, int grid, cu
 }
 
 cudaError_t launch_pack(const double* pos, const double* mass, const double* eps2, int64_t n,
-                        int64_t npad, float4* body, float* hsoft, cudaStream_t s) {
-    // Ghost bodies (zero mass, at the origin) take body 0's softening, so the
-    // pair term stays finite and contributes exactly zero.
-    pack_kernel<<<grid_for(npad, 256), 256, 0, s>>>(pos, mass, eps2, n, npad, body, hsoft, -1.0f);
+                        int64_t npad, const Shadow& sh, cudaStream_t s) {
+    pack_kernel<<<grid_for(npad, 256), 256, 0, s>>>(pos, mass, eps2, n, npad, sh);
     return cudaGetLastError();
 }
 

@@ -72,9 +72,11 @@ __device__ d3 fex(const FieldConsts& F, const d3& p) {
     return d3{s * p.x, s * p.y, s * p.z};
 }
 
-__device__ __forceinline__ void write_shadow(float4* body, int64_t i, const d3& p, double m) {
-    body[i] = make_float4(static_cast<float>(p.x), static_cast<float>(p.y), static_cast<float>(p.z),
-                          static_cast<float>(m));
+// Positions of the FP32 shadow (its masses and softenings never change).
+__device__ __forceinline__ void write_shadow(const Shadow& sh, int64_t i, const d3& p) {
+    sh.x[i] = static_cast<float>(p.x);
+    sh.y[i] = static_cast<float>(p.y);
+    sh.z[i] = static_cast<float>(p.z);
 }
 
 // Predictor (istep 0): v* = v + dt f, x* = x + dt/2 (v + v*), f = a + fex(x).
@@ -89,7 +91,7 @@ __device__ __forceinline__ void predict(const StepArgs& a, int64_t i, const d3& 
     pt.z = r.z + 0.5 * a.dt * (v.z + vt.z);
     st3(a.post, i, pt);
     st3(a.velt, i, vt);
-    write_shadow(a.body, i, pt, a.mass[i]);
+    write_shadow(a.shadow, i, pt);
 }
 
 __global__ void predictor_kernel(const StepArgs a) {

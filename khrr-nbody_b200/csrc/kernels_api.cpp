@@ -27,15 +27,15 @@ khrr_status prepare_kernel_pass(khrr_ctx* c, const double* pos_i, const double* 
                                 bool phi, const ForceVariant** vout) {
     if (n < 1 || n > (int64_t(1) << 30)) return c->fail(KHRR_ERR_INVALID_ARG, "n out of range");
     if (!pos_i || !pos_j || !mass_j || !eps2_j) return c->fail(KHRR_ERR_INVALID_ARG, "null device pointer");
+    const bool packed = c->tuning.packed != 0;
     const ForceVariant* v =
-        find_force_variant(c->tuning.threads, c->tuning.i_per_thread, c->tuning.j_tile, false, acc, phi);
+        find_force_variant(c->tuning.threads, c->tuning.i_per_thread, c->tuning.j_tile, packed, false, acc, phi);
     const ForceVariant* vplan =
-        find_force_variant(c->tuning.threads, c->tuning.i_per_thread, c->tuning.j_tile, false, true, false);
+        find_force_variant(c->tuning.threads, c->tuning.i_per_thread, c->tuning.j_tile, packed, false, true, false);
     if (!v || !vplan) return c->fail(KHRR_ERR_INVALID_ARG, "no force kernel for the current tuning");
     const int64_t npad = round_up(n, kPad);
     khrr_status st;
-    if ((st = c->cuda(c->kbody.ensure(npad), "alloc")) != KHRR_OK) return st;
-    if ((st = c->cuda(c->khsoft.ensure(npad), "alloc")) != KHRR_OK) return st;
+    if ((st = c->cuda(c->kshadow.ensure(5 * static_cast<size_t>(npad)), "alloc")) != KHRR_OK) return st;
     ForcePlan& p = c->kplan;
     const int ctas = c->resident_ctas(vplan);
     if (!p.valid || c->kplan_n != n || p.threads != v->threads || p.ipt != v->i_per_thread ||
@@ -58,12 +58,12 @@ khrr_status prepare_kernel_pass(khrr_ctx* c, const double* pos_i, const double* 
     if ((st = c->cuda(c->kpart.ensure(static_cast<size_t>(p.nslots) * npad), "alloc partials")) != KHRR_OK)
         return st;
     cudaStream_t s = c->stream;
-    if ((st = c->cuda(launch_pack(pos_j, mass_j, eps2_j, n, npad, c->kbody.p, c->khsoft.p, s), "pack")) != KHRR_OK)
+    if ((st = c->cuda(launch_pack(pos_j, mass_j, eps2_j, n, npad, shadow_at(c->kshadow.p, npad), s), "pack")) !=
+        KHRR_OK)
         return st;
     if (pos_i != pos_j) {
-        if ((st = c->cuda(c->kibody.ensure(npad), "alloc")) != KHRR_OK) return st;
-        if ((st = c->cuda(c->kihsoft.ensure(npad), "alloc")) != KHRR_OK) return st;
-        if ((st = c->cuda(launch_pack(pos_i, mass_j, eps2_j, n, npad, c->kibody.p, c->kihsoft.p, s), "pack")) !=
+        if ((st = c->cuda(c->kishadow.ensure(5 * static_cast<size_t>(npad)), "alloc")) != KHRR_OK) return st;
+        if ((st = c->cuda(launch_pack(pos_i, mass_j, eps2_j, n, npad, shadow_at(c->kishadow.p, npad), s), "pack")) !=
             KHRR_OK)
             return st;
     }
@@ -74,15 +74,14 @@ khrr_status prepare_kernel_pass(khrr_ctx* c, const double* pos_i, const double* 
 khrr_status run_kernel_pass(khrr_ctx* c, const ForceVariant* v, bool distinct_i) {
     ForcePlan& p = c->kplan;
     ForceArgs a{};
-    a.body = c->kbody.p;
-    a.hsoft = c->khsoft.p;
-    a.ibody = distinct_i ? c->kibody.p : c->kbody.p;
-    a.ihsoft = distinct_i ? c->kihsoft.p : c->khsoft.p;
+    const int64_t npad = round_up(c->kplan_n, kPad);
+    a.j = shadow_at(c->kshadow.p, npad);
+    a.i = distinct_i ? shadow_at(c->kishadow.p, npad) : a.j;
     a.items = p.d_items.p;
     a.n_items = static_cast<int>(p.items.size());
     a.queue = c->queue.p;
     a.part = c->kpart.p;
-    a.npad = round_up(c->kplan_n, kPad);
+    a.npad = npad;
     a.h_uniform = 0.0f;
     a.err = c->errflag.p;
     cudaStream_t s = c->stream;
@@ -161,8 +160,8 @@ khrr_status khrr_autotune(khrr_ctx* c, const char* cache_path) {
         const size_t at = text.find(needle);
         if (at != std::string::npos) {
             khrr_tuning t{};
-            if (std::sscanf(text.c_str() + at + needle.size(), "%d, %d, %d, %d", &t.threads, &t.i_per_thread,
-                            &t.j_tile, &t.j_split) == 4 &&
+            if (std::sscanf(text.c_str() + at + needle.size(), "%d, %d, %d, %d, %d", &t.threads, &t.i_per_thread,
+                            &t.j_tile, &t.j_split, &t.packed) == 5 &&
                 khrr_set_tuning(c, &t) == KHRR_OK)
                 return KHRR_OK;
         }
@@ -171,9 +170,11 @@ khrr_status khrr_autotune(khrr_ctx* c, const char* cache_path) {
     const khrr_tuning keep = c->tuning;
     khrr_tuning best = keep;
     double best_ms = 1e300;
-    const int shapes[][2] = {{128, 4}, {128, 8}, {256, 4}, {256, 8}};
+    // {threads, i bodies per thread, packed}
+    const int shapes[][3] = {{128, 2, 1}, {128, 4, 1}, {256, 2, 1}, {256, 4, 1},
+                             {128, 4, 0}, {128, 8, 0}, {256, 4, 0}, {256, 8, 0}};
     for (const auto& sh : shapes) {
-        khrr_tuning t{sh[0], sh[1], 128, 0};
+        khrr_tuning t{sh[0], sh[1], 128, 0, sh[2]};
         if (khrr_set_tuning(c, &t) != KHRR_OK) continue;
         khrr_enable_timing(c, 0);
         khrr_status st = khrr_forces(c, KHRR_ACC);  // warm-up (plans, caches)
@@ -200,7 +201,7 @@ khrr_status khrr_autotune(khrr_ctx* c, const char* cache_path) {
         // Append (or start) the JSON object.
         std::string entry = std::string("\"") + key + "\": [" + std::to_string(best.threads) + ", " +
                             std::to_string(best.i_per_thread) + ", " + std::to_string(best.j_tile) + ", " +
-                            std::to_string(best.j_split) + "]";
+                            std::to_string(best.j_split) + ", " + std::to_string(best.packed) + "]";
         std::string out;
         const size_t close = text.rfind('}');
         if (close == std::string::npos || text.find('{') == std::string::npos) {

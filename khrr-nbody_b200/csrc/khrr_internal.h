@@ -23,15 +23,29 @@ struct WorkItem {
     int j_end;    // end of the chunk (multiple of the j tile)
     int slot;     // partial-sum slot this chunk writes
     int sys;      // system index
-    int pad0, pad1;
+    int pad0;     // i bodies in the tile (planner's cost estimate only)
+    int pad1;
 };
+
+// FP32 shadow of a body set in structure-of-arrays form (padded length each):
+// x, y, z, m and h = eps^2 / 2.  The force kernel streams j tiles of every
+// array with bulk copies (16-byte aligned: j tiles start at multiples of 128).
+struct Shadow {
+    float* x;
+    float* y;
+    float* z;
+    float* m;
+    float* h;
+};
+
+inline Shadow shadow_at(float* base, int64_t npad) {
+    return Shadow{base, base + npad, base + 2 * npad, base + 3 * npad, base + 4 * npad};
+}
 
 // Arguments of one force-kernel launch.
 struct ForceArgs {
-    const float4* body;      // padded FP32 shadow of the j bodies: x, y, z, m
-    const float* hsoft;      // padded 0.5 * eps2 (FP32) of the j bodies
-    const float4* ibody;     // i bodies (x, y, z; equal to body unless the i and j sets differ)
-    const float* ihsoft;     // 0.5 * eps2 of the i bodies
+    Shadow j;                // the j (source) bodies
+    Shadow i;                // the i (target) bodies; equal to j unless the sets differ
     const WorkItem* items;   // work queue
     int n_items;
     unsigned* queue;         // next-item counter (zeroed before each launch)
@@ -44,7 +58,7 @@ struct ForceArgs {
 // One compiled force-kernel instance.
 struct ForceVariant {
     int threads, i_per_thread, j_tile, stages;
-    bool uniform_eps, acc, phi;
+    bool packed, uniform_eps, acc, phi;
     const void* fn;
     size_t smem;
 };
@@ -60,12 +74,12 @@ FieldConsts make_field(double Mh, double a, double Rh, double Mb, double b, doub
 // ---- force.cu ---------------------------------------------------------------
 int force_variant_count();
 const ForceVariant* force_variant(int idx);
-const ForceVariant* find_force_variant(int threads, int ipt, int jt, bool unif, bool acc,
-                                       bool phi);
+const ForceVariant* find_force_variant(int threads, int ipt, int jt, bool packed, bool unif,
+                                       bool acc, bool phi);
 cudaError_t launch_force(const ForceVariant* v, const ForceArgs& a, int grid, cudaStream_t s);
-// FP64 AoS positions -> padded FP32 shadow (x, y, z, m) and 0.5 * eps2.
+// FP64 AoS positions -> padded FP32 SoA shadow (x, y, z, m, eps2 / 2).
 cudaError_t launch_pack(const double* pos, const double* mass, const double* eps2, int64_t n,
-                        int64_t npad, float4* body, float* hsoft, cudaStream_t s);
+                        int64_t npad, const Shadow& sh, cudaStream_t s);
 // Partials -> out[i] (+)= sum_s part[s][i] (xyz) and/or phi[i] (-)= ...
 cudaError_t launch_reduce_partials(const double4* part, long long npad, int nslots, int64_t n,
                                    double* acc, double* phi, bool overwrite, cudaStream_t s);
@@ -86,7 +100,7 @@ struct StepArgs {
     double* acct;         // force workspace of the literal reference loop
     const double* mass;   // [npad]
     double* phi;          // [npad] potential (written when want_phi)
-    float4* body;         // FP32 shadow written with the predicted positions
+    Shadow shadow;        // FP32 shadow: x, y, z rewritten with the predicted positions
     const double4* part;  // force partials [slot][npad]
     long long npad;
     const unsigned char* nsplit;  // partial slots per body

@@ -80,23 +80,21 @@ struct khrr_ctx {
     int64_t n = 0, npad = 0;
     std::vector<int64_t> off, poff, cnt;  // real offsets, padded offsets, counts per system
     khrr::DevBuf<double> pos, vel, acc, post, velt, acct, mass, eps2, phi;
-    khrr::DevBuf<float4> body;
-    khrr::DevBuf<float> hsoft;
+    khrr::DevBuf<float> shadow_buf;  // SoA FP32 shadow, 5 x npad
     khrr::DevBuf<double4> part;
     khrr::DevBuf<unsigned> queue, errflag;
     khrr::DevBuf<double> cons_blocks, scratch;
     bool uniform = false;
     float h_uniform = 0.0f;
     khrr::FieldConsts field{};
-    khrr_tuning tuning{128, 8, 128, 0};
+    khrr_tuning tuning{128, 4, 128, 0, 1};
     khrr::ForcePlan plan_batched, plan_plain;
     bool predicted = false;
     double pred_dt = 0.0;
     std::map<std::tuple<uint64_t, bool, bool, bool>, khrr::StepGraph> graphs;
 
     // Kernel-level entry points: their own shadow, partials and plan.
-    khrr::DevBuf<float4> kbody, kibody;
-    khrr::DevBuf<float> khsoft, kihsoft;
+    khrr::DevBuf<float> kshadow, kishadow;
     khrr::DevBuf<double4> kpart;
     khrr::ForcePlan kplan;
     int64_t kplan_n = -1;
@@ -120,6 +118,7 @@ struct khrr_ctx {
     khrr::ForceArgs force_args(const khrr::ForcePlan& p, int item_begin, int item_end);
     khrr_status enqueue_force(bool plain, bool acc, bool phi, bool events);
     khrr::StepArgs step_args(const khrr::ForcePlan& p, double dt);
+    khrr::Shadow shadow() { return khrr::shadow_at(shadow_buf.p, npad); }
     khrr_status enqueue_step(double dt, bool plain, bool phi_now, bool compat);
     khrr_status get_step_graph(double dt, bool plain, bool phi_now, bool compat, khrr::StepGraph** out);
     khrr_status timing_pair(cudaEvent_t* e0, cudaEvent_t* e1);

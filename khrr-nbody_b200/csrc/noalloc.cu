@@ -3,12 +3,12 @@
 // their call path (a host program that fixes its device-memory budget at
 // start-up, or a plugin host that only hands out buffers it owns).
 //
-// It drives the same force kernel as khrr_accel (shape 128 threads x 4 i
-// bodies, 128-body j tiles, non-uniform softening) over the same work
+// It drives the same force kernel as khrr_accel (packed form, 128 threads x
+// 4 i bodies, 128-body j tiles, non-uniform softening) over the same work
 // decomposition, but takes every scratch buffer from g_noalloc_scratch:
 //   counters  queue counter + error flag (cleared on every call)
-//   body      FP32 shadow of the j bodies, hsoft their eps^2 / 2
-//   ibody     shadow of the i bodies when pos_i != pos_j
+//   jshadow   FP32 SoA shadow of the j bodies (x, y, z, m, eps^2 / 2)
+//   ishadow   shadow of the i bodies when pos_i != pos_j
 //   items     the work queue, written on the device by noalloc_items_kernel
 //   part      per-chunk FP64 partial sums, reduced into acc at the end
 // Host code never uses the array's name as an address: the device address is
@@ -33,16 +33,13 @@ constexpr int64_t kMaxItems = (kMaxBodies + kItile - 1) / kItile * kMaxSplit;
 
 // Byte offsets of the sections; every one is a multiple of 256.
 constexpr size_t kOffCounters = 0;
-constexpr size_t kOffBody = 256;
-constexpr size_t kOffHsoft = kOffBody + kMaxBodies * sizeof(float4);
-constexpr size_t kOffIBody = kOffHsoft + kMaxBodies * sizeof(float);
-constexpr size_t kOffIHsoft = kOffIBody + kMaxBodies * sizeof(float4);
-constexpr size_t kOffItems = kOffIHsoft + kMaxBodies * sizeof(float);
+constexpr size_t kOffJShadow = 256;
+constexpr size_t kOffIShadow = kOffJShadow + 5 * kMaxBodies * sizeof(float);
+constexpr size_t kOffItems = kOffIShadow + 5 * kMaxBodies * sizeof(float);
 constexpr size_t kOffPart = kOffItems + kMaxItems * sizeof(WorkItem);
 constexpr size_t kScratchBytes = kOffPart + static_cast<size_t>(kMaxSplit) * kMaxBodies * sizeof(double4);
 static_assert(kMaxBodies % kPad == 0, "maximum must be a multiple of the padding");
-static_assert(kOffHsoft % 256 == 0 && kOffIBody % 256 == 0 && kOffIHsoft % 256 == 0 &&
-                  kOffItems % 256 == 0 && kOffPart % 256 == 0,
+static_assert(kOffIShadow % 256 == 0 && kOffItems % 256 == 0 && kOffPart % 256 == 0,
               "scratch sections must stay 256-byte aligned");
 
 }  // namespace
@@ -114,7 +111,7 @@ extern "C" khrr_status khrr_accel_noalloc(double* acc, const double* pos_i, cons
     using namespace khrr;
     if (!acc || !pos_i || !pos_j || !mass_j || !eps2_j || n < 1) return KHRR_ERR_INVALID_ARG;
     if (n > kMaxBodies) return KHRR_ERR_TOO_LARGE;
-    const ForceVariant* v = find_force_variant(kThreads, kIpt, kJt, false, true, false);
+    const ForceVariant* v = find_force_variant(kThreads, kIpt, kJt, true, false, true, false);
     if (!v) return KHRR_ERR_UNSUPPORTED;
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
@@ -130,10 +127,8 @@ extern "C" khrr_status khrr_accel_noalloc(double* acc, const double* pos_i, cons
     const int nitems = nit * split;
 
     unsigned* counters = reinterpret_cast<unsigned*>(s->base + kOffCounters);
-    float4* body = reinterpret_cast<float4*>(s->base + kOffBody);
-    float* hsoft = reinterpret_cast<float*>(s->base + kOffHsoft);
-    float4* ibody = reinterpret_cast<float4*>(s->base + kOffIBody);
-    float* ihsoft = reinterpret_cast<float*>(s->base + kOffIHsoft);
+    const Shadow jsh = shadow_at(reinterpret_cast<float*>(s->base + kOffJShadow), npad);
+    const Shadow ish = shadow_at(reinterpret_cast<float*>(s->base + kOffIShadow), npad);
     WorkItem* items = reinterpret_cast<WorkItem*>(s->base + kOffItems);
     double4* part = reinterpret_cast<double4*>(s->base + kOffPart);
 
@@ -143,16 +138,13 @@ extern "C" khrr_status khrr_accel_noalloc(double* acc, const double* pos_i, cons
     noalloc_items_kernel<<<(nitems + 127) / 128, 128, 0, st>>>(items, static_cast<int>(n), static_cast<int>(kItile),
                                                               split, tiles, nitems);
     if ((e = cudaGetLastError()) != cudaSuccess) return as_status(e);
-    if ((e = launch_pack(pos_j, mass_j, eps2_j, n, npad, body, hsoft, st)) != cudaSuccess) return as_status(e);
+    if ((e = launch_pack(pos_j, mass_j, eps2_j, n, npad, jsh, st)) != cudaSuccess) return as_status(e);
     const bool distinct = pos_i != pos_j;
-    if (distinct && (e = launch_pack(pos_i, mass_j, eps2_j, n, npad, ibody, ihsoft, st)) != cudaSuccess)
-        return as_status(e);
+    if (distinct && (e = launch_pack(pos_i, mass_j, eps2_j, n, npad, ish, st)) != cudaSuccess) return as_status(e);
 
     ForceArgs a{};
-    a.body = body;
-    a.hsoft = hsoft;
-    a.ibody = distinct ? ibody : body;
-    a.ihsoft = distinct ? ihsoft : hsoft;
+    a.j = jsh;
+    a.i = distinct ? ish : jsh;
     a.items = items;
     a.n_items = nitems;
     a.queue = counters;

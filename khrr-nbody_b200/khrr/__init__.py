@@ -50,7 +50,7 @@ class Lie(C.Structure):
 
 
 class Tuning(C.Structure):
-    _fields_ = [(k, C.c_int) for k in ("threads", "i_per_thread", "j_tile", "j_split")]
+    _fields_ = [(k, C.c_int) for k in ("threads", "i_per_thread", "j_tile", "j_split", "packed")]
 
 
 _lib = None
@@ -245,8 +245,8 @@ class Context:
         self._check(self.L.khrr_conservation(self.h, C.byref(out)))
         return out.as_dict()
 
-    def set_tuning(self, threads=128, i_per_thread=8, j_tile=128, j_split=0):
-        t = Tuning(threads, i_per_thread, j_tile, j_split)
+    def set_tuning(self, threads=128, i_per_thread=4, j_tile=128, j_split=0, packed=1):
+        t = Tuning(threads, i_per_thread, j_tile, j_split, packed)
         self._check(self.L.khrr_set_tuning(self.h, C.byref(t)))
 
     def get_tuning(self) -> dict:

@@ -118,16 +118,38 @@ def test_accel_distinct_target_set(ctx, torch_cuda):
     assert rel_rms(a, ref) <= SMALL_N_TOL
 
 
-@pytest.mark.parametrize("threads,ipt", [(128, 4), (128, 8), (256, 4), (256, 8)])
+SHAPES = [(128, 2, 1), (128, 4, 1), (256, 2, 1), (256, 4, 1),
+          (128, 4, 0), (128, 8, 0), (256, 4, 0), (256, 8, 0)]
+
+
+@pytest.mark.parametrize("threads,ipt,packed", SHAPES)
 @pytest.mark.parametrize("split", [0, 1, 3, 7])
-def test_every_kernel_shape_and_split(ctx, torch_cuda, golden, threads, ipt, split):
+def test_every_kernel_shape_and_split(ctx, torch_cuda, golden, threads, ipt, packed, split):
     g = golden("forces_n1536.npz")
-    ctx.set_tuning(threads, ipt, 128, split)
+    ctx.set_tuning(threads, ipt, 128, split, packed)
     try:
         a = kernel_accel(ctx, torch_cuda, g["pos"], g["mass"], g["eps2"])
     finally:
-        ctx.set_tuning(128, 8, 128, 0)
+        ctx.set_tuning()
     assert rel_rms(a, g["acc_f64"]) <= 1e-6
+
+
+@pytest.mark.parametrize("threads,ipt,packed", SHAPES)
+def test_every_shape_in_time_steps(ctx, golden, threads, ipt, packed):
+    """Uniform-softening kernels (the state API picks them) in graph steps,
+    with the potential fused into the last pass."""
+    import khrr
+    g = golden("steps_n1024.npz")
+    ctx.set_tuning(threads, ipt, 128, 0, packed)
+    try:
+        ctx.upload(g["pos"], g["vel"], g["mass"], g["eps2"])
+        ctx.forces(khrr.ACC)
+        ctx.step(float(g["dt"]), int(g["nsteps"]), khrr.PHI)
+        out = ctx.download()
+    finally:
+        ctx.set_tuning()
+    assert np.abs(out["pos"].reshape(-1) - g["corrected_pos"]).max() <= 1e-7
+    assert rel_rms(out["acc"], g["corrected_acc"]) <= 1e-5
 
 
 def test_integ_time_matches_reference(ctx, torch_cuda, golden, oracle):
