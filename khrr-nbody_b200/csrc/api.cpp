@@ -76,9 +76,15 @@ int khrr_ctx::resident_ctas(const ForceVariant* v) {
     return occ * sm_count;
 }
 
+// The state's kernel: the tile-mass form where the layout allows it and the
+// shape has one, else the general form.
 const ForceVariant* khrr_ctx::variant(bool unif, bool acc, bool phi) const {
-    return find_force_variant(tuning.threads, tuning.i_per_thread, tuning.j_tile, tuning.packed != 0, unif, acc,
-                              phi);
+    const bool packed = tuning.packed != 0;
+    if (tile_uniform_mass)
+        if (const ForceVariant* v =
+                find_force_variant(tuning.threads, tuning.i_per_thread, tuning.j_tile, packed, unif, acc, phi, true))
+            return v;
+    return find_force_variant(tuning.threads, tuning.i_per_thread, tuning.j_tile, packed, unif, acc, phi, false);
 }
 
 // ---------------------------------------------------------------------------
@@ -228,6 +234,7 @@ ForceArgs khrr_ctx::force_args(const ForcePlan& p, int item_begin, int item_end)
     a.part = part.p;
     a.npad = npad;
     a.h_uniform = h_uniform;
+    a.tile_mass = tile_mass.p;
     a.err = errflag.p;
     return a;
 }
@@ -551,7 +558,27 @@ khrr_status khrr_upload_state(khrr_ctx* c, int64_t n, const double* pos, const d
     }
     c->uniform = uniform_new;
     c->h_uniform = static_cast<float>(0.5 * eps2[0]);
-    st = c->cuda(cudaMemcpyAsync(c->eps2.p, e2.data(), np * sizeof(double), cudaMemcpyHostToDevice, s), "upload");
+    // One mass per 128-body tile (and no ghosts) lets the kernel factor the
+    // mass out of each tile sum; the reference's layouts have it (component
+    // counts are multiples of 1024).
+    std::vector<float> tm(np / kPad, 0.0f);
+    bool tile_uniform = true;
+    for (int k = 0; k < nsys && tile_uniform; ++k) {
+        if (c->cnt[k] % kPad) tile_uniform = false;
+        for (int64_t b = 0; b < c->cnt[k] && tile_uniform; b += kPad) {
+            const double m0 = mass[off[k] + b];
+            for (int64_t q = 1; q < kPad; ++q)
+                if (mass[off[k] + b + q] != m0) tile_uniform = false;
+            tm[(c->poff[k] + b) / kPad] = static_cast<float>(m0);
+        }
+    }
+    if (tile_uniform != c->tile_uniform_mass) c->drop_graphs();
+    c->tile_uniform_mass = tile_uniform;
+    if ((st = c->cuda(c->tile_mass.ensure(tm.size()), "alloc tile masses")) != KHRR_OK) return st;
+    st = c->cuda(cudaMemcpyAsync(c->tile_mass.p, tm.data(), tm.size() * sizeof(float), cudaMemcpyHostToDevice, s),
+                 "upload");
+    if (st == KHRR_OK)
+        st = c->cuda(cudaMemcpyAsync(c->eps2.p, e2.data(), np * sizeof(double), cudaMemcpyHostToDevice, s), "upload");
     for (int k = 0; k < nsys && st == KHRR_OK; ++k) {
         const size_t o = static_cast<size_t>(off[k]), q = static_cast<size_t>(c->poff[k]);
         const size_t m = static_cast<size_t>(c->cnt[k]);

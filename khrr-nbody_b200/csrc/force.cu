@@ -116,10 +116,20 @@ __device__ __forceinline__ float2 f2(float a, float b) { return make_float2(a, b
 
 constexpr int kBarBytes = 128;  // mbarriers live in the first 128 bytes
 
-template <int NT, int K, int JT, int STAGES, bool UNIF, bool ACC, bool PHI>
+// Kernel features (template bit mask).
+constexpr unsigned kUnif = 1;     // every body has the same softening: no h array
+constexpr unsigned kAcc = 2;      // accumulate accelerations
+constexpr unsigned kPhi = 4;      // accumulate potentials
+constexpr unsigned kPacked = 8;   // packed f32x2 inner loop (two j bodies per instruction)
+constexpr unsigned kTileMass = 16;  // each j tile has one mass (ForceArgs::tile_mass): m factored out
+
+template <int NT, int K, int JT, int STAGES, unsigned F>
 struct ForceShape {
+    static constexpr bool UNIF = F & kUnif, ACC = F & kAcc, PHI = F & kPhi, TMASS = F & kTileMass;
     static constexpr int NC = (ACC ? 3 : 0) + (PHI ? 1 : 0);
-    static constexpr int NCOMP = UNIF ? 4 : 5;  // shadow arrays copied per tile
+    // Shadow arrays copied per tile, in ring order: x, y, z, [m], [h].
+    static constexpr int NCOMP = 3 + (TMASS ? 0 : 1) + (UNIF ? 0 : 1);
+    static constexpr int kOffM = 3, kOffH = TMASS ? 3 : 4;
     static constexpr unsigned kTileBytes = NCOMP * JT * 4u;
     static constexpr size_t kSmem = kBarBytes + (size_t)STAGES * kTileBytes + (size_t)K * NC * 2 * NT * 4;
 };
@@ -155,9 +165,11 @@ struct TileAcc<K, false> {
     __device__ __forceinline__ float p(int k) const { return pp[k]; }
 };
 
-template <int NT, int K, int JT, int STAGES, bool UNIF, bool ACC, bool PHI, bool PACKED>
+template <int NT, int K, int JT, int STAGES, unsigned F>
 __global__ void __launch_bounds__(NT) force_kernel(const ForceArgs a) {
-    using S = ForceShape<NT, K, JT, STAGES, UNIF, ACC, PHI>;
+    using S = ForceShape<NT, K, JT, STAGES, F>;
+    constexpr bool UNIF = S::UNIF, ACC = S::ACC, PHI = S::PHI, TMASS = S::TMASS;
+    constexpr bool PACKED = F & kPacked;
     constexpr int NC = S::NC;
     constexpr int NCOMP = S::NCOMP;
     static_assert(NC > 0, "nothing to accumulate");
@@ -184,8 +196,8 @@ __global__ void __launch_bounds__(NT) force_kernel(const ForceArgs a) {
         bulk_copy_g2s(dst, a.j.x + jstart, JT * 4u, &full[stage]);
         bulk_copy_g2s(dst + JT, a.j.y + jstart, JT * 4u, &full[stage]);
         bulk_copy_g2s(dst + 2 * JT, a.j.z + jstart, JT * 4u, &full[stage]);
-        bulk_copy_g2s(dst + 3 * JT, a.j.m + jstart, JT * 4u, &full[stage]);
-        if (!UNIF) bulk_copy_g2s(dst + 4 * JT, a.j.h + jstart, JT * 4u, &full[stage]);
+        if (!TMASS) bulk_copy_g2s(dst + S::kOffM * JT, a.j.m + jstart, JT * 4u, &full[stage]);
+        if (!UNIF) bulk_copy_g2s(dst + S::kOffH * JT, a.j.h + jstart, JT * 4u, &full[stage]);
     };
 
     unsigned consumed = 0;  // tiles this CTA has consumed, over all its items
@@ -203,7 +215,7 @@ __global__ void __launch_bounds__(NT) force_kernel(const ForceArgs a) {
         }
 
         // i bodies: negated coordinates (d = x_j + (-x_i) rounds like x_j - x_i)
-        // and the eps term, duplicated into both lanes for the packed form.
+        // and the eps term.
         float nx[K], ny[K], nz[K], hh[K];
 #pragma unroll
         for (int k = 0; k < K; ++k) {
@@ -224,6 +236,7 @@ __global__ void __launch_bounds__(NT) force_kernel(const ForceArgs a) {
         for (int t = 0; t < ntiles; ++t) {
             const unsigned q = consumed + static_cast<unsigned>(t);
             const int stage = static_cast<int>(q % STAGES);
+            const float mt = TMASS ? a.tile_mass[(w.j_begin + t * JT) / JT] : 1.0f;
             const bool ok = mbar_wait_bounded(&full[stage], (q / STAGES) & 1u);
 
             TileAcc<K, PACKED> acc;
@@ -232,11 +245,12 @@ __global__ void __launch_bounds__(NT) force_kernel(const ForceArgs a) {
                 const float4* tx = reinterpret_cast<const float4*>(ring + stage * NCOMP * JT);
                 const float4* ty = tx + JT / 4;
                 const float4* tz = tx + 2 * (JT / 4);
-                const float4* tm = tx + 3 * (JT / 4);
-                const float4* th = tx + 4 * (JT / 4);
+                const float4* tm = tx + S::kOffM * (JT / 4);
+                const float4* th = tx + S::kOffH * (JT / 4);
 #pragma unroll 1
                 for (int q4 = 0; q4 < JT / 4; ++q4) {
-                    const float4 X = tx[q4], Y = ty[q4], Z = tz[q4], M = tm[q4];
+                    const float4 X = tx[q4], Y = ty[q4], Z = tz[q4];
+                    const float4 M = TMASS ? make_float4(1.f, 1.f, 1.f, 1.f) : tm[q4];
                     const float4 H = UNIF ? make_float4(0.f, 0.f, 0.f, 0.f) : th[q4];
                     if constexpr (PACKED) {
 #pragma unroll
@@ -256,7 +270,8 @@ __global__ void __launch_bounds__(NT) force_kernel(const ForceArgs a) {
                                 r2 = __ffma2_rn(dy, dy, r2);
                                 r2 = __ffma2_rn(dz, dz, r2);
                                 const float2 inv = f2(rsqrt_approx(r2.x), rsqrt_approx(r2.y));
-                                const float2 minv = __fmul2_rn(mj, inv);
+                                // m r^-1 (the tile mass is applied once per tile when factored out)
+                                const float2 minv = TMASS ? inv : __fmul2_rn(mj, inv);
                                 if (ACC) {
                                     const float2 f = __fmul2_rn(minv, __fmul2_rn(inv, inv));
                                     acc.ax[k] = __ffma2_rn(dx, f, acc.ax[k]);
@@ -279,7 +294,7 @@ __global__ void __launch_bounds__(NT) force_kernel(const ForceArgs a) {
                                 const float dz = zs[u] + nz[k];
                                 const float r2 = fmaf(dz, dz, fmaf(dy, dy, fmaf(dx, dx, UNIF ? hh[k] : hh[k] + hs[u])));
                                 const float inv = rsqrt_approx(r2);
-                                const float minv = ms[u] * inv;
+                                const float minv = TMASS ? inv : ms[u] * inv;
                                 if (ACC) {
                                     const float f = minv * (inv * inv);
                                     acc.ax[k] = fmaf(dx, f, acc.ax[k]);
@@ -292,29 +307,30 @@ __global__ void __launch_bounds__(NT) force_kernel(const ForceArgs a) {
                     }
                 }
             }
-            // Fold the tile partials into the compensated running sums.
+            // Fold the tile partials (times the tile mass when it was factored
+            // out) into the compensated running sums.
 #pragma unroll
             for (int k = 0; k < K; ++k) {
                 float* r = run + (k * NC * 2) * NT + tid;
                 int c = 0;
                 if (ACC) {
                     float h0 = r[0], l0 = r[NT];
-                    two_sum_into(h0, l0, acc.x(k));
+                    two_sum_into(h0, l0, TMASS ? mt * acc.x(k) : acc.x(k));
                     r[0] = h0;
                     r[NT] = l0;
                     float h1 = r[2 * NT], l1 = r[3 * NT];
-                    two_sum_into(h1, l1, acc.y(k));
+                    two_sum_into(h1, l1, TMASS ? mt * acc.y(k) : acc.y(k));
                     r[2 * NT] = h1;
                     r[3 * NT] = l1;
                     float h2 = r[4 * NT], l2 = r[5 * NT];
-                    two_sum_into(h2, l2, acc.z(k));
+                    two_sum_into(h2, l2, TMASS ? mt * acc.z(k) : acc.z(k));
                     r[4 * NT] = h2;
                     r[5 * NT] = l2;
                     c = 3;
                 }
                 if (PHI) {
                     float h3 = r[(2 * c) * NT], l3 = r[(2 * c + 1) * NT];
-                    two_sum_into(h3, l3, acc.p(k));
+                    two_sum_into(h3, l3, TMASS ? mt * acc.p(k) : acc.p(k));
                     r[(2 * c) * NT] = h3;
                     r[(2 * c + 1) * NT] = l3;
                 }
@@ -360,43 +376,50 @@ __global__ void __launch_bounds__(NT) force_kernel(const ForceArgs a) {
     }
 }
 
-template <int NT, int K, bool PACKED, int JT, int STAGES, bool UNIF, bool ACC, bool PHI>
+template <int NT, int K, unsigned F>
 ForceVariant make_variant() {
-    using S = ForceShape<NT, K, JT, STAGES, UNIF, ACC, PHI>;
+    constexpr int JT = 128, STAGES = 3;
+    using S = ForceShape<NT, K, JT, STAGES, F>;
     return ForceVariant{NT,
                         K,
                         JT,
                         STAGES,
-                        PACKED,
-                        UNIF,
-                        ACC,
-                        PHI,
-                        reinterpret_cast<const void*>(&force_kernel<NT, K, JT, STAGES, UNIF, ACC, PHI, PACKED>),
+                        (F & kPacked) != 0,
+                        (F & kUnif) != 0,
+                        (F & kAcc) != 0,
+                        (F & kPhi) != 0,
+                        (F & kTileMass) != 0,
+                        reinterpret_cast<const void*>(&force_kernel<NT, K, JT, STAGES, F>),
                         S::kSmem};
 }
 
-template <int NT, int K, bool PACKED>
+// Every softening form x every output set of one shape (and mass form).
+template <int NT, int K, unsigned BASE>
 void add_shape(ForceVariant* v, int& n) {
-    v[n++] = make_variant<NT, K, PACKED, 128, 3, false, true, false>();
-    v[n++] = make_variant<NT, K, PACKED, 128, 3, false, true, true>();
-    v[n++] = make_variant<NT, K, PACKED, 128, 3, false, false, true>();
-    v[n++] = make_variant<NT, K, PACKED, 128, 3, true, true, false>();
-    v[n++] = make_variant<NT, K, PACKED, 128, 3, true, true, true>();
-    v[n++] = make_variant<NT, K, PACKED, 128, 3, true, false, true>();
+    v[n++] = make_variant<NT, K, BASE | kAcc>();
+    v[n++] = make_variant<NT, K, BASE | kAcc | kPhi>();
+    v[n++] = make_variant<NT, K, BASE | kPhi>();
+    v[n++] = make_variant<NT, K, BASE | kUnif | kAcc>();
+    v[n++] = make_variant<NT, K, BASE | kUnif | kAcc | kPhi>();
+    v[n++] = make_variant<NT, K, BASE | kUnif | kPhi>();
 }
 
 struct VariantTable {
-    ForceVariant v[64];
+    ForceVariant v[96];
     int n = 0;
     VariantTable() {
-        add_shape<128, 2, true>(v, n);
-        add_shape<128, 4, true>(v, n);
-        add_shape<256, 2, true>(v, n);
-        add_shape<256, 4, true>(v, n);
-        add_shape<128, 4, false>(v, n);
-        add_shape<128, 8, false>(v, n);
-        add_shape<256, 4, false>(v, n);
-        add_shape<256, 8, false>(v, n);
+        add_shape<128, 2, kPacked>(v, n);
+        add_shape<128, 4, kPacked>(v, n);
+        add_shape<256, 2, kPacked>(v, n);
+        add_shape<256, 4, kPacked>(v, n);
+        add_shape<128, 2, kPacked | kTileMass>(v, n);
+        add_shape<128, 4, kPacked | kTileMass>(v, n);
+        add_shape<256, 2, kPacked | kTileMass>(v, n);
+        add_shape<256, 4, kPacked | kTileMass>(v, n);
+        add_shape<128, 4, 0>(v, n);
+        add_shape<128, 8, 0>(v, n);
+        add_shape<256, 4, 0>(v, n);
+        add_shape<256, 8, 0>(v, n);
     }
 };
 
@@ -526,12 +549,12 @@ const ForceVariant* force_variant(int idx) {
 }
 
 const ForceVariant* find_force_variant(int threads, int ipt, int jt, bool packed, bool unif, bool acc,
-                                       bool phi) {
+                                       bool phi, bool tile_mass) {
     const VariantTable& t = table();
     for (int i = 0; i < t.n; ++i) {
         const ForceVariant& v = t.v[i];
         if (v.threads == threads && v.i_per_thread == ipt && v.j_tile == jt && v.packed == packed &&
-            v.uniform_eps == unif && v.acc == acc && v.phi == phi)
+            v.uniform_eps == unif && v.acc == acc && v.phi == phi && v.tile_mass == tile_mass)
             return &v;
     }
     return nullptr;

@@ -52,13 +52,14 @@ struct ForceArgs {
     double4* part;           // partial sums [slot][npad]: ax, ay, az, sum m/r
     long long npad;          // slot stride
     float h_uniform;         // 0.5 * eps2 when every body shares it
+    const float* tile_mass;  // mass of each 128-body j tile (tile-mass kernels only)
     unsigned* err;           // device error flag word
 };
 
 // One compiled force-kernel instance.
 struct ForceVariant {
     int threads, i_per_thread, j_tile, stages;
-    bool packed, uniform_eps, acc, phi;
+    bool packed, uniform_eps, acc, phi, tile_mass;
     const void* fn;
     size_t smem;
 };
@@ -74,8 +75,10 @@ FieldConsts make_field(double Mh, double a, double Rh, double Mb, double b, doub
 // ---- force.cu ---------------------------------------------------------------
 int force_variant_count();
 const ForceVariant* force_variant(int idx);
+// tile_mass: the variant that factors each j tile's single mass out of the
+// tile sum (compiled for the packed shapes only).
 const ForceVariant* find_force_variant(int threads, int ipt, int jt, bool packed, bool unif,
-                                       bool acc, bool phi);
+                                       bool acc, bool phi, bool tile_mass = false);
 cudaError_t launch_force(const ForceVariant* v, const ForceArgs& a, int grid, cudaStream_t s);
 // FP64 AoS positions -> padded FP32 SoA shadow (x, y, z, m, eps2 / 2).
 cudaError_t launch_pack(const double* pos, const double* mass, const double* eps2, int64_t n,

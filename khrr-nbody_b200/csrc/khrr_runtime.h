@@ -86,6 +86,8 @@ struct khrr_ctx {
     khrr::DevBuf<double> cons_blocks, scratch;
     bool uniform = false;
     float h_uniform = 0.0f;
+    bool tile_uniform_mass = false;     // every 128-body tile of the layout has one mass
+    khrr::DevBuf<float> tile_mass;      // that mass per tile (FP32)
     khrr::FieldConsts field{};
     khrr_tuning tuning{128, 4, 128, 0, 1};
     khrr::ForcePlan plan_batched, plan_plain;

@@ -152,6 +152,28 @@ def test_every_shape_in_time_steps(ctx, golden, threads, ipt, packed):
     assert rel_rms(out["acc"], g["corrected_acc"]) <= 1e-5
 
 
+@pytest.mark.parametrize("threads,ipt", [(128, 2), (128, 4), (256, 2), (256, 4)])
+def test_tile_mass_form_matches_general_form(ctx, torch_cuda, oracle, threads, ipt):
+    """Component counts that are multiples of 128 give one mass per j tile, so
+    the state path factors the mass out of each tile sum; the kernel-level
+    path (general form) and the FP64 oracle must agree with it."""
+    import khrr
+    pos, vel, mass, eps2 = galaxy(2048, 4096, seed=12)
+    ctx.set_tuning(threads, ipt, 128, 0, 1)
+    try:
+        ctx.upload(pos, vel, mass, eps2)
+        ctx.forces(khrr.ACC | khrr.PHI)
+        s = ctx.download()
+        general = kernel_accel(ctx, torch_cuda, pos, mass, eps2)
+    finally:
+        ctx.set_tuning()
+    ref = oracle.accel_f64(pos, mass, eps2)
+    assert rel_rms(s["acc"], ref) <= 1e-6
+    assert rel_rms(general, ref) <= 1e-6
+    assert rel_rms(s["acc"], general) <= 1e-6
+    assert rel_rms(s["phi"], oracle.phi_f64(pos, mass, eps2)) <= 1e-6
+
+
 def test_integ_time_matches_reference(ctx, torch_cuda, golden, oracle):
     torch = torch_cuda
     f = golden("forces_n1536.npz")
