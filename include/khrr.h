@@ -117,6 +117,83 @@ khrr_status khrr_integ_time(khrr_ctx* ctx, const double* acc, double* pos_t, dou
                             const double* pos, const double* vel, double dt, int istep,
                             double t, double* acc0, int64_t n);
 
+/* ---- p2mesh: binning, prefix sums, deposits, wave stencil, gather ------- */
+/* Mesh geometry (WaveEqData.domainMin / cellSize / gridSize, common.cuh:57-61). */
+typedef struct khrr_mesh {
+    double lo[3];
+    double cell[3];
+    int grid[3];
+} khrr_mesh;
+
+/* Wave-equation constants (WaveEqData, common.cuh:62-71; values as
+ * nbody/src/nbody.cu:1134-1143 derives them: dt = 0.5 dx / (c sqrt 3),
+ * sim_l = nx dx / 2, bc_l = sim_l / 10). */
+typedef struct khrr_wave_params {
+    int nx;
+    double dx, dt, c, diss_base, diss_extra, sim_l, bc_l;
+} khrr_wave_params;
+
+enum {
+    KHRR_SCAN_REFERENCE = 0, /* start_id = total of all earlier 512-cell blocks (the reference) */
+    KHRR_SCAN_EXCLUSIVE = 1  /* start_id = exclusive prefix sum of the counts (a true scan)     */
+};
+
+/* assignParticlesToCells (p2mesh-kernel.cuh:11-57), fused with
+ * computeCellMassesUnsorted (:126-137) when mass and cell_mass are given.
+ * pos: n double3; particle_cell_info: n x {cell_id, id_in_cell} (int pairs);
+ * cell_info: C x {count, start_id}; cell_count: C (the reference's slot
+ * counter, may be NULL); cell_mass: C (may be NULL).  Counts and masses are
+ * accumulated into, as in the reference (its driver zeroes them first,
+ * nbody.cu:149-153).  Cell indices follow the reference bit for bit
+ * (IEEE FP64 division, truncation, clamps, iz clamped to gridSize.y - 1,
+ * id = iz*gx*gy + iy*gz + ix); id_in_cell is a valid slot order within each
+ * cell (atomics, as in the reference). */
+khrr_status khrr_assign_particles_to_cells(khrr_ctx* ctx, const double* pos, int64_t n,
+                                           const khrr_mesh* mesh, int* particle_cell_info,
+                                           int* cell_info, int* cell_count, const double* mass,
+                                           double* cell_mass);
+/* computePrefixSums + adjustGlobalPrefixSums (p2mesh-kernel.cuh:62-123):
+ * reads cell_info.count, writes cell_info.start_id (per mode) and max_pbc
+ * (ceil(ncells/512) ints: inclusive prefix of 512-cell block totals, the
+ * array the reference leaves in its second argument). */
+khrr_status khrr_compute_prefix_sums(khrr_ctx* ctx, int* cell_info, int* max_pbc, int64_t ncells,
+                                     int mode);
+/* computeCellPhiUnsorted (p2mesh-kernel.cuh:152-167): cell_phi[c] += phi_i /
+ * count[c] for every body (accumulates, as the reference does). */
+khrr_status khrr_cell_phi(khrr_ctx* ctx, const double* phi, const int* particle_cell_info,
+                          const int* cell_info, int64_t n, double* cell_phi);
+/* wave_diss_iteration (wave-kernel.cuh:5-103), FP64: one leap-frog step of
+ * the damped wave equation on the nx^3 mesh (faces held at 0). */
+khrr_status khrr_wave_iteration(khrr_ctx* ctx, double* phi_new, const double* phi,
+                                const double* phi_old, const double* cell_mass,
+                                const khrr_wave_params* p);
+/* acc_field (p2mesh-kernel.cuh:169-225) over the whole nx^3 mesh (the
+ * reference's 1-D launch leaves most cells unset; this covers all of them):
+ * cell_acc = -grad(phi) / dx (central, one-sided on faces), nx^3 double3;
+ * cell_acc_abs (nx^3, may be NULL) = |cell_acc|. */
+khrr_status khrr_acc_field(khrr_ctx* ctx, double* cell_acc, double* cell_acc_abs,
+                           const double* cell_phi, int nx, double dx);
+/* apply_acceleration_to_particles + apply_cell_to_particles
+ * (p2mesh-kernel.cuh:227-254): NGP gather; either output may be NULL. */
+khrr_status khrr_apply_cells_to_particles(khrr_ctx* ctx, double* particle_acc,
+                                          double* particle_value, const double* cell_acc,
+                                          const double* cell_value,
+                                          const int* particle_cell_info, int64_t n);
+
+/* Context-level mesh pipeline on the uploaded positions: bin, scan (both
+ * views), deposit masses; results stay on the device for khrr_wave_solve and
+ * are copied to any non-NULL host array (n or C entries). */
+khrr_status khrr_bin(khrr_ctx* ctx, const khrr_mesh* mesh, int* cell_id, int* id_in_cell,
+                     int* count, int* start, int* start_ref, double* cell_mass);
+/* Damped-wave Poisson solve on the last khrr_bin's masses (mesh: p->nx^3,
+ * same geometry): FP32 stencil, the residual |phi_new - phi|_2 / |phi_new|_2
+ * reduced in FP64 every check_every iterations; stops below tol or after
+ * max_iter.  Starts from the previous solve's field (warm start) unless
+ * cold != 0.  phi_out (nx^3 floats, may be NULL) receives the field. */
+khrr_status khrr_wave_solve(khrr_ctx* ctx, const khrr_wave_params* p, double tol, int max_iter,
+                            int check_every, int cold, int* iters, double* resid,
+                            float* phi_out);
+
 /* Largest n khrr_accel_noalloc accepts. */
 #define KHRR_NOALLOC_MAX_BODIES 32768
 /* khrr_accel without any device allocation.  This entry point has no

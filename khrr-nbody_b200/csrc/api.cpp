@@ -219,6 +219,11 @@ void khrr_ctx::drop_graphs() {
         if (kv.second.graph) cudaGraphDestroy(kv.second.graph);
     }
     graphs.clear();
+    for (auto& kv : wave_graphs) {
+        if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
+        if (kv.second.graph) cudaGraphDestroy(kv.second.graph);
+    }
+    wave_graphs.clear();
 }
 
 // ---------------------------------------------------------------------------

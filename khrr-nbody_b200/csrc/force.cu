@@ -116,6 +116,17 @@ __device__ __forceinline__ float2 f2(float a, float b) { return make_float2(a, b
 
 constexpr int kBarBytes = 128;  // mbarriers live in the first 128 bytes
 
+// Compile-time tuning: resident threads per SM the register allocation aims
+// at (0 = compiler's choice) and the unroll of the j loop (4 j per step).
+#ifndef KHRR_FORCE_THREADS_PER_SM
+#define KHRR_FORCE_THREADS_PER_SM 0
+#endif
+#ifndef KHRR_FORCE_J_UNROLL
+#define KHRR_FORCE_J_UNROLL 1
+#endif
+constexpr int kThreadsPerSm = KHRR_FORCE_THREADS_PER_SM;
+constexpr int kJUnroll = KHRR_FORCE_J_UNROLL;
+
 // Kernel features (template bit mask).
 constexpr unsigned kUnif = 1;     // every body has the same softening: no h array
 constexpr unsigned kAcc = 2;      // accumulate accelerations
@@ -166,7 +177,7 @@ struct TileAcc<K, false> {
 };
 
 template <int NT, int K, int JT, int STAGES, unsigned F>
-__global__ void __launch_bounds__(NT) force_kernel(const ForceArgs a) {
+__global__ void __launch_bounds__(NT, (kThreadsPerSm > 0 ? kThreadsPerSm / NT : 1)) force_kernel(const ForceArgs a) {
     using S = ForceShape<NT, K, JT, STAGES, F>;
     constexpr bool UNIF = S::UNIF, ACC = S::ACC, PHI = S::PHI, TMASS = S::TMASS;
     constexpr bool PACKED = F & kPacked;
@@ -247,7 +258,7 @@ __global__ void __launch_bounds__(NT) force_kernel(const ForceArgs a) {
                 const float4* tz = tx + 2 * (JT / 4);
                 const float4* tm = tx + S::kOffM * (JT / 4);
                 const float4* th = tx + S::kOffH * (JT / 4);
-#pragma unroll 1
+#pragma unroll kJUnroll
                 for (int q4 = 0; q4 < JT / 4; ++q4) {
                     const float4 X = tx[q4], Y = ty[q4], Z = tz[q4];
                     const float4 M = TMASS ? make_float4(1.f, 1.f, 1.f, 1.f) : tm[q4];

@@ -129,4 +129,47 @@ cudaError_t launch_conservation(const double* pos, const double* vel, const doub
                                 double* out16, cudaStream_t s);
 int conservation_blocks(int64_t n);
 
+// ---- mesh.cu ------------------------------------------------------------------
+struct MeshGeom {
+    double lo[3];
+    double cs[3];
+    int g[3];
+};
+struct WaveConsts {
+    int nx;
+    double dx, dt, c, diss_base, diss_extra, sim_l, bc_l;
+};
+// FP32 stencil constants: per-axis sponge tables (device arrays of nx) and
+// cdt_half = c dt / 2, K = c^2 dt^2 / dx^2, A = 2 (1 - 3K), S = -c^2 dt^2 4 pi / dx^3.
+struct WaveF32 {
+    int nx;
+    float diss_base, cdt_half, K, A, S;
+    const float* sx;
+    const float* sy;
+    const float* sz;
+};
+// Bins n bodies: slots from counter (stride counter_stride); count2 (may be
+// NULL) receives the same counts; cell_mass (may be NULL) the mass deposit.
+cudaError_t launch_assign(const double* pos, int64_t n, const MeshGeom& m, int2* pci, int* counter,
+                          int counter_stride, int* count2, int count2_stride, const double* mass, double* cell_mass,
+                          cudaStream_t s);
+int64_t scan_block_count(int64_t ncells);
+// count (stride cstride) -> maxpbc (scan_block_count entries, inclusive block
+// totals), start (true exclusive scan) and start_ref (reference view); start
+// or start_ref may be NULL.
+cudaError_t launch_scan(const int* count, int cstride, int64_t ncells, int* maxpbc, int* start, int sstride,
+                        int* start_ref, int rstride, cudaStream_t s);
+cudaError_t launch_cell_phi(const double* phi, const int2* pci, const int* count, int cstride, int64_t n,
+                            double* cell_phi, cudaStream_t s);
+cudaError_t launch_wave_f64(double* phi_new, const double* phi, const double* phi_old, const double* mass,
+                            const WaveConsts& w, cudaStream_t s);
+cudaError_t launch_wave_f32(float* phi_new, const float* phi, const float* phi_old, const float* mass,
+                            const WaveF32& w, double* resid, cudaStream_t s);
+cudaError_t launch_acc_field(double* cell_acc, double* cell_acc_abs, const double* phi, int nx, double dx,
+                             cudaStream_t s);
+cudaError_t launch_apply(double* pacc, double* pval, const double* cacc, const double* cval, const int2* pci,
+                         int64_t n, cudaStream_t s);
+cudaError_t launch_deinterleave(const int2* pci, int64_t n, int* a, int* b, cudaStream_t s);
+cudaError_t launch_to_float(const double* src, float* dst, int64_t n, cudaStream_t s);
+
 }  // namespace khrr

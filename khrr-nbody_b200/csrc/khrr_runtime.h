@@ -101,6 +101,19 @@ struct khrr_ctx {
     khrr::ForcePlan kplan;
     int64_t kplan_n = -1;
 
+    // Mesh pipeline (khrr_bin / khrr_wave_solve).
+    bool has_bin = false;
+    khrr::MeshGeom mesh{};
+    int64_t ncells = 0;
+    khrr::DevBuf<int2> pci;                              // per padded body: {cell, slot}
+    khrr::DevBuf<int> mcount, mstart, mstart_ref, maxpbc, mtmp;
+    khrr::DevBuf<double> cell_mass, wave_resid;
+    khrr::DevBuf<float> wave_phi, wave_mass, wave_tab;   // 3 C, C, 3 nx
+    int wave_nx = 0;
+    int wave_rot = 0;                                    // which buffer holds phi^n
+    bool wave_warm = false;
+    std::map<std::pair<int, int>, khrr::StepGraph> wave_graphs;  // (chunk, rotation)
+
     // Timing.
     bool timing = false;
     cudaEvent_t ph0 = nullptr, ph1 = nullptr;  // placeholders captured in graphs

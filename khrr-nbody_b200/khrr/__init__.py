@@ -53,6 +53,37 @@ class Tuning(C.Structure):
     _fields_ = [(k, C.c_int) for k in ("threads", "i_per_thread", "j_tile", "j_split", "packed")]
 
 
+class Mesh(C.Structure):
+    _fields_ = [("lo", C.c_double * 3), ("cell", C.c_double * 3), ("grid", C.c_int * 3)]
+
+    @classmethod
+    def make(cls, lo, cell, grid):
+        m = cls()
+        for k in range(3):
+            m.lo[k], m.cell[k], m.grid[k] = float(lo[k]), float(cell[k]), int(grid[k])
+        return m
+
+
+class WaveParams(C.Structure):
+    _fields_ = [("nx", C.c_int)] + [(k, C.c_double) for k in (
+        "dx", "dt", "c", "diss_base", "diss_extra", "sim_l", "bc_l")]
+
+    @classmethod
+    def make(cls, nx, dx, c=4574.337022617616, dt=None, diss_base=0.1, diss_extra=0.01,
+             sim_l=None, bc_l=None):
+        """Constants as the reference derives them (nbody/src/nbody.cu:1134-1143)."""
+        if dt is None:
+            dt = 0.5 * dx / (c * np.sqrt(3.0))
+        if sim_l is None:
+            sim_l = 0.5 * nx * dx
+        if bc_l is None:
+            bc_l = sim_l / 10.0
+        return cls(int(nx), dx, dt, c, diss_base, diss_extra, sim_l, bc_l)
+
+SCAN_REFERENCE = 0
+SCAN_EXCLUSIVE = 1
+
+
 _lib = None
 
 
@@ -93,6 +124,14 @@ def lib(path: pathlib.Path | str | None = None) -> C.CDLL:
         "khrr_fp32_probe": ([vp, C.POINTER(d)], i),
         "khrr_set_accelerations": ([vp, vp], i),
         "khrr_accel_fp64_sample": ([vp, vp, i64, vp, vp], i),
+        "khrr_assign_particles_to_cells": ([vp, vp, i64, C.POINTER(Mesh), vp, vp, vp, vp, vp], i),
+        "khrr_compute_prefix_sums": ([vp, vp, vp, i64, i], i),
+        "khrr_cell_phi": ([vp, vp, vp, vp, i64, vp], i),
+        "khrr_wave_iteration": ([vp, vp, vp, vp, vp, C.POINTER(WaveParams)], i),
+        "khrr_acc_field": ([vp, vp, vp, vp, i, d], i),
+        "khrr_apply_cells_to_particles": ([vp, vp, vp, vp, vp, vp, i64], i),
+        "khrr_bin": ([vp, C.POINTER(Mesh), vp, vp, vp, vp, vp, vp], i),
+        "khrr_wave_solve": ([vp, C.POINTER(WaveParams), d, i, i, i, C.POINTER(i), C.POINTER(d), vp], i),
     }
     for name, (args, res) in sigs.items():
         fn = getattr(L, name)
@@ -276,3 +315,47 @@ class Context:
         t = C.c_double()
         self._check(self.L.khrr_fp32_probe(self.h, C.byref(t)))
         return t.value
+
+    # -- p2mesh ----------------------------------------------------------------
+    def assign_particles_to_cells(self, pos_ptr, n, mesh: Mesh, pci_ptr, cell_info_ptr,
+                                  cell_count_ptr=None, mass_ptr=None, cell_mass_ptr=None):
+        self._check(self.L.khrr_assign_particles_to_cells(self.h, pos_ptr, n, C.byref(mesh), pci_ptr,
+                                                          cell_info_ptr, cell_count_ptr, mass_ptr,
+                                                          cell_mass_ptr))
+
+    def compute_prefix_sums(self, cell_info_ptr, max_pbc_ptr, ncells, mode=SCAN_REFERENCE):
+        self._check(self.L.khrr_compute_prefix_sums(self.h, cell_info_ptr, max_pbc_ptr, ncells, mode))
+
+    def cell_phi(self, phi_ptr, pci_ptr, cell_info_ptr, n, cell_phi_ptr):
+        self._check(self.L.khrr_cell_phi(self.h, phi_ptr, pci_ptr, cell_info_ptr, n, cell_phi_ptr))
+
+    def wave_iteration(self, phi_new_ptr, phi_ptr, phi_old_ptr, mass_ptr, params: WaveParams):
+        self._check(self.L.khrr_wave_iteration(self.h, phi_new_ptr, phi_ptr, phi_old_ptr, mass_ptr,
+                                               C.byref(params)))
+
+    def acc_field(self, cell_acc_ptr, cell_acc_abs_ptr, cell_phi_ptr, nx, dx):
+        self._check(self.L.khrr_acc_field(self.h, cell_acc_ptr, cell_acc_abs_ptr, cell_phi_ptr, nx, dx))
+
+    def apply_cells_to_particles(self, pacc_ptr, pval_ptr, cacc_ptr, cval_ptr, pci_ptr, n):
+        self._check(self.L.khrr_apply_cells_to_particles(self.h, pacc_ptr, pval_ptr, cacc_ptr, cval_ptr,
+                                                         pci_ptr, n))
+
+    def bin(self, lo, cell, grid):
+        """Bin the uploaded bodies -> dict(cell_id, id_in_cell, count, start, start_ref, cell_mass)."""
+        m = Mesh.make(lo, cell, grid)
+        ncells = int(grid[0]) * int(grid[1]) * int(grid[2])
+        out = {"cell_id": np.empty(self.n, np.int32), "id_in_cell": np.empty(self.n, np.int32),
+               "count": np.empty(ncells, np.int32), "start": np.empty(ncells, np.int32),
+               "start_ref": np.empty(ncells, np.int32), "cell_mass": np.empty(ncells)}
+        self._check(self.L.khrr_bin(self.h, C.byref(m), *[_ptr(out[k]) for k in (
+            "cell_id", "id_in_cell", "count", "start", "start_ref", "cell_mass")]))
+        return out
+
+    def wave_solve(self, params: WaveParams, tol=1e-5, max_iter=1000, check_every=30, cold=False,
+                   want_phi=True):
+        it = C.c_int()
+        res = C.c_double()
+        phi = np.empty(params.nx ** 3, np.float32) if want_phi else None
+        self._check(self.L.khrr_wave_solve(self.h, C.byref(params), tol, max_iter, check_every,
+                                           1 if cold else 0, C.byref(it), C.byref(res), _ptr(phi)))
+        return it.value, res.value, phi

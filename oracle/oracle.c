@@ -419,12 +419,35 @@ void orc_wave_iter_f64(const orc_wave* W, double* phi_new, const double* phi,
             }
 }
 
-/* The same update in FP32 storage and arithmetic, with the per-cell
- * coefficients evaluated in FP64 and rounded once (the product's FP32 form). */
+/* The product's FP32 form of the same update.  The sponge is separable:
+ * diss = base + sx[ix] + sy[iy] + sz[iz], the per-axis terms of wave_diss
+ * evaluated in FP64 and rounded once (sz uses the y test, like z does in the
+ * reference).  Per interior cell, in FP32: Q = diss c dt/2, w = 1/(1 + Q),
+ * out = fma(nb, K w, fma(phi, A w, fma(phi_old, (Q - 1) w, mass (S w))))
+ * with nb the six-neighbour sum, K = c^2 dt^2/dx^2, A = 2(1 - 3K),
+ * S = -c^2 dt^2 4 pi/dx^3 (constants from FP64).  Algebraically the reference's
+ * KM, KA, KO, KF f terms; the FP32 rounding is the product's. */
 void orc_wave_iter_f32(const orc_wave* W, float* phi_new, const float* phi, const float* phi_old,
                        const float* mass) {
     const int NX = W->nx;
     const double DX = W->dx, C = W->c, DT = W->dt;
+    const double L = W->sim_l - W->bc_l;
+    float* sx = (float*)malloc(sizeof(float) * (size_t)NX);
+    float* sy = (float*)malloc(sizeof(float) * (size_t)NX);
+    for (int i = 0; i < NX; ++i) {
+        const double x = i * W->dx;
+        double a = 0.0, b = 0.0;
+        if (x > -L) a = W->diss_extra * fabs(x - L) * fabs(x - L);
+        else if (x < -L) a = W->diss_extra * fabs(x + L) * fabs(x + L);
+        if (x > L) b = W->diss_extra * fabs(x - L) * fabs(x - L);
+        else if (x < -L) b = W->diss_extra * fabs(x + L) * fabs(x + L);
+        sx[i] = (float)a;
+        sy[i] = (float)b;
+    }
+    const double K = C * C * (DT * DT) / (DX * DX);
+    const float base = (float)W->diss_base, cdt_half = (float)(C * DT * 0.5), Kf = (float)K;
+    const float Af = (float)(2.0 * (1.0 - 3.0 * K));
+    const float Sf = (float)(-(C * C) * (DT * DT) * (4.0 * ORC_PI) / (DX * DX * DX));
 #pragma omp parallel for collapse(2)
     for (int iz = 0; iz < NX; ++iz)
         for (int iy = 0; iy < NX; ++iy)
@@ -434,19 +457,16 @@ void orc_wave_iter_f32(const orc_wave* W, float* phi_new, const float* phi, cons
                     phi_new[at] = 0.0f;
                     continue;
                 }
-                const double diss = wave_diss(W, ix, iy, iz);
-                const double Q = diss * C * DT * 0.5;
-                const double Wt = 1 + Q;
-                const double K = C * C * (DT * DT) / (DX * DX);
-                const float KM = (float)(K / Wt);
-                const float KA = (float)(2 * (1. - 3 * K) / Wt);
-                const float KO = (float)((Q - 1.) / Wt);
-                const float KS = (float)(-(C * C) * (DT * DT) / Wt * (4 * ORC_PI) / (DX * DX * DX));
                 const float nb = ((phi[ORC_AT(ix - 1, iy, iz, NX)] + phi[ORC_AT(ix + 1, iy, iz, NX)]) +
                                   (phi[ORC_AT(ix, iy - 1, iz, NX)] + phi[ORC_AT(ix, iy + 1, iz, NX)])) +
                                  (phi[ORC_AT(ix, iy, iz - 1, NX)] + phi[ORC_AT(ix, iy, iz + 1, NX)]);
-                phi_new[at] = nb * KM + phi[at] * KA + phi_old[at] * KO + mass[at] * KS;
+                const float diss = ((base + sx[ix]) + sy[iy]) + sy[iz];
+                const float Q = diss * cdt_half;
+                const float w = 1.0f / (1.0f + Q);
+                phi_new[at] = fmaf(nb, Kf * w, fmaf(phi[at], Af * w, fmaf(phi_old[at], (Q - 1.0f) * w, mass[at] * (Sf * w))));
             }
+    free(sx);
+    free(sy);
 }
 
 /* acc_field (p2mesh-kernel.cuh:169-225) over the whole mesh: -grad(phi)/dx
