@@ -50,6 +50,7 @@ def parse():
     ap.add_argument("--impl", choices=["khrr", "reference"], default="khrr")
     ap.add_argument("--no-ensemble", action="store_true", help="skip the 64-galaxy batched-vs-plain leg")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-mesh", action="store_true", help="skip the p2mesh (binning, scan, wave) leg")
     ap.add_argument("--n-stars", type=int, default=N_STARS)
     ap.add_argument("--n-dm", type=int, default=N_DM)
     return ap.parse_args()
@@ -243,6 +244,64 @@ def ensemble_leg(khrr, ctx_device, torch, steps=8):
     return out
 
 
+def mesh_leg(khrr, device, torch, hbm_gbs):
+    """p2mesh on the configs' meshes: the two-galaxy encounter (786,432 bodies,
+    128^3 cells over [-4,4]^3, residual 1e-5) and the large system (2,097,152
+    bodies, 256^3 cells, residual 1e-6).  Algorithmic bytes: binning + mass
+    deposit + scan = 40 B per body (FP64 position and mass read, cell id and
+    slot written) + 24 B per cell (count and mass zeroed, count read, both
+    start views written); one FP32 stencil iteration = 16 B per cell (phi,
+    phi_old, mass read, phi_new written)."""
+    import ctypes as C
+    from khrr.galaxy import assemble, make_galaxy, two_galaxy_encounter
+    cases = {
+        "encounter_128": (lambda: two_galaxy_encounter(), 128, 4.0, 1e-5, 40000),
+        "large_256": (lambda: assemble([make_galaxy(698368, 1398784, 4000, eps_stars=0.002, eps_dm=0.002)],
+                                       [(0.0, (0, 0, 0), (0, 0, 0))]), 256, 4.0, 1e-6, 20000),
+    }
+    out = {}
+    ctx = khrr.Context(device)
+    try:
+        for label, (gen, nx, L, tol, max_iter) in cases.items():
+            pos, vel, mass, eps2 = gen()
+            n, ncells = len(mass), nx ** 3
+            ctx.upload(pos, vel, mass, eps2)
+            s = torch.cuda.ExternalStream(ctx.stream)
+            mesh = khrr.Mesh.make((-L,) * 3, (2 * L / nx,) * 3, (nx, nx, nx))
+            nul = [None] * 6
+            ctx._check(ctx.L.khrr_bin(ctx.h, C.byref(mesh), *nul))
+            best = 1e30
+            for _ in range(5):
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(s)
+                ctx._check(ctx.L.khrr_bin(ctx.h, C.byref(mesh), *nul))
+                e1.record(s)
+                e1.synchronize()
+                best = min(best, e0.elapsed_time(e1))
+            bin_bytes = 40.0 * n + 24.0 * ncells
+            W = khrr.WaveParams.make(nx, 2 * L / nx)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(s)
+            it, res, _ = ctx.wave_solve(W, tol=tol, max_iter=max_iter, check_every=50, cold=True, want_phi=False)
+            e1.record(s)
+            e1.synchronize()
+            wms = e0.elapsed_time(e1)
+            per_it = wms / max(it, 1)
+            wave_gbs = 16.0 * ncells / (per_it * 1e-3) / 1e9
+            out[label] = {
+                "bodies": n, "cells": ncells,
+                "bin_scan_deposit_ms": best, "bin_gbs": bin_bytes / (best * 1e-3) / 1e9,
+                "bin_frac_of_hbm": bin_bytes / (best * 1e-3) / 1e9 / hbm_gbs,
+                "wave_iterations": it, "wave_residual": res, "wave_ms_per_iteration": per_it,
+                "wave_gbs": wave_gbs, "wave_frac_of_hbm": wave_gbs / hbm_gbs,
+                "wave_working_set_mb": 16.0 * ncells / 1e6,
+                "wave_note": "L2-resident working set" if 16.0 * ncells < 126e6 else "HBM-resident",
+            }
+    finally:
+        ctx.close()
+    return out
+
+
 def run_khrr(args):
     import torch
     import khrr
@@ -351,6 +410,9 @@ def run_khrr(args):
     ens = None
     if not args.no_ensemble and rank == 0:
         ens = ensemble_leg(khrr, local, torch)
+    mesh = None
+    if not args.no_mesh and rank == 0:
+        mesh = mesh_leg(khrr, local, torch, float(peaks.get("hbm_gbs", 6650.0)))
     ctx.close()
 
     cpu = None
@@ -387,6 +449,7 @@ def run_khrr(args):
         "gpu_launches": 2 * args.steps,
         "clocks": clk.summary(),
         "ensemble": ens,
+        "mesh": mesh,
     }
     print(json.dumps(line), flush=True)
     return 0

@@ -190,6 +190,36 @@ def place(pos: np.ndarray, vel: np.ndarray, alpha_deg: float,
     return p, v
 
 
+def assemble(galaxies, placements):
+    """Reference memory layout of several galaxies (nbody/src/nbody.cu:1318-1417):
+    the stars of every galaxy first, then the dark matter of every galaxy,
+    each placed by ``place`` (tilt alpha_deg, centre, bulk velocity).
+    Returns (pos, vel, mass, eps2)."""
+    parts = {"s": [], "d": []}
+    for g, (alpha, centre, bulk) in zip(galaxies, placements):
+        if g.n_stars:
+            p, v = place(g.star_pos, g.star_vel, alpha, centre, bulk)
+            parts["s"].append((p, v, g.m_stars / g.n_stars, g.eps_stars, g.n_stars))
+        if g.n_dm:
+            p, v = place(g.dm_pos, g.dm_vel, alpha, centre, bulk)
+            parts["d"].append((p, v, g.m_dm / g.n_dm, g.eps_dm, g.n_dm))
+    seq = parts["s"] + parts["d"]
+    pos = np.concatenate([s[0] for s in seq])
+    vel = np.concatenate([s[1] for s in seq])
+    mass = np.concatenate([np.full(s[4], s[2]) for s in seq])
+    eps2 = np.concatenate([np.full(s[4], s[3] * s[3]) for s in seq])
+    return pos, vel, mass, eps2
+
+
+def two_galaxy_encounter(n_stars: int = 131072, n_dm: int = 262144, seed: int = 3000):
+    """Two generator galaxies centred at (+-1.5, 0, 0) with bulk velocities
+    (-+0.3, +-0.1, 0); the second is tilted by 30 degrees."""
+    g1 = make_galaxy(n_stars, n_dm, seed)
+    g2 = make_galaxy(n_stars, n_dm, seed + 1)
+    return assemble([g1, g2], [(0.0, (1.5, 0.0, 0.0), (-0.3, 0.1, 0.0)),
+                               (30.0, (-1.5, 0.0, 0.0), (0.3, -0.1, 0.0))])
+
+
 def round_to(n: int, m: int = 1024) -> int:
     return max(m, int(round(n / m)) * m)
 
