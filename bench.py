@@ -51,6 +51,7 @@ def parse():
     ap.add_argument("--no-ensemble", action="store_true", help="skip the 64-galaxy batched-vs-plain leg")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-mesh", action="store_true", help="skip the p2mesh (binning, scan, wave) leg")
+    ap.add_argument("--mesh-max-iter", type=int, default=0, help="cap on wave iterations (0 = to tolerance)")
     ap.add_argument("--n-stars", type=int, default=N_STARS)
     ap.add_argument("--n-dm", type=int, default=N_DM)
     return ap.parse_args()
@@ -244,7 +245,7 @@ def ensemble_leg(khrr, ctx_device, torch, steps=8):
     return out
 
 
-def mesh_leg(khrr, device, torch, hbm_gbs):
+def mesh_leg(khrr, device, torch, hbm_gbs, iter_cap=0):
     """p2mesh on the configs' meshes: the two-galaxy encounter (786,432 bodies,
     128^3 cells over [-4,4]^3, residual 1e-5) and the large system (2,097,152
     bodies, 256^3 cells, residual 1e-6).  Algorithmic bytes: binning + mass
@@ -282,6 +283,8 @@ def mesh_leg(khrr, device, torch, hbm_gbs):
             W = khrr.WaveParams.make(nx, 2 * L / nx)
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record(s)
+            if iter_cap > 0:
+                max_iter = min(max_iter, iter_cap)
             it, res, _ = ctx.wave_solve(W, tol=tol, max_iter=max_iter, check_every=50, cold=True, want_phi=False)
             e1.record(s)
             e1.synchronize()
@@ -412,7 +415,7 @@ def run_khrr(args):
         ens = ensemble_leg(khrr, local, torch)
     mesh = None
     if not args.no_mesh and rank == 0:
-        mesh = mesh_leg(khrr, local, torch, float(peaks.get("hbm_gbs", 6650.0)))
+        mesh = mesh_leg(khrr, local, torch, float(peaks.get("hbm_gbs", 6650.0)), args.mesh_max_iter)
     ctx.close()
 
     cpu = None

@@ -55,7 +55,9 @@ enum {
     KHRR_COMPAT_ACCUMULATE = 4, /* reference time loop: the step force is added to
                                    the previous step's (nbody.cu:1559-1566 never
                                    zeroes acct_); default overwrites             */
-    KHRR_PLAIN = 8,             /* one system per launch, no j-split (baseline)   */
+    KHRR_PLAIN = 8,             /* baseline: the conventional FP32 kernel (one i
+                                   body per thread, shared-memory j tiles), one
+                                   launch per system                              */
     KHRR_OVERWRITE = 16         /* kernel-level calls: overwrite instead of +=    */
 };
 

@@ -255,15 +255,25 @@ khrr_status khrr_ctx::enqueue_force(bool plain, bool acc, bool phi, bool events)
     // khrr_step points them at fresh timing events before each replay.
     if (events && (st = cuda(cudaEventRecordWithFlags(ph0, stream, cudaEventRecordExternal), "event")) != KHRR_OK)
         return st;
-    const size_t nsys = plain ? cnt.size() : 1;
-    for (size_t k = 0; k < nsys; ++k) {
-        const int b = plain ? p.sys_item_begin[k] : 0;
-        const int e = plain ? p.sys_item_begin[k + 1] : static_cast<int>(p.items.size());
-        if (e <= b) continue;
-        if ((st = cuda(cudaMemsetAsync(queue.p, 0, sizeof(unsigned), stream), "queue reset")) != KHRR_OK)
-            return st;
-        const int grid = std::min(e - b, ctas);
-        if ((st = cuda(launch_force(v, force_args(p, b, e), grid, stream), "force kernel")) != KHRR_OK)
+    if (plain) {
+        // The conventional baseline: one launch per system, one i body per thread.
+        for (size_t k = 0; k < cnt.size(); ++k) {
+            Shadow sh = shadow();
+            const int64_t o = poff[k];
+            sh.x += o;
+            sh.y += o;
+            sh.z += o;
+            sh.m += o;
+            sh.h += o;
+            if ((st = cuda(launch_plain_force(sh, static_cast<int>(cnt[k]), static_cast<int>(poff[k + 1] - o),
+                                              part.p + o, acc, phi, stream),
+                           "plain force kernel")) != KHRR_OK)
+                return st;
+        }
+    } else {
+        if ((st = cuda(cudaMemsetAsync(queue.p, 0, sizeof(unsigned), stream), "queue reset")) != KHRR_OK) return st;
+        const int e = static_cast<int>(p.items.size());
+        if ((st = cuda(launch_force(v, force_args(p, 0, e), std::min(e, ctas), stream), "force kernel")) != KHRR_OK)
             return st;
     }
     if (events && (st = cuda(cudaEventRecordWithFlags(ph1, stream, cudaEventRecordExternal), "event")) != KHRR_OK)

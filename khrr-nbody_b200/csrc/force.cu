@@ -439,6 +439,60 @@ const VariantTable& table() {
     return t;
 }
 
+// ---- the plain path ----------------------------------------------------------
+// The conventional one-system-per-launch FP32 kernel, the baseline the batched
+// persistent kernel is compared with: one i body per thread, 256-body j tiles
+// loaded cooperatively into shared memory, scalar FP32 pair terms, one CTA
+// per 256 i bodies, no j split.  Tile partials use the same compensated
+// running sum, so both paths have the same accuracy.
+template <bool ACC, bool PHI>
+__global__ void __launch_bounds__(256) plain_force_kernel(const Shadow sh, int n, int npad, double4* __restrict__ out) {
+    constexpr int T = 256;
+    __shared__ float4 tj[T];
+    __shared__ float th[T];
+    const int tid = threadIdx.x;
+    const int i = blockIdx.x * T + tid;
+    const bool valid = i < n;
+    const float nx = valid ? -sh.x[i] : 0.0f, ny = valid ? -sh.y[i] : 0.0f, nz = valid ? -sh.z[i] : 0.0f;
+    const float hi = valid ? sh.h[i] : 1.0f;
+    float hx = 0.f, lx = 0.f, hy = 0.f, ly = 0.f, hz = 0.f, lz = 0.f, hp = 0.f, lp = 0.f;
+    for (int j0 = 0; j0 < npad; j0 += T) {
+        const int j = j0 + tid;
+        if (j < npad) {
+            tj[tid] = make_float4(sh.x[j], sh.y[j], sh.z[j], sh.m[j]);
+            th[tid] = sh.h[j];
+        } else {
+            tj[tid] = make_float4(0.f, 0.f, 0.f, 0.f);
+            th[tid] = 1.0f;
+        }
+        __syncthreads();
+        float ax = 0.f, ay = 0.f, az = 0.f, pp = 0.f;
+#pragma unroll 8
+        for (int u = 0; u < T; ++u) {
+            const float4 b = tj[u];
+            const float dx = b.x + nx, dy = b.y + ny, dz = b.z + nz;
+            const float r2 = fmaf(dz, dz, fmaf(dy, dy, fmaf(dx, dx, hi + th[u])));
+            const float inv = rsqrt_approx(r2);
+            const float minv = b.w * inv;
+            if (ACC) {
+                const float f = minv * (inv * inv);
+                ax = fmaf(dx, f, ax);
+                ay = fmaf(dy, f, ay);
+                az = fmaf(dz, f, az);
+            }
+            if (PHI) pp += minv;
+        }
+        two_sum_into(hx, lx, ax);
+        two_sum_into(hy, ly, ay);
+        two_sum_into(hz, lz, az);
+        two_sum_into(hp, lp, pp);
+        __syncthreads();
+    }
+    if (valid)
+        out[i] = make_double4(static_cast<double>(hx) + lx, static_cast<double>(hy) + ly,
+                              static_cast<double>(hz) + lz, static_cast<double>(hp) + lp);
+}
+
 // ---- helpers around the force pass -----------------------------------------
 
 // FP64 AoS state -> SoA FP32 shadow; ghosts (i >= n) get zero mass at the
@@ -577,6 +631,16 @@ cudaError_t launch_force(const ForceVariant* v, const ForceArgs& a, int grid, cu
     ForceArgs args = a;
     void* params[] = {&args};
     return cudaLaunchKernel(v->fn, dim3(grid), dim3(v->threads), params, v->smem, s);
+}
+
+cudaError_t launch_plain_force(const Shadow& sh, int n, int npad, double4* out, bool acc, bool phi,
+                               cudaStream_t s) {
+    if (n < 1) return cudaSuccess;
+    const unsigned grid = static_cast<unsigned>((n + 255) / 256);
+    if (acc && phi) plain_force_kernel<true, true><<<grid, 256, 0, s>>>(sh, n, npad, out);
+    else if (acc) plain_force_kernel<true, false><<<grid, 256, 0, s>>>(sh, n, npad, out);
+    else plain_force_kernel<false, true><<<grid, 256, 0, s>>>(sh, n, npad, out);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_pack(const double* pos, const double* mass, const double* eps2, int64_t n,

@@ -80,6 +80,10 @@ const ForceVariant* force_variant(int idx);
 const ForceVariant* find_force_variant(int threads, int ipt, int jt, bool packed, bool unif,
                                        bool acc, bool phi, bool tile_mass = false);
 cudaError_t launch_force(const ForceVariant* v, const ForceArgs& a, int grid, cudaStream_t s);
+// The plain baseline: one system (shadow offset to it, n real bodies, npad
+// padded) in one launch, one i body per thread; writes partial slot 0.
+cudaError_t launch_plain_force(const Shadow& sh, int n, int npad, double4* out, bool acc, bool phi,
+                               cudaStream_t s);
 // FP64 AoS positions -> padded FP32 SoA shadow (x, y, z, m, eps2 / 2).
 cudaError_t launch_pack(const double* pos, const double* mass, const double* eps2, int64_t n,
                         int64_t npad, const Shadow& sh, cudaStream_t s);
