@@ -158,11 +158,15 @@ cudaError_t launch_assign(const double* pos, int64_t n, const MeshGeom& m, int2*
                           int counter_stride, int* count2, int count2_stride, const double* mass, double* cell_mass,
                           cudaStream_t s);
 int64_t scan_block_count(int64_t ncells);
-// count (stride cstride) -> maxpbc (scan_block_count entries, inclusive block
-// totals), start (true exclusive scan) and start_ref (reference view); start
-// or start_ref may be NULL.
-cudaError_t launch_scan(const int* count, int cstride, int64_t ncells, int* maxpbc, int* start, int sstride,
-                        int* start_ref, int rstride, cudaStream_t s);
+int64_t scan_scratch_ints(int64_t ncells);
+// Counts -> maxpbc (scan_block_count entries: inclusive scan of 512-cell block
+// totals) and starts: the true exclusive scan, or with ref_view the
+// reference's start_id (total of earlier 512-cell blocks).  pair: count points
+// at {count, start_id} pairs and the starts go to the .start_id fields (16-byte
+// aligned); else counts and starts are plain int arrays (start 16-byte
+// aligned).  scratch: scan_scratch_ints(ncells) ints.
+cudaError_t launch_scan(int* count, bool pair, int64_t ncells, int* maxpbc, int* start, bool ref_view, int* scratch,
+                        cudaStream_t s);
 cudaError_t launch_cell_phi(const double* phi, const int2* pci, const int* count, int cstride, int64_t n,
                             double* cell_phi, cudaStream_t s);
 cudaError_t launch_wave_f64(double* phi_new, const double* phi, const double* phi_old, const double* mass,

@@ -106,7 +106,7 @@ struct khrr_ctx {
     khrr::MeshGeom mesh{};
     int64_t ncells = 0;
     khrr::DevBuf<int2> pci;                              // per padded body: {cell, slot}
-    khrr::DevBuf<int> mcount, mstart, mstart_ref, maxpbc, mtmp;
+    khrr::DevBuf<int> mcount, mstart, maxpbc, mscan, mtmp;  // mscan: scan block/tile totals
     khrr::DevBuf<double> cell_mass, wave_resid;
     khrr::DevBuf<float> wave_phi, wave_mass, wave_tab;   // 3 C, C, 3 nx
     int wave_nx = 0;

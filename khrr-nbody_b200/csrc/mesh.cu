@@ -9,21 +9,19 @@
 //
 // Binning: the cell of a body is the reference's (IEEE FP64 division,
 // truncation toward zero, clamps, including the iz clamp to gridSize.y - 1 and
-// the id iz*gx*gy + iy*gz + ix).  Slots come from atomics aggregated per warp:
-// lanes of a warp that hit the same cell take consecutive slots with one
-// atomic (__match_any_sync), and their masses are summed by the group leader
-// before one FP64 atomic, so dense cells cost one atomic per warp instead of
-// one per body.
+// the id iz*gx*gy + iy*gz + ix).  Slots and the mass deposit come from one
+// atomic each per body (fused in one pass over the bodies).
 //
-// Scan: single pass over 4096-cell tiles in three launches (tile/block totals,
-// one CTA scanning the 512-cell block totals, per-tile downsweep).  The
-// inclusive block-total scan is exactly the reference's maxPBC array, and the
-// reference's start_id (the total of earlier 512-cell blocks, its in-block
-// scan being discarded) is read off it; the true exclusive scan is produced
-// alongside.
+// Scan: 4096-cell tiles in three launches (block and tile totals with 16-byte
+// loads, one CTA scanning the tile totals, per-tile downsweep with 16-byte
+// stores).  The inclusive block-total scan is exactly the reference's maxPBC
+// array, and the reference's start_id (the total of earlier 512-cell blocks,
+// its in-block scan being discarded) is read off it; the true exclusive scan
+// is the other mode.
 //
 // This file is built without FMA contraction: the FP64 kernels evaluate the
 // reference's expressions in IEEE double; the FP32 stencil uses explicit fmaf.
+#include <algorithm>
 #include <cmath>
 #include <cstdint>
 
@@ -59,41 +57,26 @@ __global__ void assign_kernel(const double* __restrict__ pos, int64_t n, const M
     const int iy = cell_axis(pos[3 * i + 1], m.lo[1], m.cs[1], m.g[1]);
     const int iz = cell_axis(pos[3 * i + 2], m.lo[2], m.cs[2], m.g[1]);
     const int c = iz * m.g[0] * m.g[1] + iy * m.g[2] + ix;
-
-    const unsigned lane = threadIdx.x & 31u;
-    const unsigned peers = __match_any_sync(__activemask(), c);
-    const unsigned leader = __ffs(peers) - 1u;
-    const int rank = __popc(peers & ((1u << lane) - 1u));
-    int base = 0;
-    if (lane == leader) {
-        const int k = __popc(peers);
-        base = atomicAdd(&counter[static_cast<int64_t>(c) * counter_stride], k);
-        if (count2) atomicAdd(&count2[static_cast<int64_t>(c) * count2_stride], k);
-    }
-    base = __shfl_sync(peers, base, leader);
-    pci[i] = make_int2(c, base + rank);
-
-    if (cell_mass) {
-        // Group sum in lane order, then one FP64 atomic per group.
-        double s = 0.0;
-        unsigned rest = peers;
-        const double mi = mass[i];
-        while (rest) {
-            const int src = __ffs(rest) - 1;
-            const double v = __shfl_sync(peers, mi, src);
-            s += v;
-            rest &= rest - 1u;
-        }
-        if (lane == leader) atomicAdd(&cell_mass[c], s);
-    }
+    // One atomic per body, as the reference does: bodies arrive in no
+    // spatial order, so warp-level aggregation finds almost no shared cells
+    // and its match/shuffle traffic costs more than it saves.
+    const int slot = atomicAdd(&counter[static_cast<int64_t>(c) * counter_stride], 1);
+    if (count2) atomicAdd(&count2[static_cast<int64_t>(c) * count2_stride], 1);
+    pci[i] = make_int2(c, slot);
+    if (cell_mass) atomicAdd(&cell_mass[c], mass[i]);
 }
 
 // ---- prefix sums -----------------------------------------------------------
+// Counts are read, and starts written, 16 bytes at a time: each thread owns 8
+// consecutive cells (stride 1: two int4; the reference's {count, start_id}
+// pairs: four int4).  Tiles of 4096 cells = 8 of the reference's 512-cell
+// blocks.
 constexpr int kScanThreads = 512;
 constexpr int kScanPer = 8;                              // cells per thread
 constexpr int kScanTile = kScanThreads * kScanPer;       // 4096 cells
 constexpr int kRefBlock = 512;                           // the reference's BLOCK_SIZE
 constexpr int kBlocksPerTile = kScanTile / kRefBlock;    // 8
+constexpr int kThreadsPerBlock = kRefBlock / kScanPer;   // 64
 
 __device__ __forceinline__ int warp_sum(int v) {
 #pragma unroll
@@ -101,19 +84,42 @@ __device__ __forceinline__ int warp_sum(int v) {
     return v;
 }
 
-// Totals of the 512-cell blocks of one 4096-cell tile.
-__global__ void scan_block_totals_kernel(const int* __restrict__ count, int stride, int64_t ncells,
-                                         int* __restrict__ block_tot) {
+// The 8 counts of a thread; cells past ncells read as 0.  PAIR: the counts
+// are the .x of {count, start_id} pairs.
+template <bool PAIR>
+__device__ __forceinline__ void load8(const int* __restrict__ count, int64_t c0, int64_t ncells, int (&v)[kScanPer]) {
+    if (c0 + kScanPer <= ncells) {
+        if (PAIR) {
+            const int4* p = reinterpret_cast<const int4*>(count + 2 * c0);
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const int4 a = p[q];
+                v[2 * q] = a.x;
+                v[2 * q + 1] = a.z;
+            }
+        } else {
+            const int4* p = reinterpret_cast<const int4*>(count + c0);
+            const int4 a = p[0], b = p[1];
+            v[0] = a.x, v[1] = a.y, v[2] = a.z, v[3] = a.w;
+            v[4] = b.x, v[5] = b.y, v[6] = b.z, v[7] = b.w;
+        }
+    } else {
+#pragma unroll
+        for (int k = 0; k < kScanPer; ++k) v[k] = c0 + k < ncells ? count[(c0 + k) * (PAIR ? 2 : 1)] : 0;
+    }
+}
+
+// K1: per tile, the totals of its 512-cell blocks and of the tile.
+template <bool PAIR>
+__global__ void __launch_bounds__(kScanThreads) scan_totals_kernel(const int* __restrict__ count, int64_t ncells,
+                                                                   int* __restrict__ block_tot, int* __restrict__ tile_tot) {
     const int64_t t = blockIdx.x;
     const int tid = threadIdx.x;
-    const int64_t c0 = t * kScanTile + static_cast<int64_t>(tid) * kScanPer;
+    int v[kScanPer];
+    load8<PAIR>(count, t * kScanTile + static_cast<int64_t>(tid) * kScanPer, ncells, v);
     int s = 0;
 #pragma unroll
-    for (int k = 0; k < kScanPer; ++k) {
-        const int64_t c = c0 + k;
-        if (c < ncells) s += count[c * stride];
-    }
-    // 64 threads = one 512-cell block = two warps.
+    for (int k = 0; k < kScanPer; ++k) s += v[k];
     s = warp_sum(s);
     __shared__ int ws[kScanThreads / 32];
     if ((tid & 31) == 0) ws[tid >> 5] = s;
@@ -122,48 +128,56 @@ __global__ void scan_block_totals_kernel(const int* __restrict__ count, int stri
         const int64_t b = t * kBlocksPerTile + tid;
         if (b * kRefBlock < ncells) block_tot[b] = ws[2 * tid] + ws[2 * tid + 1];
     }
+    if (tid == 0) {
+        int tot = 0;
+#pragma unroll
+        for (int w = 0; w < kScanThreads / 32; ++w) tot += ws[w];
+        tile_tot[t] = tot;
+    }
 }
 
-// One CTA: inclusive scan of the block totals (in place) = maxPBC.
-__global__ void scan_blocks_kernel(int* __restrict__ tot, int64_t nb) {
+// K2 (one CTA): tile totals -> exclusive tile offsets, in place.
+__global__ void __launch_bounds__(1024) scan_tiles_kernel(int* __restrict__ tile, int64_t ntiles) {
     constexpr int T = 1024;
     __shared__ int part[T];
     const int tid = threadIdx.x;
-    const int64_t per = (nb + T - 1) / T;
-    const int64_t b0 = tid * per;
-    int s = 0;
-    for (int64_t b = b0; b < b0 + per && b < nb; ++b) s += tot[b];
-    part[tid] = s;
-    __syncthreads();
-    for (int o = 1; o < T; o <<= 1) {  // Hillis-Steele inclusive scan of thread totals
-        const int v = tid >= o ? part[tid - o] : 0;
+    const int64_t per = (ntiles + T - 1) / T;
+    // Chunks of T tiles (coalesced), scanned in order with a running carry.
+    int carry = 0;
+    for (int64_t r = 0; r < per; ++r) {
+        const int64_t e = r * T + tid;
+        const int x = e < ntiles ? tile[e] : 0;
+        part[tid] = x;
         __syncthreads();
-        part[tid] += v;
+        for (int o = 1; o < T; o <<= 1) {
+            const int y = tid >= o ? part[tid - o] : 0;
+            __syncthreads();
+            part[tid] += y;
+            __syncthreads();
+        }
+        if (e < ntiles) tile[e] = carry + part[tid] - x;
+        const int total = part[T - 1];
         __syncthreads();
-    }
-    int run = tid ? part[tid - 1] : 0;
-    for (int64_t b = b0; b < b0 + per && b < nb; ++b) {
-        run += tot[b];
-        tot[b] = run;
+        carry += total;
     }
 }
 
-// Per tile: exclusive in-tile scan + tile offset -> the true start of every
-// cell; the reference view from maxPBC.
-__global__ void scan_downsweep_kernel(const int* __restrict__ count, int cstride, int64_t ncells,
-                                      const int* __restrict__ maxpbc, int* __restrict__ start, int sstride,
-                                      int* __restrict__ start_ref, int rstride) {
+// K3: per tile, maxPBC for its blocks (inclusive block-total scan), the true
+// exclusive start of every cell and/or the reference's start_id view.
+template <bool PAIR>
+__global__ void __launch_bounds__(kScanThreads) scan_downsweep_kernel(int* __restrict__ count, int64_t ncells,
+                                                                      const int* __restrict__ block_tot,
+                                                                      const int* __restrict__ tile_off,
+                                                                      int* __restrict__ maxpbc, int* __restrict__ start,
+                                                                      bool ref_view) {
     const int64_t t = blockIdx.x;
     const int tid = threadIdx.x;
     const int64_t c0 = t * kScanTile + static_cast<int64_t>(tid) * kScanPer;
     int v[kScanPer];
+    load8<PAIR>(count, c0, ncells, v);
     int s = 0;
 #pragma unroll
-    for (int k = 0; k < kScanPer; ++k) {
-        const int64_t c = c0 + k;
-        v[k] = c < ncells ? count[c * cstride] : 0;
-        s += v[k];
-    }
+    for (int k = 0; k < kScanPer; ++k) s += v[k];
     // Exclusive scan of the 512 thread totals.
     const int lane = tid & 31, w = tid >> 5;
     int incl = s;
@@ -173,6 +187,7 @@ __global__ void scan_downsweep_kernel(const int* __restrict__ count, int cstride
         if (lane >= o) incl += y;
     }
     __shared__ int wsum[kScanThreads / 32];
+    __shared__ int bsum[kBlocksPerTile];
     if (lane == 31) wsum[w] = incl;
     __syncthreads();
     if (w == 0) {
@@ -184,20 +199,48 @@ __global__ void scan_downsweep_kernel(const int* __restrict__ count, int cstride
         }
         if (lane < kScanThreads / 32) wsum[lane] = x;
     }
+    const int toff = tile_off[t];
+    if (tid < kBlocksPerTile) {
+        // maxPBC of this tile's blocks: tile offset + inclusive scan of its block totals.
+        const int64_t b0 = t * kBlocksPerTile;
+        int run = toff;
+        for (int q = 0; q <= tid; ++q)
+            if ((b0 + q) * kRefBlock < ncells) run += block_tot[b0 + q];
+        if ((b0 + tid) * kRefBlock < ncells) maxpbc[b0 + tid] = run;
+        bsum[tid] = run - ((b0 + tid) * kRefBlock < ncells ? block_tot[b0 + tid] : 0);  // exclusive: start of block
+    }
     __syncthreads();
-    const int tile_off = t > 0 ? maxpbc[t * kBlocksPerTile - 1] : 0;
-    int run = tile_off + (w > 0 ? wsum[w - 1] : 0) + (incl - s);
+    int out[kScanPer];
+    if (ref_view) {
+        // The reference's start_id: the total of all earlier 512-cell blocks.
+        const int r = bsum[tid / kThreadsPerBlock];
 #pragma unroll
-    for (int k = 0; k < kScanPer; ++k) {
-        const int64_t c = c0 + k;
-        if (c < ncells) {
-            if (start) start[c * sstride] = run;
-            if (start_ref) {
-                const int64_t b = c / kRefBlock;
-                start_ref[c * rstride] = b > 0 ? maxpbc[b - 1] : 0;
-            }
+        for (int k = 0; k < kScanPer; ++k) out[k] = r;
+    } else {
+        int run = toff + (w > 0 ? wsum[w - 1] : 0) + (incl - s);
+#pragma unroll
+        for (int k = 0; k < kScanPer; ++k) {
+            out[k] = run;
+            run += v[k];
         }
-        run += v[k];
+    }
+    if (c0 + kScanPer <= ncells) {
+        if (PAIR) {
+            int4* p = reinterpret_cast<int4*>(count + 2 * c0);
+#pragma unroll
+            for (int q = 0; q < 4; ++q) p[q] = make_int4(v[2 * q], out[2 * q], v[2 * q + 1], out[2 * q + 1]);
+        } else {
+            int4* p = reinterpret_cast<int4*>(start + c0);
+            p[0] = make_int4(out[0], out[1], out[2], out[3]);
+            p[1] = make_int4(out[4], out[5], out[6], out[7]);
+        }
+    } else {
+#pragma unroll
+        for (int k = 0; k < kScanPer; ++k) {
+            if (c0 + k >= ncells) break;
+            if (PAIR) count[2 * (c0 + k) + 1] = out[k];
+            else start[c0 + k] = out[k];
+        }
     }
 }
 
@@ -261,37 +304,73 @@ __global__ void wave_f64_kernel(double* __restrict__ phi_new, const double* __re
                   phi_old[at] * KO + f * KF;
 }
 
-// The same step in FP32 storage and arithmetic.  The sponge is separable,
+// The FP32 form of the step.  The sponge is separable,
 // diss = base + sx[ix] + sy[iy] + sz[iz] (per-axis tables built in FP64 on the
 // host); per cell: Q = diss c dt / 2, w = 1 / (1 + Q), and
 //   phi_new = nb K w + phi (2 (1 - 3K)) w + phi_old (Q - 1) w + mass S w,
 // with nb the six-neighbour sum and S = -c^2 dt^2 4 pi / dx^3.  With resid,
 // sum (phi_new - phi)^2 and sum phi_new^2 are accumulated in FP64.
-__global__ void wave_f32_kernel(float* __restrict__ phi_new, const float* __restrict__ phi,
-                                const float* __restrict__ phi_old, const float* __restrict__ mass,
-                                const WaveF32 W, double* __restrict__ resid) {
+// Each thread computes kWZ consecutive z cells of one (x, y) column: the
+// column's phi values are loaded once and shared as z neighbours, and all
+// other loads (x/y neighbours, phi_old, mass) are issued up front, so a warp
+// keeps many requests in flight (no barriers, no shared memory).  kWZ = 8 on
+// large meshes, 4 on small ones (more CTAs).
+constexpr int kWX = 32, kWY = 8;
+
+template <int kWZ>
+__global__ void __launch_bounds__(kWX * kWY) wave_f32_kernel(float* __restrict__ phi_new, const float* __restrict__ phi,
+                                                             const float* __restrict__ phi_old,
+                                                             const float* __restrict__ mass, const WaveF32 W,
+                                                             double* __restrict__ resid) {
     const int NX = W.nx;
-    const int ix = blockIdx.x * blockDim.x + threadIdx.x;
-    const int iy = blockIdx.y * blockDim.y + threadIdx.y;
-    const int iz = blockIdx.z;
+    const int ix = blockIdx.x * kWX + threadIdx.x, iy = blockIdx.y * kWY + threadIdx.y;
+    const int zb = blockIdx.z * kWZ;
+    const int64_t sy = NX, sz = static_cast<int64_t>(NX) * NX;
     double d2 = 0.0, n2 = 0.0;
     if (ix < NX && iy < NX) {
-        const int64_t at = at3(ix, iy, iz, NX);
-        float out = 0.0f;
-        const float c0 = phi[at];
-        if (!(ix == 0 || ix == NX - 1 || iy == 0 || iy == NX - 1 || iz == 0 || iz == NX - 1)) {
-            const int64_t sy = NX, sz = static_cast<int64_t>(NX) * NX;
-            const float nb = ((phi[at - 1] + phi[at + 1]) + (phi[at - sy] + phi[at + sy])) + (phi[at - sz] + phi[at + sz]);
-            const float diss = ((W.diss_base + W.sx[ix]) + W.sy[iy]) + W.sz[iz];
-            const float Q = diss * W.cdt_half;
-            const float w = 1.0f / (1.0f + Q);
-            out = fmaf(nb, W.K * w, fmaf(c0, W.A * w, fmaf(phi_old[at], (Q - 1.0f) * w, mass[at] * (W.S * w))));
+        const int64_t col = static_cast<int64_t>(iy) * NX + ix;
+        // Neighbour offsets clamped into the mesh, so every load below is
+        // unconditional and in bounds (face cells discard their values).
+        const int64_t dxm = ix > 0 ? 1 : 0, dxp = ix < NX - 1 ? 1 : 0;
+        const int64_t dym = iy > 0 ? sy : 0, dyp = iy < NX - 1 ? sy : 0;
+        float c[kWZ + 2];  // phi at z = zb - 1 .. zb + kWZ (clamped into the mesh)
+        float xm[kWZ], xp[kWZ], ym[kWZ], yp[kWZ], po[kWZ], ms[kWZ];
+#pragma unroll
+        for (int u = 0; u < kWZ + 2; ++u) {
+            const int z = min(max(zb - 1 + u, 0), NX - 1);
+            c[u] = phi[z * sz + col];
         }
-        phi_new[at] = out;
-        if (resid) {
-            const double dd = static_cast<double>(out) - static_cast<double>(c0);
-            d2 = dd * dd;
-            n2 = static_cast<double>(out) * static_cast<double>(out);
+#pragma unroll
+        for (int u = 0; u < kWZ; ++u) {
+            const int64_t at = min(zb + u, NX - 1) * sz + col;
+            xm[u] = phi[at - dxm];
+            xp[u] = phi[at + dxp];
+            ym[u] = phi[at - dym];
+            yp[u] = phi[at + dyp];
+            po[u] = phi_old[at];
+            ms[u] = mass[at];
+        }
+        const bool edge_xy = ix == 0 || ix == NX - 1 || iy == 0 || iy == NX - 1;
+        const float sxy = (W.diss_base + W.sx[ix]) + W.sy[iy];
+#pragma unroll
+        for (int u = 0; u < kWZ; ++u) {
+            const int z = zb + u;
+            if (z >= NX) break;
+            const int64_t at = z * sz + col;
+            float out = 0.0f;
+            if (!(edge_xy || z == 0 || z == NX - 1)) {
+                const float nb = ((xm[u] + xp[u]) + (ym[u] + yp[u])) + (c[u] + c[u + 2]);
+                const float diss = sxy + W.sz[z];
+                const float Q = diss * W.cdt_half;
+                const float w = 1.0f / (1.0f + Q);
+                out = fmaf(nb, W.K * w, fmaf(c[u + 1], W.A * w, fmaf(po[u], (Q - 1.0f) * w, ms[u] * (W.S * w))));
+            }
+            phi_new[at] = out;
+            if (resid) {
+                const double dd = static_cast<double>(out) - static_cast<double>(c[u + 1]);
+                d2 += dd * dd;
+                n2 += static_cast<double>(out) * static_cast<double>(out);
+            }
         }
     }
     if (resid) {
@@ -300,7 +379,7 @@ __global__ void wave_f32_kernel(float* __restrict__ phi_new, const float* __rest
             d2 += __shfl_xor_sync(0xffffffffu, d2, o);
             n2 += __shfl_xor_sync(0xffffffffu, n2, o);
         }
-        if ((threadIdx.x & 31) == 0) {
+        if (threadIdx.x == 0) {
             atomicAdd(&resid[0], d2);
             atomicAdd(&resid[1], n2);
         }
@@ -374,14 +453,25 @@ cudaError_t launch_assign(const double* pos, int64_t n, const MeshGeom& m, int2*
 
 int64_t scan_block_count(int64_t ncells) { return (ncells + kRefBlock - 1) / kRefBlock; }
 
-cudaError_t launch_scan(const int* count, int cstride, int64_t ncells, int* maxpbc, int* start, int sstride,
-                        int* start_ref, int rstride, cudaStream_t s) {
+int64_t scan_scratch_ints(int64_t ncells) {
+    return scan_block_count(ncells) + (ncells + kScanTile - 1) / kScanTile;
+}
+
+cudaError_t launch_scan(int* count, bool pair, int64_t ncells, int* maxpbc, int* start, bool ref_view, int* scratch,
+                        cudaStream_t s) {
     if (ncells < 1) return cudaSuccess;
     const int64_t tiles = (ncells + kScanTile - 1) / kScanTile;
-    scan_block_totals_kernel<<<static_cast<unsigned>(tiles), kScanThreads, 0, s>>>(count, cstride, ncells, maxpbc);
-    scan_blocks_kernel<<<1, 1024, 0, s>>>(maxpbc, scan_block_count(ncells));
-    scan_downsweep_kernel<<<static_cast<unsigned>(tiles), kScanThreads, 0, s>>>(count, cstride, ncells, maxpbc, start,
-                                                                              sstride, start_ref, rstride);
+    int* block_tot = scratch;
+    int* tile_tot = scratch + scan_block_count(ncells);
+    const unsigned g = static_cast<unsigned>(tiles);
+    if (pair) scan_totals_kernel<true><<<g, kScanThreads, 0, s>>>(count, ncells, block_tot, tile_tot);
+    else scan_totals_kernel<false><<<g, kScanThreads, 0, s>>>(count, ncells, block_tot, tile_tot);
+    scan_tiles_kernel<<<1, 1024, 0, s>>>(tile_tot, tiles);
+    if (pair)
+        scan_downsweep_kernel<true><<<g, kScanThreads, 0, s>>>(count, ncells, block_tot, tile_tot, maxpbc, start, ref_view);
+    else
+        scan_downsweep_kernel<false><<<g, kScanThreads, 0, s>>>(count, ncells, block_tot, tile_tot, maxpbc, start,
+                                                                ref_view);
     return cudaGetLastError();
 }
 
@@ -401,8 +491,14 @@ cudaError_t launch_wave_f64(double* phi_new, const double* phi, const double* ph
 
 cudaError_t launch_wave_f32(float* phi_new, const float* phi, const float* phi_old, const float* mass,
                             const WaveF32& w, double* resid, cudaStream_t s) {
-    const dim3 block(32, 8), grid((w.nx + 31) / 32, (w.nx + 7) / 8, w.nx);
-    wave_f32_kernel<<<grid, block, 0, s>>>(phi_new, phi, phi_old, mass, w, resid);
+    const dim3 block(kWX, kWY);
+    if (w.nx >= 192) {
+        const dim3 grid((w.nx + kWX - 1) / kWX, (w.nx + kWY - 1) / kWY, (w.nx + 7) / 8);
+        wave_f32_kernel<8><<<grid, block, 0, s>>>(phi_new, phi, phi_old, mass, w, resid);
+    } else {
+        const dim3 grid((w.nx + kWX - 1) / kWX, (w.nx + kWY - 1) / kWY, (w.nx + 3) / 4);
+        wave_f32_kernel<4><<<grid, block, 0, s>>>(phi_new, phi, phi_old, mass, w, resid);
+    }
     return cudaGetLastError();
 }
 

@@ -122,9 +122,12 @@ khrr_status khrr_compute_prefix_sums(khrr_ctx* c, int* cell_info, int* max_pbc, 
     if (ncells < 1 || ncells > 0x7fffffffLL || !cell_info || !max_pbc ||
         (mode != KHRR_SCAN_REFERENCE && mode != KHRR_SCAN_EXCLUSIVE))
         return c->fail(KHRR_ERR_INVALID_ARG, "bad prefix-sum arguments");
-    int* start = cell_info + 1;
-    return c->cuda(launch_scan(cell_info, 2, ncells, max_pbc, mode == KHRR_SCAN_EXCLUSIVE ? start : nullptr, 2,
-                               mode == KHRR_SCAN_REFERENCE ? start : nullptr, 2, c->stream),
+    if (reinterpret_cast<uintptr_t>(cell_info) % 16)
+        return c->fail(KHRR_ERR_INVALID_ARG, "cell_info must be 16-byte aligned");
+    khrr_status st = c->cuda(c->mtmp.ensure(static_cast<size_t>(scan_scratch_ints(ncells))), "alloc");
+    if (st != KHRR_OK) return st;
+    return c->cuda(launch_scan(cell_info, true, ncells, max_pbc, nullptr, mode == KHRR_SCAN_REFERENCE, c->mtmp.p,
+                               c->stream),
                    "prefix sums");
 }
 
@@ -178,7 +181,7 @@ khrr_status khrr_bin(khrr_ctx* c, const khrr_mesh* mesh, int* cell_id, int* id_i
     const size_t np = static_cast<size_t>(c->npad);
     if ((st = c->cuda(c->pci.ensure(np), "alloc")) != KHRR_OK) return st;
     if ((st = c->cuda(c->mtmp.ensure(2 * np), "alloc")) != KHRR_OK) return st;
-    for (DevBuf<int>* b : {&c->mcount, &c->mstart, &c->mstart_ref})
+    for (DevBuf<int>* b : {&c->mcount, &c->mstart})
         if ((st = c->cuda(b->ensure(static_cast<size_t>(C)), "alloc")) != KHRR_OK) return st;
     if ((st = c->cuda(c->maxpbc.ensure(static_cast<size_t>(scan_block_count(C))), "alloc")) != KHRR_OK) return st;
     if ((st = c->cuda(c->cell_mass.ensure(static_cast<size_t>(C)), "alloc")) != KHRR_OK) return st;
@@ -192,7 +195,8 @@ khrr_status khrr_bin(khrr_ctx* c, const khrr_mesh* mesh, int* cell_id, int* id_i
                           "assign")) != KHRR_OK)
             return st;
     }
-    if ((st = c->cuda(launch_scan(c->mcount.p, 1, C, c->maxpbc.p, c->mstart.p, 1, c->mstart_ref.p, 1, s), "scan")) !=
+    if ((st = c->cuda(c->mscan.ensure(static_cast<size_t>(scan_scratch_ints(C))), "alloc")) != KHRR_OK) return st;
+    if ((st = c->cuda(launch_scan(c->mcount.p, false, C, c->maxpbc.p, c->mstart.p, false, c->mscan.p, s), "scan")) !=
         KHRR_OK)
         return st;
     c->mesh = g;
@@ -216,14 +220,23 @@ khrr_status khrr_bin(khrr_ctx* c, const khrr_mesh* mesh, int* cell_id, int* id_i
         return st;
     if (start && (st = c->cuda(cudaMemcpyAsync(start, c->mstart.p, cb, cudaMemcpyDeviceToHost, s), "download")) != KHRR_OK)
         return st;
-    if (start_ref &&
-        (st = c->cuda(cudaMemcpyAsync(start_ref, c->mstart_ref.p, cb, cudaMemcpyDeviceToHost, s), "download")) != KHRR_OK)
-        return st;
+    // The reference's start_id view is a function of maxPBC alone (the total
+    // of all earlier 512-cell blocks): expanded on the host when asked for.
+    std::vector<int> mp;
+    if (start_ref) {
+        mp.resize(static_cast<size_t>(scan_block_count(C)));
+        if ((st = c->cuda(cudaMemcpyAsync(mp.data(), c->maxpbc.p, mp.size() * sizeof(int), cudaMemcpyDeviceToHost, s),
+                          "download")) != KHRR_OK)
+            return st;
+    }
     if (cell_mass && (st = c->cuda(cudaMemcpyAsync(cell_mass, c->cell_mass.p, static_cast<size_t>(C) * sizeof(double),
                                                    cudaMemcpyDeviceToHost, s),
                                    "download")) != KHRR_OK)
         return st;
-    return khrr_synchronize(c);
+    if ((st = khrr_synchronize(c)) != KHRR_OK) return st;
+    if (start_ref)
+        for (int64_t cell = 0; cell < C; ++cell) start_ref[cell] = cell >= 512 ? mp[cell / 512 - 1] : 0;
+    return KHRR_OK;
 }
 
 khrr_status khrr_wave_solve(khrr_ctx* c, const khrr_wave_params* p, double tol, int max_iter, int check_every,
