@@ -196,6 +196,67 @@ khrr_status khrr_wave_solve(khrr_ctx* ctx, const khrr_wave_params* p, double tol
                             int check_every, int cold, int* iters, double* resid,
                             float* phi_out);
 
+/* Potential per cell of the last khrr_bin: cell_phi[c] += phi_i / count[c]
+ * over the uploaded bodies (computeCellPhiUnsorted, p2mesh-kernel.cuh:152-167)
+ * with phi from the last KHRR_PHI evaluation.  The sums persist in the
+ * context and accumulate over calls, as the reference's cell_phi_curr_ does
+ * (nbody.cu:1628-1634); reset != 0 clears them first.  cell_phi (host, C,
+ * may be NULL) receives the sums. */
+khrr_status khrr_bin_cell_phi(khrr_ctx* ctx, int reset, double* cell_phi);
+
+/* ---- drop-in file surface (host only; no device work) ------------------- */
+/* One entry of __start_galaxies.ini (GalaxyProperties, parse.cuh:19-62).
+ * n_star / n_dark are the bodies the reference loads: a component of zero
+ * mass has none (parse.cuh:33-42); the per-body mass is M / n. */
+typedef struct khrr_galaxy {
+    int n_star, n_dark;
+    double m_star, m_dark;
+    double eps_star, eps_dark;
+    double angle_deg;
+    double centre[3];
+    double vel[3];
+} khrr_galaxy;
+
+/* read_galaxy_properties (parse.cuh:320-367): the galaxy count, then per
+ * galaxy its id, "Ns,Ndm", "Ms,Mdm", "eps_s,eps_dm", alpha, "X,Y,Z",
+ * "Vx,Vy,Vz", each value followed by a comment to the end of the line. */
+khrr_status khrr_read_galaxies_ini(const char* path, khrr_galaxy* out, int max, int* count);
+/* read_start_info (nbody.cu:961-984): i_cont, tmax, dt_save. */
+khrr_status khrr_read_start_nbody_ini(const char* path, int* i_cont, double* tmax, double* dt_save);
+/* __gr_par.ini (nbody.cu:1080-1106): Mh, a, Rh, Mb, b, Rb, eps, dtgrav, K_m,
+ * K_r (any output pointer may be NULL). */
+khrr_status khrr_read_gr_par_ini(const char* path, khrr_field_params* field, double* eps, double* dtgrav,
+                                 double* K_m, double* K_r);
+/* __GPUs.ini: nGPU then nGPU device ids, one per line. */
+khrr_status khrr_read_gpus_ini(const char* path, int* ngpu, int* devices, int max);
+/* start_S{k}.txt / start_DM{k}.txt (nbody.cu:1331-1341): "N t" then N lines
+ * "x y z vx vy vz".  Reads up to max bodies (n = bodies read). */
+khrr_status khrr_read_start_txt(const char* path, int64_t max, double* pos, double* vel, int64_t* n,
+                                double* t);
+khrr_status khrr_write_start_txt(const char* path, int64_t n, const double* pos, const double* vel,
+                                 double t);
+/* S_/DM_ snapshots (print_particles_bin, nbody.cu:726-755): int32 count,
+ * f64 t, count x {x y z vx vy vz} f64, little-endian, no padding. */
+khrr_status khrr_write_snapshot(const char* path, int32_t count, double t, const double* pos,
+                                const double* vel);
+khrr_status khrr_read_snapshot(const char* path, int64_t max, double* pos, double* vel, int32_t* count,
+                               double* t);
+/* LIE_0.bin (nbody.cu:844-848): L0 (3 f64), Imp0 (3 f64), E0 (f64) and 16
+ * padding bytes (the reference writes E0 with sizeof(double3); written as
+ * zeros here).  The reader fills L, Imp and E. */
+khrr_status khrr_write_lie0(const char* path, const khrr_lie* lie0);
+khrr_status khrr_read_lie0(const char* path, khrr_lie* lie0);
+/* The initial-condition load of run() (nbody.cu:1315-1421): for every galaxy
+ * with stars, start_S{k}.txt from dir, then for every galaxy with dark
+ * matter start_DM{k}.txt; each body placed by the galaxy's tilt and shift
+ * exactly as the reference does (including its use of the already updated x
+ * for z, a shear for alpha != 0), masses M/n and eps2 = eps^2.  Layout: the
+ * stars of all galaxies, then the dark matter of all galaxies.  n and
+ * n_star_total receive the counts. */
+khrr_status khrr_load_initial_conditions(const char* dir, const khrr_galaxy* g, int ngal, int64_t max,
+                                         double* pos, double* vel, double* mass, double* eps2, int64_t* n,
+                                         int64_t* n_star_total);
+
 /* Largest n khrr_accel_noalloc accepts. */
 #define KHRR_NOALLOC_MAX_BODIES 32768
 /* khrr_accel without any device allocation.  This entry point has no

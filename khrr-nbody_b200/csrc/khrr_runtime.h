@@ -107,7 +107,8 @@ struct khrr_ctx {
     int64_t ncells = 0;
     khrr::DevBuf<int2> pci;                              // per padded body: {cell, slot}
     khrr::DevBuf<int> mcount, mstart, maxpbc, mscan, mtmp;  // mscan: scan block/tile totals
-    khrr::DevBuf<double> cell_mass, wave_resid;
+    khrr::DevBuf<double> cell_mass, cell_phi, wave_resid;
+    int64_t cell_phi_cells = 0;                          // mesh size the cell_phi sums belong to
     khrr::DevBuf<float> wave_phi, wave_mass, wave_tab;   // 3 C, C, 3 nx
     int wave_nx = 0;
     int wave_rot = 0;                                    // which buffer holds phi^n

@@ -239,6 +239,30 @@ khrr_status khrr_bin(khrr_ctx* c, const khrr_mesh* mesh, int* cell_id, int* id_i
     return KHRR_OK;
 }
 
+khrr_status khrr_bin_cell_phi(khrr_ctx* c, int reset, double* cell_phi) {
+    if (!c) return KHRR_ERR_INVALID_ARG;
+    if (!c->has_bin) return c->fail(KHRR_ERR_STATE, "no binned bodies (call khrr_bin first)");
+    const size_t C = static_cast<size_t>(c->ncells);
+    khrr_status st;
+    cudaStream_t s = c->stream;
+    if (reset || c->cell_phi_cells != c->ncells) {  // a new mesh starts from zero
+        if ((st = c->cuda(c->cell_phi.ensure(C), "alloc")) != KHRR_OK) return st;
+        cudaMemsetAsync(c->cell_phi.p, 0, C * sizeof(double), s);
+        c->cell_phi_cells = c->ncells;
+    }
+    for (size_t k = 0; k < c->cnt.size(); ++k) {
+        const int64_t o = c->poff[k];
+        if ((st = c->cuda(launch_cell_phi(c->phi.p + o, c->pci.p + o, c->mcount.p, 1, c->cnt[k], c->cell_phi.p, s),
+                          "cell phi")) != KHRR_OK)
+            return st;
+    }
+    if (cell_phi &&
+        (st = c->cuda(cudaMemcpyAsync(cell_phi, c->cell_phi.p, C * sizeof(double), cudaMemcpyDeviceToHost, s),
+                      "download")) != KHRR_OK)
+        return st;
+    return khrr_synchronize(c);
+}
+
 khrr_status khrr_wave_solve(khrr_ctx* c, const khrr_wave_params* p, double tol, int max_iter, int check_every,
                             int cold, int* iters, double* resid, float* phi_out) {
     if (!c) return KHRR_ERR_INVALID_ARG;

@@ -132,6 +132,21 @@ def lib(path: pathlib.Path | str | None = None) -> C.CDLL:
         "khrr_apply_cells_to_particles": ([vp, vp, vp, vp, vp, vp, i64], i),
         "khrr_bin": ([vp, C.POINTER(Mesh), vp, vp, vp, vp, vp, vp], i),
         "khrr_wave_solve": ([vp, C.POINTER(WaveParams), d, i, i, i, C.POINTER(i), C.POINTER(d), vp], i),
+        "khrr_bin_cell_phi": ([vp, i, vp], i),
+        "khrr_accel_noalloc": ([vp, vp, vp, vp, vp, i64, i, vp], i),
+        # host-only file surface
+        "khrr_read_galaxies_ini": ([C.c_char_p, vp, i, C.POINTER(i)], i),
+        "khrr_read_start_nbody_ini": ([C.c_char_p, C.POINTER(i), C.POINTER(d), C.POINTER(d)], i),
+        "khrr_read_gr_par_ini": ([C.c_char_p, vp, C.POINTER(d), C.POINTER(d), C.POINTER(d), C.POINTER(d)], i),
+        "khrr_read_gpus_ini": ([C.c_char_p, C.POINTER(i), vp, i], i),
+        "khrr_read_start_txt": ([C.c_char_p, i64, vp, vp, C.POINTER(i64), C.POINTER(d)], i),
+        "khrr_write_start_txt": ([C.c_char_p, i64, vp, vp, d], i),
+        "khrr_write_snapshot": ([C.c_char_p, C.c_int32, d, vp, vp], i),
+        "khrr_read_snapshot": ([C.c_char_p, i64, vp, vp, C.POINTER(C.c_int32), C.POINTER(d)], i),
+        "khrr_write_lie0": ([C.c_char_p, vp], i),
+        "khrr_read_lie0": ([C.c_char_p, vp], i),
+        "khrr_load_initial_conditions": ([C.c_char_p, vp, i, i64, vp, vp, vp, vp, C.POINTER(i64),
+                                          C.POINTER(i64)], i),
     }
     for name, (args, res) in sigs.items():
         fn = getattr(L, name)
