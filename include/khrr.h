@@ -58,7 +58,10 @@ enum {
     KHRR_PLAIN = 8,             /* baseline: the conventional FP32 kernel (one i
                                    body per thread, shared-memory j tiles), one
                                    launch per system                              */
-    KHRR_OVERWRITE = 16         /* kernel-level calls: overwrite instead of +=    */
+    KHRR_OVERWRITE = 16,        /* kernel-level calls: overwrite instead of +=    */
+    KHRR_MESH = 32              /* khrr_forces / khrr_step: forces from the mesh
+                                   solver (khrr_set_mesh_solver), the reference's
+                                   Wave mode, instead of the direct sum          */
 };
 
 /* Analytic halo + bulge parameters (__gr_par.ini lines 1-6); the derived
@@ -203,6 +206,61 @@ khrr_status khrr_wave_solve(khrr_ctx* ctx, const khrr_wave_params* p, double tol
  * (nbody.cu:1628-1634); reset != 0 clears them first.  cell_phi (host, C,
  * may be NULL) receives the sums. */
 khrr_status khrr_bin_cell_phi(khrr_ctx* ctx, int reset, double* cell_phi);
+
+/* ---- p2mesh beyond the reference's NGP path ------------------------------ */
+/* Mass assignment schemes of the mesh solver and the CIC entry points. */
+enum {
+    KHRR_ASSIGN_NGP = 0, /* nearest grid point: the reference's cell of each body */
+    KHRR_ASSIGN_CIC = 1  /* cloud in cell: trilinear weights about cell centres     */
+};
+
+/* Cloud-in-cell deposit (no counterpart in the reference, whose deposit is
+ * NGP, computeCellMassesUnsorted, p2mesh-kernel.cuh:126-137): each body
+ * spreads its mass over the 8 cells around u = (x - lo)/cell - 1/2 with
+ * weights (1 - f, f) per axis (f = u - floor(u)); corners outside the mesh
+ * are dropped.  Device pointers: pos n double3, mass n, cell_mass C
+ * (accumulated into, FP64 atomics).  Cubic meshes only. */
+khrr_status khrr_cic_deposit(khrr_ctx* ctx, const double* pos, const double* mass, int64_t n,
+                             const khrr_mesh* mesh, double* cell_mass);
+/* Cloud-in-cell interpolation, the gather matching khrr_cic_deposit (the
+ * reference's NGP gathers are apply_acceleration_to_particles /
+ * apply_cell_to_particles, p2mesh-kernel.cuh:227-254): particle_acc (n
+ * double3) = sum w cell_acc (C double3), particle_value (n) = sum w
+ * cell_value (C); either output may be NULL. */
+khrr_status khrr_cic_gather(khrr_ctx* ctx, const double* pos, int64_t n, const khrr_mesh* mesh,
+                            const double* cell_acc, const double* cell_value,
+                            double* particle_acc, double* particle_value);
+/* The int32 cell-index prefix-sum sort of the last khrr_bin (the reference
+ * computes start_id and id_in_cell, p2mesh-kernel.cuh:11-123, but never
+ * reorders): order[start[cell_i] + id_in_cell_i] = i, bodies numbered as
+ * uploaded (all systems).  Within a cell bodies follow their slot, the
+ * atomic order of id_in_cell.  order (host, n ints) may be NULL: the order
+ * then stays on the device only. */
+khrr_status khrr_sort_by_cell(khrr_ctx* ctx, int* order);
+
+/* The mesh-force solver: the reference's Wave mode (nbody.cu:1449-1472 at
+ * setup, 1540-1558 per step; it is compiled there but switched off by
+ * solver = NBodySolver::Nbody, nbody.cu:1132).  The mesh is the wave grid:
+ * wave.nx^3 cells of size wave.dx over [-nx dx/2, nx dx/2]^3.  Per force
+ * evaluation: zero and deposit the masses (NGP, the reference's, or CIC) at
+ * the positions the force is wanted at, run `iters_per_step` stencil
+ * iterations continuing from the previous field (the reference's
+ * (int)(dtgrav / dt_wave)), take -grad(phi) (acc_field with its 3-D launch)
+ * and gather acceleration and potential to the bodies.  khrr_forces with
+ * KHRR_MESH starts from a zero field and runs `setup_iters` iterations (the
+ * reference's 20000).  fp64 != 0 runs the reference's FP64 stencil, else the
+ * FP32 one.  NULL switches the solver off. */
+typedef struct khrr_mesh_solver {
+    khrr_wave_params wave;
+    int assign;          /* KHRR_ASSIGN_NGP or KHRR_ASSIGN_CIC */
+    int fp64;
+    int iters_per_step;
+    int setup_iters;
+} khrr_mesh_solver;
+khrr_status khrr_set_mesh_solver(khrr_ctx* ctx, const khrr_mesh_solver* solver);
+/* The mesh solver's potential field (nx^3, host, FP64; from the FP32 field
+ * when fp64 == 0), e.g. for the reference's print_cell_phi cuts. */
+khrr_status khrr_mesh_solver_phi(khrr_ctx* ctx, double* cell_phi);
 
 /* ---- drop-in file surface (host only; no device work) ------------------- */
 /* One entry of __start_galaxies.ini (GalaxyProperties, parse.cuh:19-62).

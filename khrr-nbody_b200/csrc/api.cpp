@@ -224,6 +224,7 @@ void khrr_ctx::drop_graphs() {
         if (kv.second.graph) cudaGraphDestroy(kv.second.graph);
     }
     wave_graphs.clear();
+    msolver.drop_graphs();
 }
 
 // ---------------------------------------------------------------------------
@@ -693,6 +694,7 @@ khrr_status khrr_forces(khrr_ctx* c, int flags) {
     if (!c->has_state) return c->fail(KHRR_ERR_STATE, "no state uploaded");
     const bool want_acc = (flags & KHRR_ACC) != 0, want_phi = (flags & KHRR_PHI) != 0;
     if (!want_acc && !want_phi) return c->fail(KHRR_ERR_INVALID_ARG, "flags select nothing");
+    if (flags & KHRR_MESH) return c->mesh_forces(flags);
     const bool plain = (flags & KHRR_PLAIN) != 0;
     cudaStream_t s = c->stream;
     khrr_status st;
@@ -723,6 +725,7 @@ khrr_status khrr_step(khrr_ctx* c, double dt, int nsteps, int flags) {
     if (!c->has_state) return c->fail(KHRR_ERR_STATE, "no state uploaded");
     if (nsteps < 0 || !std::isfinite(dt)) return c->fail(KHRR_ERR_INVALID_ARG, "bad step arguments");
     if (nsteps == 0) return KHRR_OK;
+    if (flags & KHRR_MESH) return c->mesh_step(dt, nsteps, flags);
     const bool plain = (flags & KHRR_PLAIN) != 0;
     const bool compat = (flags & KHRR_COMPAT_ACCUMULATE) != 0;
     const bool phi_last = (flags & KHRR_PHI) != 0;

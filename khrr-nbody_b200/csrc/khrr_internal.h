@@ -180,4 +180,27 @@ cudaError_t launch_apply(double* pacc, double* pval, const double* cacc, const d
 cudaError_t launch_deinterleave(const int2* pci, int64_t n, int* a, int* b, cudaStream_t s);
 cudaError_t launch_to_float(const double* src, float* dst, int64_t n, cudaStream_t s);
 
+// Cloud-in-cell: trilinear weights about cell centres (u = (x - lo)/cs - 1/2,
+// cells floor(u) and floor(u) + 1 per axis, corners outside the mesh dropped),
+// cell ids as the binning's.  The deposit adds m w into cell_mass (FP64
+// atomics); the gather writes acc = sum w cell_acc and value = sum w
+// cell_value (either output may be NULL), corners in z, y, x order.
+cudaError_t launch_cic_deposit(const double* pos, const double* mass, int64_t n, const MeshGeom& m,
+                               double* cell_mass, cudaStream_t s);
+cudaError_t launch_cic_gather(const double* pos, int64_t n, const MeshGeom& m, const double* cell_acc,
+                              const double* cell_value, double* pacc, double* pval, cudaStream_t s);
+// Counting sort: order[start[cell_i] + slot_i] = base + i for the n bodies of pci.
+cudaError_t launch_scatter_order(const int2* pci, const int* start, int64_t n, int base, int* order, cudaStream_t s);
+// Mesh-force gather into one partial slot per body: part[i] = {acc, -phi} of
+// the body's cell (NGP, from pci) or CIC-interpolated (from pos); phi is the
+// mesh potential in FP32 or FP64 (exactly one of phi32 / phi64 non-NULL).
+cudaError_t launch_mesh_gather(const double* pos, const int2* pci, int64_t n, const MeshGeom& m, bool cic,
+                               const double* cell_acc, const float* phi32, const double* phi64, double4* part,
+                               cudaStream_t s);
+// acc_field on an FP32 potential (differences formed in FP64, exact).
+cudaError_t launch_acc_field_f32(double* cell_acc, const float* phi, int nx, double dx, cudaStream_t s);
+// Binning without slots: pci[i] = {cell, 0} and the NGP mass deposit.
+cudaError_t launch_assign_cells(const double* pos, int64_t n, const MeshGeom& m, int2* pci, const double* mass,
+                                double* cell_mass, cudaStream_t s);
+
 }  // namespace khrr

@@ -67,6 +67,30 @@ struct StepGraph {
     cudaGraphNode_t ev0 = nullptr, ev1 = nullptr;  // event-record nodes around the force pass
 };
 
+// The mesh-force solver (khrr_set_mesh_solver): its mesh, field ring and
+// per-body gather slot, and the step graphs per (dt, ring rotation, phi).
+struct MeshSolver {
+    bool on = false;
+    khrr_mesh_solver cfg{};
+    MeshGeom geom{};
+    int64_t cells = 0;
+    DevBuf<double> cell_mass, phi64, cell_acc;  // C, 3 C, 3 C
+    DevBuf<float> mass32, phi32, tab;           // C, 3 C, 3 nx
+    DevBuf<int2> pci;                           // npad
+    DevBuf<double4> part;                       // npad: {acc, -phi} per body
+    DevBuf<unsigned char> ns;                   // npad: 1 for real bodies, 0 for ghosts
+    std::vector<int64_t> layout_poff, layout_cnt;  // the layout pci/part/ns were sized for
+    int rot = 0;                                // ring buffer holding phi^{n-1}
+    std::map<std::tuple<uint64_t, int, bool>, StepGraph> graphs;
+    void drop_graphs() {
+        for (auto& kv : graphs) {
+            if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
+            if (kv.second.graph) cudaGraphDestroy(kv.second.graph);
+        }
+        graphs.clear();
+    }
+};
+
 }  // namespace khrr
 
 struct khrr_ctx {
@@ -107,6 +131,7 @@ struct khrr_ctx {
     int64_t ncells = 0;
     khrr::DevBuf<int2> pci;                              // per padded body: {cell, slot}
     khrr::DevBuf<int> mcount, mstart, maxpbc, mscan, mtmp;  // mscan: scan block/tile totals
+    khrr::DevBuf<int> morder;                            // khrr_sort_by_cell: n body indices
     khrr::DevBuf<double> cell_mass, cell_phi, wave_resid;
     int64_t cell_phi_cells = 0;                          // mesh size the cell_phi sums belong to
     khrr::DevBuf<float> wave_phi, wave_mass, wave_tab;   // 3 C, C, 3 nx
@@ -114,6 +139,9 @@ struct khrr_ctx {
     int wave_rot = 0;                                    // which buffer holds phi^n
     bool wave_warm = false;
     std::map<std::pair<int, int>, khrr::StepGraph> wave_graphs;  // (chunk, rotation)
+
+    // Mesh-force solver (KHRR_MESH).
+    khrr::MeshSolver msolver;
 
     // Timing.
     bool timing = false;
@@ -139,4 +167,9 @@ struct khrr_ctx {
     khrr_status get_step_graph(double dt, bool plain, bool phi_now, bool compat, khrr::StepGraph** out);
     khrr_status timing_pair(cudaEvent_t* e0, cudaEvent_t* e1);
     double pairs_per_pass() const;
+    // Mesh-force solver (mesh_api.cpp).
+    khrr_status mesh_ensure_layout();
+    khrr_status mesh_enqueue_force(const double* x, int iters, int rot0);
+    khrr_status mesh_forces(int flags);
+    khrr_status mesh_step(double dt, int nsteps, int flags);
 };

@@ -48,15 +48,21 @@ __device__ __forceinline__ int cell_axis(double p, double lo, double cs, int g) 
     return 0;
 }
 
+// The reference's cell id (p2mesh-kernel.cuh:25-40): iz clamps to g[1] - 1 and
+// the y stride is g[2].
+__device__ __forceinline__ int cell_of(const double* __restrict__ p, const MeshGeom& m) {
+    const int ix = cell_axis(p[0], m.lo[0], m.cs[0], m.g[0]);
+    const int iy = cell_axis(p[1], m.lo[1], m.cs[1], m.g[1]);
+    const int iz = cell_axis(p[2], m.lo[2], m.cs[2], m.g[1]);
+    return iz * m.g[0] * m.g[1] + iy * m.g[2] + ix;
+}
+
 __global__ void assign_kernel(const double* __restrict__ pos, int64_t n, const MeshGeom m, int2* __restrict__ pci,
                               int* __restrict__ counter, int counter_stride, int* __restrict__ count2,
                               int count2_stride, const double* __restrict__ mass, double* __restrict__ cell_mass) {
     const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (i >= n) return;
-    const int ix = cell_axis(pos[3 * i], m.lo[0], m.cs[0], m.g[0]);
-    const int iy = cell_axis(pos[3 * i + 1], m.lo[1], m.cs[1], m.g[1]);
-    const int iz = cell_axis(pos[3 * i + 2], m.lo[2], m.cs[2], m.g[1]);
-    const int c = iz * m.g[0] * m.g[1] + iy * m.g[2] + ix;
+    const int c = cell_of(pos + 3 * i, m);
     // One atomic per body, as the reference does: bodies arrive in no
     // spatial order, so warp-level aggregation finds almost no shared cells
     // and its match/shuffle traffic costs more than it saves.
@@ -64,6 +70,26 @@ __global__ void assign_kernel(const double* __restrict__ pos, int64_t n, const M
     if (count2) atomicAdd(&count2[static_cast<int64_t>(c) * count2_stride], 1);
     pci[i] = make_int2(c, slot);
     if (cell_mass) atomicAdd(&cell_mass[c], mass[i]);
+}
+
+// Cells and the NGP mass deposit only (the mesh-force step needs no slots).
+__global__ void assign_cells_kernel(const double* __restrict__ pos, int64_t n, const MeshGeom m,
+                                    int2* __restrict__ pci, const double* __restrict__ mass,
+                                    double* __restrict__ cell_mass) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int c = cell_of(pos + 3 * i, m);
+    pci[i] = make_int2(c, 0);
+    atomicAdd(&cell_mass[c], mass[i]);
+}
+
+// The prefix-sum sort: each body lands at start[cell] + slot.
+__global__ void scatter_order_kernel(const int2* __restrict__ pci, const int* __restrict__ start, int64_t n, int base,
+                                     int* __restrict__ order) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int2 v = pci[i];
+    order[start[v.x] + v.y] = base + static_cast<int>(i);
 }
 
 // ---- prefix sums -----------------------------------------------------------
@@ -427,6 +453,151 @@ __global__ void apply_kernel(double* __restrict__ pacc, double* __restrict__ pva
     if (pval) pval[i] = cval[c];
 }
 
+// ---- cloud-in-cell ----------------------------------------------------------
+// One axis: u = (p - lo)/cs - 1/2 in cell-centre units; corners floor(u) and
+// floor(u) + 1 with weights 1 - f and f.  Far-away (and NaN) coordinates map
+// to corners that are both outside the mesh.
+struct CicAxis {
+    int i0;
+    double w[2];
+};
+
+__device__ __forceinline__ CicAxis cic_axis(double p, double lo, double cs, int g) {
+    const double u = (p - lo) / cs - 0.5;
+    const double fl = floor(u);
+    CicAxis a;
+    a.i0 = fl >= -1.0 ? (fl <= static_cast<double>(g) ? static_cast<int>(fl) : g) : -2;
+    const double f = u - fl;
+    a.w[0] = 1.0 - f;
+    a.w[1] = f;
+    return a;
+}
+
+__global__ void cic_deposit_kernel(const double* __restrict__ pos, const double* __restrict__ mass, int64_t n,
+                                   const MeshGeom m, double* __restrict__ cell_mass) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const CicAxis ax = cic_axis(pos[3 * i], m.lo[0], m.cs[0], m.g[0]);
+    const CicAxis ay = cic_axis(pos[3 * i + 1], m.lo[1], m.cs[1], m.g[1]);
+    const CicAxis az = cic_axis(pos[3 * i + 2], m.lo[2], m.cs[2], m.g[2]);
+    const double mi = mass[i];
+#pragma unroll
+    for (int c = 0; c < 2; ++c) {
+        const int z = az.i0 + c;
+        if (z < 0 || z >= m.g[2]) continue;
+#pragma unroll
+        for (int b = 0; b < 2; ++b) {
+            const int y = ay.i0 + b;
+            if (y < 0 || y >= m.g[1]) continue;
+#pragma unroll
+            for (int a = 0; a < 2; ++a) {
+                const int x = ax.i0 + a;
+                if (x < 0 || x >= m.g[0]) continue;
+                const double w = (ax.w[a] * ay.w[b]) * az.w[c];
+                atomicAdd(&cell_mass[static_cast<int64_t>(z) * m.g[0] * m.g[1] + static_cast<int64_t>(y) * m.g[2] + x],
+                          mi * w);
+            }
+        }
+    }
+}
+
+// Interpolation back to a body: acc (3 per cell) and a scalar field in FP32
+// or FP64; sums in z, y, x corner order.
+template <class T>
+__device__ __forceinline__ void cic_interp(const double* __restrict__ p, const MeshGeom& m,
+                                           const double* __restrict__ cacc, const T* __restrict__ cval, double (&acc)[3],
+                                           double& val) {
+    const CicAxis ax = cic_axis(p[0], m.lo[0], m.cs[0], m.g[0]);
+    const CicAxis ay = cic_axis(p[1], m.lo[1], m.cs[1], m.g[1]);
+    const CicAxis az = cic_axis(p[2], m.lo[2], m.cs[2], m.g[2]);
+    acc[0] = acc[1] = acc[2] = 0.0;
+    val = 0.0;
+#pragma unroll
+    for (int c = 0; c < 2; ++c) {
+        const int z = az.i0 + c;
+        if (z < 0 || z >= m.g[2]) continue;
+#pragma unroll
+        for (int b = 0; b < 2; ++b) {
+            const int y = ay.i0 + b;
+            if (y < 0 || y >= m.g[1]) continue;
+#pragma unroll
+            for (int a = 0; a < 2; ++a) {
+                const int x = ax.i0 + a;
+                if (x < 0 || x >= m.g[0]) continue;
+                const double w = (ax.w[a] * ay.w[b]) * az.w[c];
+                const int64_t id = static_cast<int64_t>(z) * m.g[0] * m.g[1] + static_cast<int64_t>(y) * m.g[2] + x;
+                if (cacc) {
+                    acc[0] += w * cacc[3 * id];
+                    acc[1] += w * cacc[3 * id + 1];
+                    acc[2] += w * cacc[3 * id + 2];
+                }
+                if (cval) val += w * static_cast<double>(cval[id]);
+            }
+        }
+    }
+}
+
+__global__ void cic_gather_kernel(const double* __restrict__ pos, int64_t n, const MeshGeom m,
+                                  const double* __restrict__ cacc, const double* __restrict__ cval,
+                                  double* __restrict__ pacc, double* __restrict__ pval) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double a[3], v;
+    cic_interp(pos + 3 * i, m, pacc ? cacc : nullptr, pval ? cval : nullptr, a, v);
+    if (pacc) {
+        pacc[3 * i] = a[0];
+        pacc[3 * i + 1] = a[1];
+        pacc[3 * i + 2] = a[2];
+    }
+    if (pval) pval[i] = v;
+}
+
+// The mesh-force gather into the corrector's partial slot: {acc, -phi}, so
+// the corrector's phi = 0 - (-phi) is the mesh potential (apply_acceleration_
+// to_particles and apply_cell_to_particles, p2mesh-kernel.cuh:227-254).
+template <bool CIC, class T>
+__global__ void mesh_gather_kernel(const double* __restrict__ pos, const int2* __restrict__ pci, int64_t n,
+                                   const MeshGeom m, const double* __restrict__ cacc, const T* __restrict__ phi,
+                                   double4* __restrict__ part) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double a[3], v;
+    if (CIC) {
+        cic_interp(pos + 3 * i, m, cacc, phi, a, v);
+    } else {
+        const int64_t c = pci[i].x;
+        a[0] = cacc[3 * c];
+        a[1] = cacc[3 * c + 1];
+        a[2] = cacc[3 * c + 2];
+        v = static_cast<double>(phi[c]);
+    }
+    part[i] = make_double4(a[0], a[1], a[2], -v);
+}
+
+// acc_field on an FP32 potential: the float differences are exact in FP64.
+__global__ void acc_field_f32_kernel(double* __restrict__ cell_acc, const float* __restrict__ phi, int NX, double DX) {
+    const int ix = blockIdx.x * blockDim.x + threadIdx.x;
+    const int iy = blockIdx.y * blockDim.y + threadIdx.y;
+    const int iz = blockIdx.z;
+    if (ix >= NX || iy >= NX) return;
+    const int64_t at = at3(ix, iy, iz, NX);
+    const double p0 = phi[at];
+    double d[3];
+    if (ix == 0) d[0] = static_cast<double>(phi[at3(ix + 1, iy, iz, NX)]) - p0;
+    else if (ix == NX - 1) d[0] = p0 - static_cast<double>(phi[at3(ix - 1, iy, iz, NX)]);
+    else d[0] = 0.5 * (static_cast<double>(phi[at3(ix + 1, iy, iz, NX)]) - static_cast<double>(phi[at3(ix - 1, iy, iz, NX)]));
+    if (iy == 0) d[1] = static_cast<double>(phi[at3(ix, iy + 1, iz, NX)]) - p0;
+    else if (iy == NX - 1) d[1] = p0 - static_cast<double>(phi[at3(ix, iy - 1, iz, NX)]);
+    else d[1] = 0.5 * (static_cast<double>(phi[at3(ix, iy + 1, iz, NX)]) - static_cast<double>(phi[at3(ix, iy - 1, iz, NX)]));
+    if (iz == 0) d[2] = static_cast<double>(phi[at3(ix, iy, iz + 1, NX)]) - p0;
+    else if (iz == NX - 1) d[2] = p0 - static_cast<double>(phi[at3(ix, iy, iz - 1, NX)]);
+    else d[2] = 0.5 * (static_cast<double>(phi[at3(ix, iy, iz + 1, NX)]) - static_cast<double>(phi[at3(ix, iy, iz - 1, NX)]));
+    const double coef = -1. / DX;
+    cell_acc[3 * at] = d[0] * coef;
+    cell_acc[3 * at + 1] = d[1] * coef;
+    cell_acc[3 * at + 2] = d[2] * coef;
+}
+
 __global__ void to_float_kernel(const double* __restrict__ src, float* __restrict__ dst, int64_t n) {
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
         dst[i] = static_cast<float>(src[i]);
@@ -525,6 +696,55 @@ cudaError_t launch_to_float(const double* src, float* dst, int64_t n, cudaStream
 cudaError_t launch_deinterleave(const int2* pci, int64_t n, int* a, int* b, cudaStream_t s) {
     if (n < 1) return cudaSuccess;
     deinterleave_kernel<<<static_cast<unsigned>((n + 255) / 256), 256, 0, s>>>(pci, n, a, b);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_cic_deposit(const double* pos, const double* mass, int64_t n, const MeshGeom& m,
+                               double* cell_mass, cudaStream_t s) {
+    if (n < 1) return cudaSuccess;
+    cic_deposit_kernel<<<static_cast<unsigned>((n + 255) / 256), 256, 0, s>>>(pos, mass, n, m, cell_mass);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_cic_gather(const double* pos, int64_t n, const MeshGeom& m, const double* cell_acc,
+                              const double* cell_value, double* pacc, double* pval, cudaStream_t s) {
+    if (n < 1) return cudaSuccess;
+    cic_gather_kernel<<<static_cast<unsigned>((n + 255) / 256), 256, 0, s>>>(pos, n, m, cell_acc, cell_value, pacc,
+                                                                               pval);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_scatter_order(const int2* pci, const int* start, int64_t n, int base, int* order, cudaStream_t s) {
+    if (n < 1) return cudaSuccess;
+    scatter_order_kernel<<<static_cast<unsigned>((n + 255) / 256), 256, 0, s>>>(pci, start, n, base, order);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_mesh_gather(const double* pos, const int2* pci, int64_t n, const MeshGeom& m, bool cic,
+                               const double* cell_acc, const float* phi32, const double* phi64, double4* part,
+                               cudaStream_t s) {
+    if (n < 1) return cudaSuccess;
+    const unsigned g = static_cast<unsigned>((n + 255) / 256);
+    if (cic) {
+        if (phi32) mesh_gather_kernel<true, float><<<g, 256, 0, s>>>(pos, pci, n, m, cell_acc, phi32, part);
+        else mesh_gather_kernel<true, double><<<g, 256, 0, s>>>(pos, pci, n, m, cell_acc, phi64, part);
+    } else {
+        if (phi32) mesh_gather_kernel<false, float><<<g, 256, 0, s>>>(pos, pci, n, m, cell_acc, phi32, part);
+        else mesh_gather_kernel<false, double><<<g, 256, 0, s>>>(pos, pci, n, m, cell_acc, phi64, part);
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_acc_field_f32(double* cell_acc, const float* phi, int nx, double dx, cudaStream_t s) {
+    const dim3 block(32, 8), grid((nx + 31) / 32, (nx + 7) / 8, nx);
+    acc_field_f32_kernel<<<grid, block, 0, s>>>(cell_acc, phi, nx, dx);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_assign_cells(const double* pos, int64_t n, const MeshGeom& m, int2* pci, const double* mass,
+                                double* cell_mass, cudaStream_t s) {
+    if (n < 1) return cudaSuccess;
+    assign_cells_kernel<<<static_cast<unsigned>((n + 255) / 256), 256, 0, s>>>(pos, n, m, pci, mass, cell_mass);
     return cudaGetLastError();
 }
 

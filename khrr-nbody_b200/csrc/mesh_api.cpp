@@ -367,3 +367,309 @@ khrr_status khrr_wave_solve(khrr_ctx* c, const khrr_wave_params* p, double tol, 
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Cloud-in-cell, the counting sort, and the mesh-force solver.
+// ---------------------------------------------------------------------------
+namespace {
+
+khrr_status check_cubic(khrr_ctx* c, const khrr_mesh* m, MeshGeom* g, int64_t* ncells) {
+    khrr_status st = check_mesh(c, m, g, ncells);
+    if (st != KHRR_OK) return st;
+    if (m->grid[0] != m->grid[1] || m->grid[1] != m->grid[2])
+        return c->fail(KHRR_ERR_INVALID_ARG, "cloud-in-cell needs a cubic mesh");
+    return KHRR_OK;
+}
+
+}  // namespace
+
+khrr_status khrr_cic_deposit(khrr_ctx* c, const double* pos, const double* mass, int64_t n, const khrr_mesh* mesh,
+                             double* cell_mass) {
+    if (!c) return KHRR_ERR_INVALID_ARG;
+    MeshGeom g;
+    int64_t C = 0;
+    khrr_status st = check_cubic(c, mesh, &g, &C);
+    if (st != KHRR_OK) return st;
+    if (n < 0 || (n > 0 && (!pos || !mass || !cell_mass))) return c->fail(KHRR_ERR_INVALID_ARG, "bad deposit arguments");
+    return c->cuda(launch_cic_deposit(pos, mass, n, g, cell_mass, c->stream), "cic deposit");
+}
+
+khrr_status khrr_cic_gather(khrr_ctx* c, const double* pos, int64_t n, const khrr_mesh* mesh, const double* cell_acc,
+                            const double* cell_value, double* particle_acc, double* particle_value) {
+    if (!c) return KHRR_ERR_INVALID_ARG;
+    MeshGeom g;
+    int64_t C = 0;
+    khrr_status st = check_cubic(c, mesh, &g, &C);
+    if (st != KHRR_OK) return st;
+    if (n < 0 || (n > 0 && !pos) || (particle_acc && !cell_acc) || (particle_value && !cell_value))
+        return c->fail(KHRR_ERR_INVALID_ARG, "bad gather arguments");
+    return c->cuda(launch_cic_gather(pos, n, g, cell_acc, cell_value, particle_acc, particle_value, c->stream),
+                   "cic gather");
+}
+
+khrr_status khrr_sort_by_cell(khrr_ctx* c, int* order) {
+    if (!c) return KHRR_ERR_INVALID_ARG;
+    if (!c->has_bin) return c->fail(KHRR_ERR_STATE, "no binned bodies (call khrr_bin first)");
+    if (c->n > 0x7fffffffLL) return c->fail(KHRR_ERR_INVALID_ARG, "more bodies than int32 indices");
+    khrr_status st;
+    if ((st = c->cuda(c->morder.ensure(static_cast<size_t>(c->n)), "alloc")) != KHRR_OK) return st;
+    for (size_t k = 0; k < c->cnt.size(); ++k)
+        if ((st = c->cuda(launch_scatter_order(c->pci.p + c->poff[k], c->mstart.p, c->cnt[k],
+                                               static_cast<int>(c->off[k]), c->morder.p, c->stream),
+                          "scatter")) != KHRR_OK)
+            return st;
+    if (order && (st = c->cuda(cudaMemcpyAsync(order, c->morder.p, static_cast<size_t>(c->n) * sizeof(int),
+                                               cudaMemcpyDeviceToHost, c->stream),
+                               "download")) != KHRR_OK)
+        return st;
+    return khrr_synchronize(c);
+}
+
+khrr_status khrr_set_mesh_solver(khrr_ctx* c, const khrr_mesh_solver* p) {
+    if (!c) return KHRR_ERR_INVALID_ARG;
+    MeshSolver& M = c->msolver;
+    M.drop_graphs();
+    if (!p) {
+        M.on = false;
+        return KHRR_OK;
+    }
+    khrr_status st = check_wave(c, &p->wave);
+    if (st != KHRR_OK) return st;
+    if (p->assign != KHRR_ASSIGN_NGP && p->assign != KHRR_ASSIGN_CIC)
+        return c->fail(KHRR_ERR_INVALID_ARG, "assign must be KHRR_ASSIGN_NGP or KHRR_ASSIGN_CIC");
+    if (p->iters_per_step < 1 || p->setup_iters < 0)
+        return c->fail(KHRR_ERR_INVALID_ARG, "iters_per_step must be >= 1 and setup_iters >= 0");
+    const int nx = p->wave.nx;
+    const double L = 0.5 * nx * p->wave.dx;  // _domain_l = 0.5 * _nx * _dx (nbody.cu:1136)
+    khrr_mesh m{{-L, -L, -L}, {p->wave.dx, p->wave.dx, p->wave.dx}, {nx, nx, nx}};
+    MeshGeom g;
+    int64_t C = 0;
+    if ((st = check_mesh(c, &m, &g, &C)) != KHRR_OK) return st;
+    const size_t cz = static_cast<size_t>(C);
+    if ((st = c->cuda(M.cell_mass.ensure(cz), "alloc")) != KHRR_OK) return st;
+    if ((st = c->cuda(M.cell_acc.ensure(3 * cz), "alloc")) != KHRR_OK) return st;
+    if (p->fp64) {
+        if ((st = c->cuda(M.phi64.ensure(3 * cz), "alloc")) != KHRR_OK) return st;
+    } else {
+        if ((st = c->cuda(M.phi32.ensure(3 * cz), "alloc")) != KHRR_OK) return st;
+        if ((st = c->cuda(M.mass32.ensure(cz), "alloc")) != KHRR_OK) return st;
+        if ((st = c->cuda(M.tab.ensure(3 * static_cast<size_t>(nx)), "alloc")) != KHRR_OK) return st;
+        std::vector<float> tab;
+        sponge_tables(&p->wave, tab);
+        if ((st = c->cuda(cudaMemcpyAsync(M.tab.p, tab.data(), tab.size() * sizeof(float), cudaMemcpyHostToDevice,
+                                          c->stream),
+                          "upload")) != KHRR_OK)
+            return st;
+    }
+    M.cfg = *p;
+    M.geom = g;
+    M.cells = C;
+    M.rot = 0;
+    M.on = true;
+    // The field starts at zero, as the reference's freshly allocated arrays.
+    if (p->fp64) cudaMemsetAsync(M.phi64.p, 0, 3 * cz * sizeof(double), c->stream);
+    else cudaMemsetAsync(M.phi32.p, 0, 3 * cz * sizeof(float), c->stream);
+    return khrr_synchronize(c);
+}
+
+khrr_status khrr_mesh_solver_phi(khrr_ctx* c, double* cell_phi) {
+    if (!c || !cell_phi) return KHRR_ERR_INVALID_ARG;
+    MeshSolver& M = c->msolver;
+    if (!M.on) return c->fail(KHRR_ERR_STATE, "no mesh solver set");
+    const size_t cz = static_cast<size_t>(M.cells);
+    const size_t cur = static_cast<size_t>((M.rot + 1) % 3) * cz;
+    khrr_status st;
+    if (M.cfg.fp64) {
+        st = c->cuda(cudaMemcpyAsync(cell_phi, M.phi64.p + cur, cz * sizeof(double), cudaMemcpyDeviceToHost, c->stream),
+                     "download");
+        if (st != KHRR_OK) return st;
+        return khrr_synchronize(c);
+    }
+    std::vector<float> f(cz);
+    if ((st = c->cuda(cudaMemcpyAsync(f.data(), M.phi32.p + cur, cz * sizeof(float), cudaMemcpyDeviceToHost, c->stream),
+                      "download")) != KHRR_OK)
+        return st;
+    if ((st = khrr_synchronize(c)) != KHRR_OK) return st;
+    for (size_t i = 0; i < cz; ++i) cell_phi[i] = f[i];
+    return KHRR_OK;
+}
+
+// Per-body buffers of the solver, sized for the uploaded layout.
+khrr_status khrr_ctx::mesh_ensure_layout() {
+    MeshSolver& M = msolver;
+    // All bodies share the one mesh: several independent systems would
+    // attract each other through it.
+    if (cnt.size() != 1) return fail(KHRR_ERR_INVALID_ARG, "the mesh solver runs one system (got %zu)", cnt.size());
+    if (M.layout_poff == poff && M.layout_cnt == cnt && M.ns.p) return KHRR_OK;
+    const size_t np = static_cast<size_t>(npad);
+    khrr_status st;
+    if ((st = cuda(M.pci.ensure(np), "alloc")) != KHRR_OK) return st;
+    if ((st = cuda(M.part.ensure(np), "alloc")) != KHRR_OK) return st;
+    if ((st = cuda(M.ns.ensure(np), "alloc")) != KHRR_OK) return st;
+    std::vector<unsigned char> ns(np, 0);
+    for (size_t k = 0; k < cnt.size(); ++k)
+        std::fill(ns.begin() + poff[k], ns.begin() + poff[k] + cnt[k], static_cast<unsigned char>(1));
+    if ((st = cuda(cudaMemcpyAsync(M.ns.p, ns.data(), np, cudaMemcpyHostToDevice, stream), "upload")) != KHRR_OK)
+        return st;
+    cudaMemsetAsync(M.part.p, 0, np * sizeof(double4), stream);
+    if ((st = cuda(cudaStreamSynchronize(stream), "sync")) != KHRR_OK) return st;  // ns outlives the call
+    M.layout_poff = poff;
+    M.layout_cnt = cnt;
+    M.drop_graphs();
+    return KHRR_OK;
+}
+
+// calc_acceleration_by_grid (nbody.cu:183-285) at positions x: deposit, `iters`
+// stencil iterations from ring rotation rot0, gradient, gather into M.part.
+khrr_status khrr_ctx::mesh_enqueue_force(const double* x, int iters, int rot0) {
+    MeshSolver& M = msolver;
+    const khrr_mesh_solver& P = M.cfg;
+    const size_t cz = static_cast<size_t>(M.cells);
+    const bool cic = P.assign == KHRR_ASSIGN_CIC;
+    cudaStream_t s = stream;
+    khrr_status st;
+    if ((st = cuda(cudaMemsetAsync(M.cell_mass.p, 0, cz * sizeof(double), s), "memset")) != KHRR_OK) return st;
+    for (size_t k = 0; k < cnt.size(); ++k) {
+        const int64_t o = poff[k];
+        cudaError_t e = cic ? launch_cic_deposit(x + 3 * o, mass.p + o, cnt[k], M.geom, M.cell_mass.p, s)
+                            : launch_assign_cells(x + 3 * o, cnt[k], M.geom, M.pci.p + o, mass.p + o, M.cell_mass.p, s);
+        if ((st = cuda(e, "deposit")) != KHRR_OK) return st;
+    }
+    const int nx = P.wave.nx;
+    int r = rot0;
+    if (P.fp64) {
+        const WaveConsts w = wave_consts(&P.wave);
+        for (int i = 0; i < iters; ++i, r = (r + 1) % 3) {
+            double* old = M.phi64.p + static_cast<size_t>(r) * cz;
+            double* cur = M.phi64.p + static_cast<size_t>((r + 1) % 3) * cz;
+            double* nxt = M.phi64.p + static_cast<size_t>((r + 2) % 3) * cz;
+            if ((st = cuda(launch_wave_f64(nxt, cur, old, M.cell_mass.p, w, s), "wave")) != KHRR_OK) return st;
+        }
+        const double* cur = M.phi64.p + static_cast<size_t>((r + 1) % 3) * cz;
+        if ((st = cuda(launch_acc_field(M.cell_acc.p, nullptr, cur, nx, P.wave.dx, s), "acc_field")) != KHRR_OK)
+            return st;
+        for (size_t k = 0; k < cnt.size(); ++k) {
+            const int64_t o = poff[k];
+            if ((st = cuda(launch_mesh_gather(x + 3 * o, M.pci.p + o, cnt[k], M.geom, cic, M.cell_acc.p, nullptr, cur,
+                                              M.part.p + o, s),
+                           "gather")) != KHRR_OK)
+                return st;
+        }
+        return KHRR_OK;
+    }
+    if ((st = cuda(launch_to_float(M.cell_mass.p, M.mass32.p, M.cells, s), "mass to float")) != KHRR_OK) return st;
+    const WaveF32 w = wave_f32(&P.wave, M.tab.p);
+    for (int i = 0; i < iters; ++i, r = (r + 1) % 3) {
+        float* old = M.phi32.p + static_cast<size_t>(r) * cz;
+        float* cur = M.phi32.p + static_cast<size_t>((r + 1) % 3) * cz;
+        float* nxt = M.phi32.p + static_cast<size_t>((r + 2) % 3) * cz;
+        if ((st = cuda(launch_wave_f32(nxt, cur, old, M.mass32.p, w, nullptr, s), "wave")) != KHRR_OK) return st;
+    }
+    const float* cur = M.phi32.p + static_cast<size_t>((r + 1) % 3) * cz;
+    if ((st = cuda(launch_acc_field_f32(M.cell_acc.p, cur, nx, P.wave.dx, s), "acc_field")) != KHRR_OK) return st;
+    for (size_t k = 0; k < cnt.size(); ++k) {
+        const int64_t o = poff[k];
+        if ((st = cuda(launch_mesh_gather(x + 3 * o, M.pci.p + o, cnt[k], M.geom, cic, M.cell_acc.p, cur, nullptr,
+                                          M.part.p + o, s),
+                       "gather")) != KHRR_OK)
+            return st;
+    }
+    return KHRR_OK;
+}
+
+namespace {
+
+StepArgs mesh_step_args(khrr_ctx* c, double dt) {
+    StepArgs a{};
+    a.pos = c->pos.p;
+    a.vel = c->vel.p;
+    a.acc = c->acc.p;
+    a.post = c->post.p;
+    a.velt = c->velt.p;
+    a.acct = c->acct.p;
+    a.mass = c->mass.p;
+    a.phi = c->phi.p;
+    a.shadow = c->shadow();
+    a.part = c->msolver.part.p;
+    a.npad = c->npad;
+    a.nsplit = c->msolver.ns.p;
+    a.n = c->npad;
+    a.dt = dt;
+    a.field = c->field;
+    return a;
+}
+
+}  // namespace
+
+// Setup evaluation (nbody.cu:1449-1472): the field from zero, setup_iters
+// iterations, at the current positions.
+khrr_status khrr_ctx::mesh_forces(int flags) {
+    MeshSolver& M = msolver;
+    if (!M.on) return fail(KHRR_ERR_STATE, "KHRR_MESH without a mesh solver (khrr_set_mesh_solver)");
+    khrr_status st = mesh_ensure_layout();
+    if (st != KHRR_OK) return st;
+    const size_t cz = static_cast<size_t>(M.cells);
+    if (M.cfg.fp64) cudaMemsetAsync(M.phi64.p, 0, 3 * cz * sizeof(double), stream);
+    else cudaMemsetAsync(M.phi32.p, 0, 3 * cz * sizeof(float), stream);
+    if ((st = mesh_enqueue_force(pos.p, M.cfg.setup_iters, 0)) != KHRR_OK) return st;
+    M.rot = M.cfg.setup_iters % 3;
+    StepArgs sa = mesh_step_args(this, 0.0);
+    sa.want_phi = (flags & KHRR_PHI) ? 1 : 0;
+    if ((st = cuda(launch_collect(sa, (flags & KHRR_ACC) != 0, false, stream), "collect")) != KHRR_OK) return st;
+    predicted = false;
+    return KHRR_OK;
+}
+
+// Steps in Wave mode (nbody.cu:1521-1589): predictor, the mesh force at the
+// predicted positions (acct_ zeroed first, nbody.cu:1542, so there is no
+// accumulation), corrector fused with the next predictor; one graph per
+// (dt, ring rotation, phi).
+khrr_status khrr_ctx::mesh_step(double dt, int nsteps, int flags) {
+    MeshSolver& M = msolver;
+    if (!M.on) return fail(KHRR_ERR_STATE, "KHRR_MESH without a mesh solver (khrr_set_mesh_solver)");
+    khrr_status st = mesh_ensure_layout();
+    if (st != KHRR_OK) return st;
+    if (!predicted || pred_dt != dt) {
+        if ((st = cuda(launch_predictor(mesh_step_args(this, dt), stream), "predictor")) != KHRR_OK) return st;
+    }
+    const bool phi_last = (flags & KHRR_PHI) != 0;
+    const int iters = M.cfg.iters_per_step;
+    uint64_t dt_bits;
+    std::memcpy(&dt_bits, &dt, sizeof dt_bits);
+    for (int k = 0; k < nsteps; ++k) {
+        const bool phi_now = phi_last && k == nsteps - 1;
+        const auto key = std::make_tuple(dt_bits, M.rot, phi_now);
+        auto it = M.graphs.find(key);
+        if (it == M.graphs.end()) {
+            StepGraph g{};
+            if ((st = cuda(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal), "begin capture")) !=
+                KHRR_OK)
+                return st;
+            khrr_status est = mesh_enqueue_force(post.p, iters, M.rot);
+            if (est == KHRR_OK) {
+                StepArgs sa = mesh_step_args(this, dt);
+                sa.want_phi = phi_now ? 1 : 0;
+                sa.predict_next = 1;
+                est = cuda(launch_corrector(sa, stream), "corrector");
+            }
+            cudaGraph_t graph = nullptr;
+            cudaError_t ce = cudaStreamEndCapture(stream, &graph);
+            if (est != KHRR_OK) {
+                if (graph) cudaGraphDestroy(graph);
+                return est;
+            }
+            if ((st = cuda(ce, "end capture")) != KHRR_OK) return st;
+            g.graph = graph;
+            if ((st = cuda(cudaGraphInstantiate(&g.exec, graph, 0), "graph instantiate")) != KHRR_OK) {
+                cudaGraphDestroy(graph);
+                return st;
+            }
+            it = M.graphs.emplace(key, g).first;
+        }
+        if ((st = cuda(cudaGraphLaunch(it->second.exec, stream), "graph launch")) != KHRR_OK) return st;
+        M.rot = (M.rot + iters) % 3;
+    }
+    predicted = true;
+    pred_dt = dt;
+    return KHRR_OK;
+}

@@ -21,6 +21,9 @@ PHI = 2
 COMPAT_ACCUMULATE = 4
 PLAIN = 8
 OVERWRITE = 16
+MESH = 32
+ASSIGN_NGP = 0
+ASSIGN_CIC = 1
 
 STATUS = {0: "KHRR_OK", 1: "KHRR_ERR_INVALID_ARG", 2: "KHRR_ERR_NOT_MULTIPLE", 3: "KHRR_ERR_CUDA",
           4: "KHRR_ERR_IO", 5: "KHRR_ERR_TIMEOUT", 6: "KHRR_ERR_STATE", 7: "KHRR_ERR_OOM",
@@ -80,6 +83,12 @@ class WaveParams(C.Structure):
             bc_l = sim_l / 10.0
         return cls(int(nx), dx, dt, c, diss_base, diss_extra, sim_l, bc_l)
 
+
+class MeshSolver(C.Structure):
+    _fields_ = [("wave", WaveParams), ("assign", C.c_int), ("fp64", C.c_int), ("iters_per_step", C.c_int),
+                ("setup_iters", C.c_int)]
+
+
 SCAN_REFERENCE = 0
 SCAN_EXCLUSIVE = 1
 
@@ -134,6 +143,11 @@ def lib(path: pathlib.Path | str | None = None) -> C.CDLL:
         "khrr_wave_solve": ([vp, C.POINTER(WaveParams), d, i, i, i, C.POINTER(i), C.POINTER(d), vp], i),
         "khrr_bin_cell_phi": ([vp, i, vp], i),
         "khrr_accel_noalloc": ([vp, vp, vp, vp, vp, i64, i, vp], i),
+        "khrr_cic_deposit": ([vp, vp, vp, i64, C.POINTER(Mesh), vp], i),
+        "khrr_cic_gather": ([vp, vp, i64, C.POINTER(Mesh), vp, vp, vp, vp], i),
+        "khrr_sort_by_cell": ([vp, vp], i),
+        "khrr_set_mesh_solver": ([vp, C.POINTER(MeshSolver)], i),
+        "khrr_mesh_solver_phi": ([vp, vp], i),
         # host-only file surface
         "khrr_read_galaxies_ini": ([C.c_char_p, vp, i, C.POINTER(i)], i),
         "khrr_read_start_nbody_ini": ([C.c_char_p, C.POINTER(i), C.POINTER(d), C.POINTER(d)], i),
@@ -364,6 +378,36 @@ class Context:
                "start_ref": np.empty(ncells, np.int32), "cell_mass": np.empty(ncells)}
         self._check(self.L.khrr_bin(self.h, C.byref(m), *[_ptr(out[k]) for k in (
             "cell_id", "id_in_cell", "count", "start", "start_ref", "cell_mass")]))
+        return out
+
+    def cic_deposit(self, pos_ptr, mass_ptr, n, mesh: Mesh, cell_mass_ptr):
+        self._check(self.L.khrr_cic_deposit(self.h, _ptr(pos_ptr), _ptr(mass_ptr), n, C.byref(mesh),
+                                            _ptr(cell_mass_ptr)))
+
+    def cic_gather(self, pos_ptr, n, mesh: Mesh, cell_acc_ptr, cell_val_ptr, pacc_ptr, pval_ptr):
+        self._check(self.L.khrr_cic_gather(self.h, _ptr(pos_ptr), n, C.byref(mesh), _ptr(cell_acc_ptr),
+                                           _ptr(cell_val_ptr), _ptr(pacc_ptr), _ptr(pval_ptr)))
+
+    def sort_by_cell(self, want=True):
+        """Counting-sort order of the last bin (body indices by cell)."""
+        order = np.empty(self.n, np.int32) if want else None
+        self._check(self.L.khrr_sort_by_cell(self.h, _ptr(order)))
+        return order
+
+    def set_mesh_solver(self, params: WaveParams | None, assign=ASSIGN_NGP, fp64=False, iters_per_step=None,
+                        setup_iters=20000, dt=0.002):
+        """The reference's Wave mode; iters_per_step defaults to (int)(dt / params.dt)."""
+        if params is None:
+            self._check(self.L.khrr_set_mesh_solver(self.h, None))
+            return
+        if iters_per_step is None:
+            iters_per_step = int(dt / params.dt)
+        ms = MeshSolver(params, int(assign), 1 if fp64 else 0, int(iters_per_step), int(setup_iters))
+        self._check(self.L.khrr_set_mesh_solver(self.h, C.byref(ms)))
+
+    def mesh_solver_phi(self, nx):
+        out = np.empty(nx ** 3)
+        self._check(self.L.khrr_mesh_solver_phi(self.h, _ptr(out)))
         return out
 
     def wave_solve(self, params: WaveParams, tol=1e-5, max_iter=1000, check_every=30, cold=False,

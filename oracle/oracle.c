@@ -510,6 +510,153 @@ void orc_gather(int64_t n, const int* cell_id, const double* cell_acc, const dou
     }
 }
 
+/* ------------------------------------------------------------------------ */
+/* Beyond the reference's NGP path: cloud-in-cell, the counting sort and the */
+/* mesh-force evaluation of its (disabled) Wave mode                         */
+/* ------------------------------------------------------------------------ */
+
+/* One CIC axis: u = (p - lo)/cs - 1/2 in cell-centre units, corners floor(u)
+ * and floor(u) + 1 with weights 1 - f and f (f = u - floor(u)); coordinates
+ * far outside the mesh (and NaN) map to two outside corners.  This is the
+ * textbook cloud-in-cell scheme (Hockney & Eastwood, "Computer Simulation
+ * Using Particles", ch. 5); the reference deposits NGP only. */
+static void cic_axis(double p, double lo, double cs, int g, int* i0, double w[2]) {
+    const double u = (p - lo) / cs - 0.5;
+    const double fl = floor(u);
+    *i0 = fl >= -1.0 ? (fl <= (double)g ? (int)fl : g) : -2;
+    const double f = u - fl;
+    w[0] = 1.0 - f;
+    w[1] = f;
+}
+
+/* CIC deposit in body order: cell_mass[c] += m * ((wx * wy) * wz) over the 8
+ * corners inside the (cubic) mesh, corners in z, y, x order; cell ids as the
+ * binning's (iz*g*g + iy*g + ix). */
+void orc_cic_deposit(int64_t n, const double* pos, const double* mass, const double* lo, const double* cs,
+                     const int* g, double* cell_mass) {
+    for (int64_t i = 0; i < n; ++i) {
+        int i0[3];
+        double w[3][2];
+        for (int k = 0; k < 3; ++k) cic_axis(pos[3 * i + k], lo[k], cs[k], g[k], &i0[k], w[k]);
+        for (int c = 0; c < 2; ++c) {
+            const int z = i0[2] + c;
+            if (z < 0 || z >= g[2]) continue;
+            for (int b = 0; b < 2; ++b) {
+                const int y = i0[1] + b;
+                if (y < 0 || y >= g[1]) continue;
+                for (int a = 0; a < 2; ++a) {
+                    const int x = i0[0] + a;
+                    if (x < 0 || x >= g[0]) continue;
+                    const double wt = (w[0][a] * w[1][b]) * w[2][c];
+                    cell_mass[(int64_t)z * g[0] * g[1] + (int64_t)y * g[2] + x] += mass[i] * wt;
+                }
+            }
+        }
+    }
+}
+
+/* CIC interpolation with the same weights: acc = sum w cell_acc, val = sum w
+ * cell_val (either output may be NULL), corners in z, y, x order. */
+void orc_cic_gather(int64_t n, const double* pos, const double* lo, const double* cs, const int* g,
+                    const double* cell_acc, const double* cell_val, double* acc, double* val) {
+#pragma omp parallel for
+    for (int64_t i = 0; i < n; ++i) {
+        int i0[3];
+        double w[3][2];
+        for (int k = 0; k < 3; ++k) cic_axis(pos[3 * i + k], lo[k], cs[k], g[k], &i0[k], w[k]);
+        double a[3] = {0.0, 0.0, 0.0}, v = 0.0;
+        for (int c = 0; c < 2; ++c) {
+            const int z = i0[2] + c;
+            if (z < 0 || z >= g[2]) continue;
+            for (int b = 0; b < 2; ++b) {
+                const int y = i0[1] + b;
+                if (y < 0 || y >= g[1]) continue;
+                for (int x0 = 0; x0 < 2; ++x0) {
+                    const int x = i0[0] + x0;
+                    if (x < 0 || x >= g[0]) continue;
+                    const double wt = (w[0][x0] * w[1][b]) * w[2][c];
+                    const int64_t id = (int64_t)z * g[0] * g[1] + (int64_t)y * g[2] + x;
+                    if (acc) {
+                        a[0] += wt * cell_acc[3 * id];
+                        a[1] += wt * cell_acc[3 * id + 1];
+                        a[2] += wt * cell_acc[3 * id + 2];
+                    }
+                    if (val) v += wt * cell_val[id];
+                }
+            }
+        }
+        if (acc) {
+            acc[3 * i] = a[0];
+            acc[3 * i + 1] = a[1];
+            acc[3 * i + 2] = a[2];
+        }
+        if (val) val[i] = v;
+    }
+}
+
+/* The prefix-sum sort from binning results: order[start[cell_i] + slot_i] = i. */
+void orc_scatter_order(int64_t n, const int* cell_id, const int* slot, const int* start, int* order) {
+    for (int64_t i = 0; i < n; ++i) order[start[cell_id[i]] + slot[i]] = (int)i;
+}
+
+/* One mesh-force evaluation of the reference's Wave mode
+ * (calc_acceleration_by_grid, nbody/src/nbody.cu:183-285) on a cubic nx^3
+ * mesh over [-nx dx/2, nx dx/2]^3: deposit (cic = 0: the reference's NGP
+ * cell of each body, assignParticlesToCells + computeCellMassesUnsorted;
+ * cic = 1: the CIC deposit above), `iters` stencil iterations on the ring
+ * ring[3] (FP64: ring64, wave_diss_iteration; FP32: ring32, the FP32 form
+ * above, masses rounded to float) starting at rotation *rot (old = ring[r],
+ * cur = ring[r+1], new -> ring[r+2]), then acc_field on the current field and
+ * the gather (NGP: apply_acceleration_to_particles / apply_cell_to_particles;
+ * or CIC).  acc (n x 3) and phi (n) receive the body values; *rot advances. */
+void orc_mesh_force(const orc_wave* W, int cic, int fp64, int iters, int64_t n, const double* pos,
+                    const double* mass, double* ring64, float* ring32, int* rot, double* acc, double* phi) {
+    const int NX = W->nx;
+    const int64_t C = (int64_t)NX * NX * NX;
+    const double L = 0.5 * NX * W->dx;
+    const double lo[3] = {-L, -L, -L}, cs[3] = {W->dx, W->dx, W->dx};
+    const int g[3] = {NX, NX, NX};
+    double* cell_mass = (double*)calloc((size_t)C, sizeof(double));
+    int* cell_id = (int*)malloc(sizeof(int) * (size_t)(n > 0 ? n : 1));
+    if (cic) {
+        orc_cic_deposit(n, pos, mass, lo, cs, g, cell_mass);
+    } else {
+        for (int64_t i = 0; i < n; ++i) {
+            const int ix = cell_axis(pos[3 * i], lo[0], cs[0], g[0]);
+            const int iy = cell_axis(pos[3 * i + 1], lo[1], cs[1], g[1]);
+            const int iz = cell_axis(pos[3 * i + 2], lo[2], cs[2], g[1]);
+            cell_id[i] = iz * g[0] * g[1] + iy * g[2] + ix;
+            cell_mass[cell_id[i]] += mass[i];
+        }
+    }
+    double* cur64 = (double*)malloc(sizeof(double) * (size_t)C);
+    int r = *rot;
+    if (fp64) {
+        for (int it = 0; it < iters; ++it, r = (r + 1) % 3)
+            orc_wave_iter_f64(W, ring64 + (size_t)((r + 2) % 3) * C, ring64 + (size_t)((r + 1) % 3) * C,
+                              ring64 + (size_t)r * C, cell_mass);
+        memcpy(cur64, ring64 + (size_t)((r + 1) % 3) * C, sizeof(double) * (size_t)C);
+    } else {
+        float* m32 = (float*)malloc(sizeof(float) * (size_t)C);
+        for (int64_t c = 0; c < C; ++c) m32[c] = (float)cell_mass[c];
+        for (int it = 0; it < iters; ++it, r = (r + 1) % 3)
+            orc_wave_iter_f32(W, ring32 + (size_t)((r + 2) % 3) * C, ring32 + (size_t)((r + 1) % 3) * C,
+                              ring32 + (size_t)r * C, m32);
+        const float* cur = ring32 + (size_t)((r + 1) % 3) * C;
+        for (int64_t c = 0; c < C; ++c) cur64[c] = (double)cur[c];
+        free(m32);
+    }
+    *rot = r;
+    double* cell_acc = (double*)malloc(sizeof(double) * 3 * (size_t)C);
+    orc_acc_field(NX, W->dx, cur64, cell_acc);
+    if (cic) orc_cic_gather(n, pos, lo, cs, g, cell_acc, cur64, acc, phi);
+    else orc_gather(n, cell_id, cell_acc, cur64, acc, phi);
+    free(cell_acc);
+    free(cur64);
+    free(cell_id);
+    free(cell_mass);
+}
+
 int orc_max_threads(void) {
 #ifdef _OPENMP
     return omp_get_max_threads();

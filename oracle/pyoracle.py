@@ -81,6 +81,11 @@ class Oracle:
         L.orc_wave_iter_f32.argtypes = [C.POINTER(OrcWave), _f32p, _f32p, _f32p, _f32p]
         L.orc_acc_field.argtypes = [C.c_int, _d, _f64p, _f64p]
         L.orc_gather.argtypes = [_i64, _i32p, _vp, _vp, _vp, _vp]
+        L.orc_cic_deposit.argtypes = [_i64, _f64p, _f64p, _f64p, _f64p, _i32p, _f64p]
+        L.orc_cic_gather.argtypes = [_i64, _f64p, _f64p, _f64p, _i32p, _vp, _vp, _vp, _vp]
+        L.orc_scatter_order.argtypes = [_i64, _i32p, _i32p, _i32p, _i32p]
+        L.orc_mesh_force.argtypes = [C.POINTER(OrcWave), C.c_int, C.c_int, C.c_int, _i64, _f64p, _f64p,
+                                     _vp, _vp, C.POINTER(C.c_int), _f64p, _f64p]
         L.orc_max_threads.restype = C.c_int
 
     # -- field ------------------------------------------------------------
@@ -221,6 +226,81 @@ class Oracle:
         self.L.orc_gather(n, np.ascontiguousarray(cell_id, np.int32), ca.ctypes.data,
                           cp.ctypes.data, acc.ctypes.data, phi.ctypes.data)
         return acc.reshape(-1, 3), phi
+
+    # -- beyond the reference's NGP path -----------------------------------------
+    def cic_deposit(self, pos, mass, lo, cs, grid, cell_mass=None):
+        g = np.ascontiguousarray(grid, np.int32)
+        ncells = int(g[0]) * int(g[1]) * int(g[2])
+        out = np.zeros(ncells) if cell_mass is None else np.ascontiguousarray(cell_mass, np.float64).copy()
+        p = _c3(pos)
+        self.L.orc_cic_deposit(p.size // 3, p, np.ascontiguousarray(mass, np.float64),
+                               np.ascontiguousarray(lo, np.float64), np.ascontiguousarray(cs, np.float64), g, out)
+        return out
+
+    def cic_gather(self, pos, lo, cs, grid, cell_acc, cell_val):
+        p = _c3(pos)
+        n = p.size // 3
+        acc = np.zeros(3 * n)
+        val = np.zeros(n)
+        ca = _c3(cell_acc)
+        cv = np.ascontiguousarray(cell_val, np.float64)
+        self.L.orc_cic_gather(n, p, np.ascontiguousarray(lo, np.float64), np.ascontiguousarray(cs, np.float64),
+                              np.ascontiguousarray(grid, np.int32), ca.ctypes.data, cv.ctypes.data,
+                              acc.ctypes.data, val.ctypes.data)
+        return acc.reshape(-1, 3), val
+
+    def scatter_order(self, cell_id, slot, start):
+        n = len(cell_id)
+        order = np.full(n, -1, np.int32)
+        self.L.orc_scatter_order(n, np.ascontiguousarray(cell_id, np.int32), np.ascontiguousarray(slot, np.int32),
+                                 np.ascontiguousarray(start, np.int32), order)
+        return order
+
+    def mesh_force(self, W: OrcWave, pos, mass, iters, cic=False, fp64=True):
+        """One mesh-force evaluation from a zero field (orc_mesh_force)."""
+        ncells = W.nx ** 3
+        ring64 = np.zeros(3 * ncells)
+        ring32 = np.zeros(3 * ncells, np.float32)
+        rot = C.c_int(0)
+        p = _c3(pos)
+        n = p.size // 3
+        acc = np.zeros(3 * n)
+        phi = np.zeros(n)
+        self.L.orc_mesh_force(C.byref(W), int(cic), int(fp64), int(iters), n, p,
+                              np.ascontiguousarray(mass, np.float64), ring64.ctypes.data, ring32.ctypes.data,
+                              C.byref(rot), acc, phi)
+        return acc.reshape(-1, 3), phi
+
+    def mesh_steps(self, W: OrcWave, pos, vel, mass, dt, nsteps, iters, setup_iters, cic=False, fp64=True,
+                   field=None):
+        """The reference's Wave-mode run (nbody/src/nbody.cu:1449-1472 setup,
+        1521-1589 per step) with the mesh force of orc_mesh_force: setup from a
+        zero field, then per step predictor, acct = mesh force at the predicted
+        positions, corrector.  Returns pos, vel, acc, phi after nsteps."""
+        nx = W.nx
+        ncells = nx ** 3
+        ring64 = np.zeros(3 * ncells)
+        ring32 = np.zeros(3 * ncells, np.float32)
+        rot = C.c_int(0)
+        pos = _c3(pos).copy()
+        vel = _c3(vel).copy()
+        m = np.ascontiguousarray(mass, np.float64)
+        n = pos.size // 3
+        acc = np.zeros(3 * n)
+        phi = np.zeros(n)
+
+        self.L.orc_mesh_force(C.byref(W), int(cic), int(fp64), setup_iters, n, pos, m, ring64.ctypes.data,
+                              ring32.ctypes.data, C.byref(rot), acc, phi)
+        fref = C.byref(field) if field is not None else None
+        post = np.zeros_like(pos)
+        velt = np.zeros_like(vel)
+        acct = np.zeros(3 * n)
+        for _ in range(nsteps):
+            self.L.orc_integ(n, fref, acc, post, velt, pos, vel, dt, 0, acc)
+            self.L.orc_mesh_force(C.byref(W), int(cic), int(fp64), iters, n, post, m, ring64.ctypes.data,
+                                  ring32.ctypes.data, C.byref(rot), acct, phi)
+            self.L.orc_integ(n, fref, acct, pos, vel, post, velt, dt, 1, acc)
+        return pos.reshape(-1, 3), vel.reshape(-1, 3), acc.reshape(-1, 3), phi
 
     def max_threads(self) -> int:
         return int(self.L.orc_max_threads())

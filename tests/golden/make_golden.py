@@ -6,7 +6,8 @@ inputs + outputs as compressed .npz files.  The reference has no tests or
 golden vectors of its own, so these fixtures are the pin for the oracle
 restatement (oracle/oracle.c) and, through it, for the CUDA path.
 
-Usage:  python tests/golden/make_golden.py      (needs the reference tree)
+Usage:  python tests/golden/make_golden.py [meshforce]   (needs the reference tree;
+        with "meshforce" only that fixture is written)
 """
 from __future__ import annotations
 
@@ -121,6 +122,8 @@ def main() -> None:
     np.savez_compressed(OUT / "wave_nx16.npz", cell_mass=cm, phi_prev=prev, phi=cur,
                         cell_acc=cell_acc, nx=nx, dx=dx, dt=dt, c=c, sim_l=sim_l)
 
+    meshforce(R)
+
     # --- the reference's .ini reader on two galaxy files ---------------------
     parsed = {}
     with tempfile.TemporaryDirectory() as td:
@@ -136,5 +139,33 @@ def main() -> None:
     print("golden fixtures written to", OUT)
 
 
+def meshforce(R) -> None:
+    """The reference's Wave-mode force (calc_acceleration_by_grid,
+    nbody/src/nbody.cu:183-285) composed from its own kernels: bin + NGP
+    deposit, 40 wave iterations from a zero field, acc_field, the two
+    gathers.  A 16^3 mesh of dx = 0.2 over [-1.6, 1.6]^3 (some bodies outside,
+    clamped into the faces)."""
+    pos, vel, mass, eps2 = galaxy_inputs(1024, 2048, seed=17)
+    nx, dx, iters = 16, 0.2, 40
+    c = 4574.337022617616
+    dt = 0.5 * dx / (c * np.sqrt(3.0))
+    sim_l = 0.5 * nx * dx
+    R.set_mesh((-sim_l,) * 3, (dx,) * 3, (nx, nx, nx), nx_wave=nx, dx_wave=dx, dt_wave=dt,
+               c_wave=c, diss_base=0.1, diss_extra=0.01, sim_l=sim_l, bc_l=sim_l / 10.0)
+    b = R.bin(pos, mass, nx ** 3)
+    prev, cur = np.zeros(nx ** 3), np.zeros(nx ** 3)
+    for _ in range(iters):
+        nxt = R.wave(cur, prev, b["cell_mass"])
+        prev, cur = cur, nxt
+    cell_acc = R.acc_field(nx, dx, cur)
+    acc, phi = R.apply(b["pci"], cell_acc, cur)
+    np.savez_compressed(OUT / "meshforce_n3072.npz", pos=pos, mass=mass, acc=acc, phi=phi, cell_phi=cur,
+                        nx=nx, dx=dx, dt=dt, c=c, sim_l=sim_l, iters=iters)
+
+
 if __name__ == "__main__":
-    main()
+    if sys.argv[1:] == ["meshforce"]:
+        build()
+        meshforce(Reference())
+    else:
+        main()
