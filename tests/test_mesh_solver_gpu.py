@@ -55,6 +55,7 @@ def test_cic_deposit_and_gather(ctx, torch_cuda, oracle):
     C = nx ** 3
     P, M = dev(torch, pos), dev(torch, mass)
     cm = torch.zeros(C, dtype=torch.float64, device="cuda")
+    torch.cuda.synchronize()   # torch's fill runs on its own stream, the deposit on the context's
     ctx.cic_deposit(P.data_ptr(), M.data_ptr(), len(mass), mesh, cm.data_ptr())
     ctx.synchronize()
     want = oracle.cic_deposit(pos, mass, (-L,) * 3, (cs,) * 3, (nx,) * 3)
@@ -65,8 +66,9 @@ def test_cic_deposit_and_gather(ctx, torch_cuda, oracle):
     cval = rng.normal(size=C)
     A = torch.zeros((len(mass), 3), dtype=torch.float64, device="cuda")
     V = torch.zeros(len(mass), dtype=torch.float64, device="cuda")
-    ctx.cic_gather(P.data_ptr(), len(mass), mesh, dev(torch, cacc).data_ptr(), dev(torch, cval).data_ptr(),
-                   A.data_ptr(), V.data_ptr())
+    CA, CV = dev(torch, cacc), dev(torch, cval)   # held until the kernel has run
+    torch.cuda.synchronize()
+    ctx.cic_gather(P.data_ptr(), len(mass), mesh, CA.data_ptr(), CV.data_ptr(), A.data_ptr(), V.data_ptr())
     ctx.synchronize()
     wa, wv = oracle.cic_gather(pos, (-L,) * 3, (cs,) * 3, (nx,) * 3, cacc, cval)
     assert np.array_equal(A.cpu().numpy(), wa)
