@@ -291,6 +291,30 @@ def mesh_leg(khrr, device, torch, hbm_gbs, iter_cap=0):
             wms = e0.elapsed_time(e1)
             per_it = wms / max(it, 1)
             wave_gbs = 16.0 * ncells / (per_it * 1e-3) / 1e9
+
+            def timed(fn, reps=5):
+                best = 1e30
+                for _ in range(reps):
+                    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                    a.record(s)
+                    fn()
+                    b.record(s)
+                    b.synchronize()
+                    best = min(best, a.elapsed_time(b))
+                return best
+
+            # CIC deposit (the configs bin CIC) and the counting-sort order of the bin.
+            P = torch.as_tensor(np.ascontiguousarray(pos).reshape(-1), device=device)
+            M = torch.as_tensor(np.ascontiguousarray(mass), device=device)
+            CM = torch.zeros(ncells, dtype=torch.float64, device=device)
+            torch.cuda.synchronize()
+
+            def cic():
+                ctx._check(ctx.L.khrr_cic_deposit(ctx.h, P.data_ptr(), M.data_ptr(), n, C.byref(mesh), CM.data_ptr()))
+            cic_ms = timed(cic)
+            cic_bytes = 32.0 * n + 16.0 * ncells
+            sort_ms = timed(lambda: ctx.sort_by_cell(want=False))
+            del P, M, CM
             out[label] = {
                 "bodies": n, "cells": ncells,
                 "bin_scan_deposit_ms": best, "bin_gbs": bin_bytes / (best * 1e-3) / 1e9,
@@ -299,7 +323,23 @@ def mesh_leg(khrr, device, torch, hbm_gbs, iter_cap=0):
                 "wave_gbs": wave_gbs, "wave_frac_of_hbm": wave_gbs / hbm_gbs,
                 "wave_working_set_mb": 16.0 * ncells / 1e6,
                 "wave_note": "L2-resident working set" if 16.0 * ncells < 126e6 else "HBM-resident",
+                "cic_deposit_ms": cic_ms, "cic_gbs": cic_bytes / (cic_ms * 1e-3) / 1e9,
+                "cic_bytes_note": "32 B per body (FP64 position, mass) + 16 B per cell (zeroed, summed)",
+                "sort_ms": sort_ms, "sort_gbs": 16.0 * n / (sort_ms * 1e-3) / 1e9,
             }
+            if label == "encounter_128":
+                # The reference's Wave mode on this mesh: FP32 stencil, CIC,
+                # (int)(dt / dt_wave) iterations per dt = 0.002 step.
+                ips = int(0.002 / W.dt)
+                ctx.set_mesh_solver(W, assign=khrr.ASSIGN_CIC, fp64=False, iters_per_step=ips, setup_iters=2000)
+                try:
+                    ctx.forces(khrr.ACC | khrr.MESH)
+                    ctx.step(0.002, 3, khrr.MESH)   # builds the graphs of all three ring rotations
+                    step_ms = timed(lambda: ctx.step(0.002, 1, khrr.MESH), reps=3)
+                finally:
+                    ctx.set_mesh_solver(None)
+                out[label].update({"wave_mode_step_ms": step_ms, "wave_mode_iters_per_step": ips,
+                                   "wave_mode_gbs": 16.0 * ncells * ips / (step_ms * 1e-3) / 1e9})
     finally:
         ctx.close()
     return out

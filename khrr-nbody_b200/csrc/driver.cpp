@@ -3,7 +3,15 @@
 // out/ files, and runs the time loop on the GPU through the C ABI.
 //
 //   khrr_nbody [--data DIR] [--device K] [--compat-accumulate] [--no-mesh]
-//              [--mesh-nx N] [--mesh-dx D] [--quiet]
+//              [--mesh-nx N] [--mesh-dx D] [--wave] [--wave-fp32] [--cic]
+//              [--wave-setup ITERS] [--quiet]
+//
+// --wave selects the reference's Wave solver (NBodySolver::Wave, compiled in
+// the reference but switched off at nbody.cu:1132): forces and potentials
+// from the damped-wave mesh field (setup ITERS iterations, default 20000,
+// then (int)(dtgrav / dt_wave) per step), the FP64 stencil and NGP deposit
+// unless --wave-fp32 / --cic; phi/ cuts then show that field (nbody.cu:1485,
+// 1666).
 //
 // DIR defaults to $KHRR_DATA or ./data/nbody (the reference's BASE_PATH,
 // target_dir.h.in:5-9); inputs come from DIR/ini, outputs go to DIR/bin and
@@ -42,6 +50,10 @@ struct Options {
     bool mesh = true;
     int mesh_nx = 200;     // nbody.cu:1134
     double mesh_dx = 0.2;  // nbody.cu:1135
+    bool wave = false;
+    bool wave_fp32 = false;
+    bool cic = false;
+    int wave_setup = 20000;  // _iterations_to_setup, nbody.cu:1143
     bool quiet = false;
 };
 
@@ -157,6 +169,10 @@ Options parse(int argc, char** argv) {
         else if (a == "--no-mesh") o.mesh = false;
         else if (a == "--mesh-nx") o.mesh_nx = std::stoi(next());
         else if (a == "--mesh-dx") o.mesh_dx = std::stod(next());
+        else if (a == "--wave") o.wave = true;
+        else if (a == "--wave-fp32") o.wave_fp32 = true;
+        else if (a == "--cic") o.cic = true;
+        else if (a == "--wave-setup") o.wave_setup = std::stoi(next());
         else if (a == "--quiet") o.quiet = true;
         else die("unknown argument " + a);
     }
@@ -272,8 +288,56 @@ int main(int argc, char** argv) {
     if (khrr_create(device, &ctx) != KHRR_OK) die(std::format("no usable sm_100 device {}", device));
     if (field.Mh != 0.0 || field.Mb != 0.0) check(khrr_set_external_field(ctx, &field), ctx, "external field");
     check(khrr_upload_state(ctx, nn, pos.data(), vel.data(), mass.data(), eps2.data(), 1, nullptr), ctx, "upload");
+    // Mesh of the save-time binning and of the Wave solver (nbody.cu:1134-1143).
+    const int NX = opt.mesh_nx;
+    const double L = 0.5 * NX * opt.mesh_dx;
+    khrr_mesh mesh{};
+    for (int q = 0; q < 3; ++q) {
+        mesh.lo[q] = -L;
+        mesh.cell[q] = opt.mesh_dx;
+        mesh.grid[q] = NX;
+    }
+    int solver_flag = 0;
+    if (opt.wave) {
+        khrr_mesh_solver ms{};
+        const double c_wave = 4574.337022617616;  // nbody.cu:1137
+        ms.wave.nx = NX;
+        ms.wave.dx = opt.mesh_dx;
+        ms.wave.c = c_wave;
+        ms.wave.dt = 0.5 * opt.mesh_dx / (c_wave * std::sqrt(3.0));
+        ms.wave.diss_base = 0.1;
+        ms.wave.diss_extra = 0.01;
+        ms.wave.sim_l = L;
+        ms.wave.bc_l = L / 10.;
+        ms.assign = opt.cic ? KHRR_ASSIGN_CIC : KHRR_ASSIGN_NGP;
+        ms.fp64 = opt.wave_fp32 ? 0 : 1;
+        ms.iters_per_step = static_cast<int>(dtgrav / ms.wave.dt);  // calc_acceleration_by_grid's int argument
+        ms.setup_iters = opt.wave_setup;
+        if (ms.iters_per_step < 1) die("dtgrav is shorter than one wave step");
+        std::printf("Wave eq iterations: %d\n", ms.iters_per_step);
+        check(khrr_set_mesh_solver(ctx, &ms), ctx, "mesh solver");
+        solver_flag = KHRR_MESH;
+    }
+    std::vector<double> cell_phi(opt.mesh || opt.wave ? static_cast<size_t>(NX) * NX * NX : 0);
+    auto print_cell_phi = [&](int iter) {
+        const fs::path dir = out / "phi";
+        fs::create_directories(dir, ec);
+        std::ofstream s(dir / std::format("phi_{:5}.csv", iter));
+        s << "x, phi" << std::endl;
+        const int IY = NX / 2, IZ = NX / 2;
+        for (int i = 0; i < NX; ++i) {
+            const double x = -L + i * opt.mesh_dx;
+            const size_t at = static_cast<size_t>(i) + static_cast<size_t>(IY) * NX + static_cast<size_t>(IZ) * NX * NX;
+            s << std::format("{}, {:.7f}", x, cell_phi[at]) << std::endl;
+        }
+    };
+
     const auto t_setup = std::chrono::steady_clock::now();
-    check(khrr_forces(ctx, KHRR_ACC | KHRR_PHI), ctx, "setup forces");
+    check(khrr_forces(ctx, KHRR_ACC | KHRR_PHI | solver_flag), ctx, "setup forces");
+    if (opt.wave) {
+        check(khrr_mesh_solver_phi(ctx, cell_phi.data()), ctx, "mesh field");
+        print_cell_phi(0);
+    }
     check(khrr_synchronize(ctx), ctx, "setup");
     std::printf("time for setup: %g seconds \n",
                 std::chrono::duration<double>(std::chrono::steady_clock::now() - t_setup).count());
@@ -283,19 +347,9 @@ int main(int argc, char** argv) {
         w.result(ctx, pos, vel, ns, nn, 0, 0.0, 0);
     }
 
-    // Mesh of the save-time binning (nbody.cu:1134-1143, 1612-1634).
-    const int NX = opt.mesh_nx;
-    const double L = 0.5 * NX * opt.mesh_dx;
-    khrr_mesh mesh{};
-    for (int q = 0; q < 3; ++q) {
-        mesh.lo[q] = -L;
-        mesh.cell[q] = opt.mesh_dx;
-        mesh.grid[q] = NX;
-    }
-    std::vector<double> cell_phi(opt.mesh ? static_cast<size_t>(NX) * NX * NX : 0);
-
     // ---- time loop (nbody.cu:1518-1709) ----
-    const int flags_compat = opt.compat ? KHRR_COMPAT_ACCUMULATE : 0;
+    // The Wave branch zeroes acct_ every step (nbody.cu:1542): nothing to accumulate.
+    const int flags_compat = opt.compat && !opt.wave ? KHRR_COMPAT_ACCUMULATE : 0;
     int it_grav = 0;
     long long total_steps = 0;
     double gpu_time = 0.0;
@@ -318,11 +372,13 @@ int main(int argc, char** argv) {
             }
             ++itt;
         } while (t < tmax);
-        check(khrr_step(ctx, dtgrav, k, flags_compat | (save ? KHRR_PHI : 0)), ctx, "step");
+        check(khrr_step(ctx, dtgrav, k, flags_compat | solver_flag | (save ? KHRR_PHI : 0)), ctx, "step");
         total_steps += k;
         if (save) {
             tsave = tgrav;
-            if (opt.mesh) {
+            if (opt.wave) {
+                check(khrr_mesh_solver_phi(ctx, cell_phi.data()), ctx, "mesh field");
+            } else if (opt.mesh) {  // the Nbody branch's save-time binning (nbody.cu:1601-1634)
                 check(khrr_bin(ctx, &mesh, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr), ctx, "binning");
                 check(khrr_bin_cell_phi(ctx, 0, cell_phi.data()), ctx, "cell phi");
             }
@@ -334,19 +390,7 @@ int main(int argc, char** argv) {
             std::printf("--------------------------------------------------------------------------------\n");
             std::printf("<Time_frame> = %.3f s, frame = %d, iter = %d, iter_g = %d\n", gpu_time, it, itt, ittg);
             std::printf("Time = (%g,  %g) ---  dt = (%g,  %g)\n", t, tgrav - dtgrav, dtsave / itt, dtgrav);
-            if (opt.mesh) {
-                const fs::path dir = out / "phi";
-                fs::create_directories(dir, ec);
-                std::ofstream s(dir / std::format("phi_{:5}.csv", itt * it));
-                s << "x, phi" << std::endl;
-                const int IY = NX / 2, IZ = NX / 2;
-                for (int i = 0; i < NX; ++i) {
-                    const double x = -L + i * opt.mesh_dx;
-                    const size_t at = static_cast<size_t>(i) + static_cast<size_t>(IY) * NX +
-                                      static_cast<size_t>(IZ) * NX * NX;
-                    s << std::format("{}, {:.7f}", x, cell_phi[at]) << std::endl;
-                }
-            }
+            if (opt.mesh || opt.wave) print_cell_phi(itt * it);
             {
                 // sample.csv: body 1 (nbody.cu:1668-1699).
                 std::ofstream s(out / "sample.csv", it == 1 ? std::ios::out : std::ios::app);

@@ -129,3 +129,60 @@ def test_driver_run_outputs_and_restart(libkhrr, tmp_path):
     _, pd2, _ = read_snapshot(bins / "DM_   20.bin", n - ns)
     assert abs(t2 - 0.2) < 1e-12
     assert np.abs(np.concatenate([ps2, pd2]) - state2["pos"]).max() <= 1e-12
+
+
+def test_driver_wave_mode(libkhrr, tmp_path):
+    """--wave: the reference's Wave solver; the trajectory equals the API
+    run with the same mesh solver, and the phi/ cuts show the wave field from
+    the setup (frame 0) on."""
+    torch = pytest.importorskip("torch")
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    import khrr
+    d = tmp_path / "nbody"
+    write_inputs(d, 0, 0.02)
+    r = subprocess.run([str(DRIVER), "--data", str(d), "--quiet", "--mesh-nx", "32", "--mesh-dx", "0.25", "--wave",
+                        "--wave-setup", "300"], capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
+    iters = int(0.002 / (0.5 * 0.25 / (4574.337022617616 * np.sqrt(3.0))))
+    assert f"Wave eq iterations: {iters}" in r.stdout
+    out, bins = d / "out", d / "bin"
+    phi_files = sorted((out / "phi").glob("phi_*.csv"))
+    assert len(phi_files) == 3 and (out / "phi" / "phi_    0.csv").exists()
+    assert len((out / "E(t).csv").read_text().splitlines()) == 4
+    # the same run through the API
+    from test_io import Galaxy
+    L = khrr.lib()
+    gals = (Galaxy * 4)()
+    cnt = C.c_int()
+    assert L.khrr_read_galaxies_ini(str(d / "ini" / "__start_galaxies.ini").encode(), gals, 4, C.byref(cnt)) == 0
+    nmax = 4000
+    pos, vel, mass, eps2 = np.zeros((nmax, 3)), np.zeros((nmax, 3)), np.zeros(nmax), np.zeros(nmax)
+    n, ns = C.c_int64(), C.c_int64()
+    assert L.khrr_load_initial_conditions(str(d / "ini").encode(), gals, cnt.value, nmax, pos.ctypes.data,
+                                          vel.ctypes.data, mass.ctypes.data, eps2.ctypes.data, C.byref(n),
+                                          C.byref(ns)) == 0
+    n = n.value
+    ctx = khrr.Context(0)
+    try:
+        ctx.set_external_field(Mh=1.0, a=0.3333, Rh=1.0, Mb=0.0, b=0.0431, Rb=0.2)
+        ctx.upload(pos[:n], vel[:n], mass[:n], eps2[:n])
+        ctx.set_mesh_solver(khrr.WaveParams.make(32, 0.25), assign=khrr.ASSIGN_NGP, fp64=True,
+                            iters_per_step=iters, setup_iters=300)
+        ctx.forces(khrr.ACC | khrr.PHI | khrr.MESH)
+        ctx.step(0.002, 10, khrr.MESH | khrr.PHI)
+        st = ctx.download()
+        field = ctx.mesh_solver_phi(32)
+    finally:
+        ctx.close()
+    last = (out / "phi" / "phi_   10.csv").read_text().splitlines()[1:]
+    cut = np.array([float(l.split(", ")[1]) for l in last])
+    want = field.reshape(32, 32, 32)[16, 16, :]
+    assert np.abs(cut - want).max() <= 1e-7 * max(1.0, np.abs(want).max())
+    rows = [l.split(", ") for l in (out / "E(t).csv").read_text().splitlines()[1:]]
+    assert int(rows[-1][0]) == 10
+    # body 1 of sample.csv (6 significant digits) is the API run's body 1
+    srow = (out / "sample.csv").read_text().splitlines()[-1].split(", ")
+    assert abs(float(srow[5]) - st["pos"][1, 2]) <= 1e-5 * abs(st["pos"][1, 2]) + 1e-12
+    # and the final snapshot-free state: phi of body 1 is the gathered field
+    assert abs(float(srow[7]) - st["phi"][1]) <= 1e-5 * abs(st["phi"][1])
