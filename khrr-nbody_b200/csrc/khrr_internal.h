@@ -173,6 +173,47 @@ cudaError_t launch_wave_f64(double* phi_new, const double* phi, const double* ph
                             const WaveConsts& w, cudaStream_t s);
 cudaError_t launch_wave_f32(float* phi_new, const float* phi, const float* phi_old, const float* mass,
                             const WaveF32& w, double* resid, cudaStream_t s);
+// Two FP32 iterations in one launch: out1 = phi^{n+1}, out2 = phi^{n+2}
+// (bit-identical to two launch_wave_f32 calls); resid (may be NULL) sums
+// (phi^{n+2} - phi^{n+1})^2 and (phi^{n+2})^2.  out1 and out2 must differ
+// from phi and phi_old.
+cudaError_t launch_wave2_f32(float* out1, float* out2, const float* phi, const float* phi_old, const float* mass,
+                             const WaveF32& w, double* resid, cudaStream_t s);
+// The four-buffer field ring of the FP32 solver: state = 4 * old + cur; a
+// single iteration writes the lower free buffer (state -> 4 * cur + f0), a
+// pair writes f0 and f1 (state -> 4 * f0 + f1).
+constexpr int kRingStart = 1;  // old = buffer 0, cur = buffer 1
+inline void ring_free(int st, int& f0, int& f1) {
+    const int o = st / 4, c = st % 4;
+    int f[2], n = 0;
+    for (int b = 0; b < 4; ++b)
+        if (b != o && b != c) f[n++] = b;
+    f0 = f[0];
+    f1 = f[1];
+}
+inline int ring_step1(int st) {
+    int f0, f1;
+    ring_free(st, f0, f1);
+    return 4 * (st % 4) + f0;
+}
+inline int ring_step2(int st) {
+    int f0, f1;
+    ring_free(st, f0, f1);
+    return 4 * f0 + f1;
+}
+// k FP32 iterations: pairs, then a single one when k is odd.
+inline int ring_after_f32(int st, int k) {
+    for (int i = 0; i < k / 2; ++i) st = ring_step2(st);
+    return k % 2 ? ring_step1(st) : st;
+}
+inline int ring_after_f64(int st, int k) {
+    for (int i = 0; i < k; ++i) st = ring_step1(st);
+    return st;
+}
+// Enqueues k FP32 iterations on the ring (4 buffers of cells floats) from
+// state st; resid (may be NULL) is reduced by the last one.
+cudaError_t enqueue_wave_f32(float* ring, int64_t cells, const float* mass, const WaveF32& w, int k, int st,
+                             double* resid, cudaStream_t s);
 cudaError_t launch_acc_field(double* cell_acc, double* cell_acc_abs, const double* phi, int nx, double dx,
                              cudaStream_t s);
 cudaError_t launch_apply(double* pacc, double* pval, const double* cacc, const double* cval, const int2* pci,

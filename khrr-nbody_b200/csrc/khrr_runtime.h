@@ -68,19 +68,19 @@ struct StepGraph {
 };
 
 // The mesh-force solver (khrr_set_mesh_solver): its mesh, field ring and
-// per-body gather slot, and the step graphs per (dt, ring rotation, phi).
+// per-body gather slot, and the step graphs per (dt, ring state, phi).
 struct MeshSolver {
     bool on = false;
     khrr_mesh_solver cfg{};
     MeshGeom geom{};
     int64_t cells = 0;
-    DevBuf<double> cell_mass, phi64, cell_acc;  // C, 3 C, 3 C
-    DevBuf<float> mass32, phi32, tab;           // C, 3 C, 3 nx
+    DevBuf<double> cell_mass, phi64, cell_acc;  // C, 4 C (field ring), 3 C
+    DevBuf<float> mass32, phi32, tab;           // C, 4 C (field ring), 3 nx
     DevBuf<int2> pci;                           // npad
     DevBuf<double4> part;                       // npad: {acc, -phi} per body
     DevBuf<unsigned char> ns;                   // npad: 1 for real bodies, 0 for ghosts
     std::vector<int64_t> layout_poff, layout_cnt;  // the layout pci/part/ns were sized for
-    int rot = 0;                                // ring buffer holding phi^{n-1}
+    int rot = kRingStart;                       // ring state: 4 * (phi^{n-1} buffer) + phi^n buffer
     std::map<std::tuple<uint64_t, int, bool>, StepGraph> graphs;
     void drop_graphs() {
         for (auto& kv : graphs) {
@@ -134,9 +134,9 @@ struct khrr_ctx {
     khrr::DevBuf<int> morder;                            // khrr_sort_by_cell: n body indices
     khrr::DevBuf<double> cell_mass, cell_phi, wave_resid;
     int64_t cell_phi_cells = 0;                          // mesh size the cell_phi sums belong to
-    khrr::DevBuf<float> wave_phi, wave_mass, wave_tab;   // 3 C, C, 3 nx
+    khrr::DevBuf<float> wave_phi, wave_mass, wave_tab;   // 4 C (field ring), C, 3 nx
     int wave_nx = 0;
-    int wave_rot = 0;                                    // which buffer holds phi^n
+    int wave_rot = khrr::kRingStart;                     // ring state: 4 * (phi^{n-1} buffer) + phi^n buffer
     bool wave_warm = false;
     std::map<std::pair<int, int>, khrr::StepGraph> wave_graphs;  // (chunk, rotation)
 

@@ -412,6 +412,166 @@ __global__ void __launch_bounds__(kWX * kWY) wave_f32_kernel(float* __restrict__
     }
 }
 
+// Two leap-frog steps per launch (temporal blocking).  A CTA owns a 32 x 8
+// column tile and TZ planes of it and marches up in z.  At each plane it
+// first computes phi^{n+1} on the tile extended by one cell in x and y
+// (34 x 10: its own 256 points plus an 84-point ring spread over every third
+// thread) into a 3-plane shared-memory ring, then phi^{n+2} one plane below
+// from those values (x/y neighbours from shared memory, z neighbours from
+// registers).  Per cell the arithmetic is exactly wave_f32_kernel's, so two
+// launches of that kernel and one of this give identical bits.  It reads
+// phi^n, phi^{n-1} and the mass once and writes phi^{n+1} (inner tile) and
+// phi^{n+2}: 20 bytes per cell for two iterations instead of 32.  out1 and
+// out2 must be buffers this launch does not read (neighbouring CTAs still
+// read phi^{n-1} and phi^n).  Loads for the next plane are issued before the
+// barrier so they overlap the second step.
+constexpr int kT2X = 32, kT2Y = 8;
+constexpr int kT2EX = kT2X + 2, kT2EY = kT2Y + 2;
+constexpr int kT2Ring = 2 * kT2EX + 2 * kT2Y;  // 84 border points of the extended plane
+
+// Inputs of one first-step point at one plane (gathered one plane ahead).
+struct Wave1In {
+    float xm, xp, ym, yp, zp2, po, ms;
+};
+
+__device__ __forceinline__ Wave1In wave1_load(const float* __restrict__ p0, const float* __restrict__ pm,
+                                              const float* __restrict__ mass, int gx, int gy, int z, int NX) {
+    // Coordinates clamped into the mesh: every load is in bounds; values of
+    // points outside the mesh are never used (faces are zero).
+    const int cx = min(max(gx, 0), NX - 1), cy = min(max(gy, 0), NX - 1);
+    const int cz = min(max(z, 0), NX - 1), cz2 = min(max(z + 1, 0), NX - 1);
+    const int64_t sy = NX, sz = static_cast<int64_t>(NX) * NX;
+    const int64_t at = cz * sz + cy * sy + cx;
+    Wave1In r;
+    r.xm = p0[at - (cx > 0 ? 1 : 0)];
+    r.xp = p0[at + (cx < NX - 1 ? 1 : 0)];
+    r.ym = p0[at - (cy > 0 ? sy : 0)];
+    r.yp = p0[at + (cy < NX - 1 ? sy : 0)];
+    r.zp2 = p0[cz2 * sz + cy * sy + cx];  // phi^n one plane above z (the march's next value)
+    r.po = pm[at];
+    r.ms = mass[at];
+    return r;
+}
+
+// One stencil update (wave_f32_kernel's expression) or 0 on faces and
+// outside the mesh.
+__device__ __forceinline__ float wave1_point(const WaveF32& W, float sxy, bool edge_xy, int z, float xm, float xp,
+                                             float ym, float yp, float zm, float c, float zp, float po, float ms) {
+    if (edge_xy || z <= 0 || z >= W.nx - 1) return 0.0f;
+    const float nb = ((xm + xp) + (ym + yp)) + (zm + zp);
+    const float diss = sxy + W.sz[z];
+    const float Q = diss * W.cdt_half;
+    const float w = 1.0f / (1.0f + Q);
+    return fmaf(nb, W.K * w, fmaf(c, W.A * w, fmaf(po, (Q - 1.0f) * w, ms * (W.S * w))));
+}
+
+template <int TZ>
+__global__ void __launch_bounds__(kT2X * kT2Y) wave2_f32_kernel(float* __restrict__ out1, float* __restrict__ out2,
+                                                               const float* __restrict__ p0,
+                                                               const float* __restrict__ pm,
+                                                               const float* __restrict__ mass, const WaveF32 W,
+                                                               double* __restrict__ resid) {
+    __shared__ float s1[3][kT2EY][kT2EX];
+    const int NX = W.nx;
+    const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * kT2X + tx;
+    const int x0 = blockIdx.x * kT2X, y0 = blockIdx.y * kT2Y, z0 = blockIdx.z * TZ;
+    const int64_t sz = static_cast<int64_t>(NX) * NX;
+
+    // Own point (inner tile) and, for every third thread, one ring point.
+    const int ox = x0 + tx, oy = y0 + ty;
+    const bool own_in = ox < NX && oy < NX;
+    const bool has_ring = (tid % 3 == 0) && (tid / 3 < kT2Ring);
+    int rex = 0, rey = 0;
+    if (has_ring) {
+        const int r = tid / 3;
+        if (r < kT2EX) rex = r, rey = 0;
+        else if (r < 2 * kT2EX) rex = r - kT2EX, rey = kT2EY - 1;
+        else if (r < 2 * kT2EX + kT2Y) rex = 0, rey = r - 2 * kT2EX + 1;
+        else rex = kT2EX - 1, rey = r - 2 * kT2EX - kT2Y + 1;
+    }
+    const int rx = x0 - 1 + rex, ry = y0 - 1 + rey;
+    auto edge = [&](int gx, int gy) { return gx <= 0 || gx >= NX - 1 || gy <= 0 || gy >= NX - 1; };
+    auto sxy_of = [&](int gx, int gy) {
+        const int cx = min(max(gx, 0), NX - 1), cy = min(max(gy, 0), NX - 1);
+        return (W.diss_base + W.sx[cx]) + W.sy[cy];
+    };
+    const bool own_edge = edge(ox, oy), ring_edge = edge(rx, ry);
+    const float own_sxy = sxy_of(ox, oy), ring_sxy = sxy_of(rx, ry);
+
+    // phi^n march registers (planes zs - 1, zs, zs + 1) of both points.
+    auto colv = [&](int gx, int gy, int z) {
+        const int cx = min(max(gx, 0), NX - 1), cy = min(max(gy, 0), NX - 1), cz = min(max(z, 0), NX - 1);
+        return p0[cz * sz + static_cast<int64_t>(cy) * NX + cx];
+    };
+    int zs = z0 - 1;  // first first-step plane
+    float oa0 = colv(ox, oy, zs - 1), oa1 = colv(ox, oy, zs);
+    float ra0 = has_ring ? colv(rx, ry, zs - 1) : 0.0f, ra1 = has_ring ? colv(rx, ry, zs) : 0.0f;
+    Wave1In oin = wave1_load(p0, pm, mass, ox, oy, zs, NX);
+    Wave1In rin = has_ring ? wave1_load(p0, pm, mass, rx, ry, zs, NX) : Wave1In{};
+
+    float o1m = 0.0f, o1c = 0.0f;   // own phi^{n+1} at planes zs - 2, zs - 1
+    float om_prev = 0.0f;           // own mass at plane zs - 1
+    float oa_prev = 0.0f;           // own phi^n at plane zs - 1 (before the shift below)
+    double d2 = 0.0, n2 = 0.0;
+    const int zend = min(z0 + TZ, NX);  // last output plane + 1
+    for (int j = 0; zs <= zend; ++j, ++zs) {
+        // First step at plane zs.
+        const float oa2 = oin.zp2, ra2 = rin.zp2;
+        const float o1 = wave1_point(W, own_sxy, own_edge, zs, oin.xm, oin.xp, oin.ym, oin.yp, oa0, oa1, oa2, oin.po,
+                                     oin.ms);
+        s1[j % 3][ty + 1][tx + 1] = o1;
+        if (has_ring)
+            s1[j % 3][rey][rex] = wave1_point(W, ring_sxy, ring_edge, zs, rin.xm, rin.xp, rin.ym, rin.yp, ra0, ra1, ra2,
+                                              rin.po, rin.ms);
+        const float om_cur = oin.ms;
+        oa_prev = oa0;
+        oa0 = oa1, oa1 = oa2;
+        ra0 = ra1, ra1 = ra2;
+        // The next plane's inputs, in flight across the barrier and the second step.
+        if (zs + 1 <= zend) {
+            oin = wave1_load(p0, pm, mass, ox, oy, zs + 1, NX);
+            if (has_ring) rin = wave1_load(p0, pm, mass, rx, ry, zs + 1, NX);
+        }
+        __syncthreads();
+        // Second step at plane k = zs - 1 (needs first-step planes zs - 2 .. zs).
+        const int k = zs - 1;
+        if (j >= 2 && own_in && k < zend) {
+            const float(&pl)[kT2EY][kT2EX] = s1[(j + 2) % 3];  // plane k
+            float o2 = 0.0f;
+            if (!(own_edge || k <= 0 || k >= NX - 1)) {
+                const float nb = ((pl[ty + 1][tx] + pl[ty + 1][tx + 2]) + (pl[ty][tx + 1] + pl[ty + 2][tx + 1])) +
+                                 (o1m + o1);
+                const float diss = own_sxy + W.sz[k];
+                const float Q = diss * W.cdt_half;
+                const float w = 1.0f / (1.0f + Q);
+                o2 = fmaf(nb, W.K * w, fmaf(o1c, W.A * w, fmaf(oa_prev, (Q - 1.0f) * w, om_prev * (W.S * w))));
+            }
+            const int64_t at = k * sz + static_cast<int64_t>(oy) * NX + ox;
+            out1[at] = o1c;
+            out2[at] = o2;
+            if (resid) {
+                const double dd = static_cast<double>(o2) - static_cast<double>(o1c);
+                d2 += dd * dd;
+                n2 += static_cast<double>(o2) * static_cast<double>(o2);
+            }
+        }
+        o1m = o1c;
+        o1c = o1;
+        om_prev = om_cur;
+    }
+    if (resid) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            d2 += __shfl_xor_sync(0xffffffffu, d2, o);
+            n2 += __shfl_xor_sync(0xffffffffu, n2, o);
+        }
+        if (tx == 0) {
+            atomicAdd(&resid[0], d2);
+            atomicAdd(&resid[1], n2);
+        }
+    }
+}
+
 // acc_field (p2mesh-kernel.cuh:169-225) with a 3-D launch over the mesh.
 __global__ void acc_field_kernel(double* __restrict__ cell_acc, double* __restrict__ cell_acc_abs,
                                  const double* __restrict__ phi, int NX, double DX) {
@@ -669,6 +829,39 @@ cudaError_t launch_wave_f32(float* phi_new, const float* phi, const float* phi_o
     } else {
         const dim3 grid((w.nx + kWX - 1) / kWX, (w.nx + kWY - 1) / kWY, (w.nx + 3) / 4);
         wave_f32_kernel<4><<<grid, block, 0, s>>>(phi_new, phi, phi_old, mass, w, resid);
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t enqueue_wave_f32(float* ring, int64_t cells, const float* mass, const WaveF32& w, int k, int st,
+                             double* resid, cudaStream_t s) {
+    const size_t cz = static_cast<size_t>(cells);
+    for (int i = 0; i + 1 < k; i += 2) {
+        int f0, f1;
+        ring_free(st, f0, f1);
+        cudaError_t e = launch_wave2_f32(ring + f0 * cz, ring + f1 * cz, ring + (st % 4) * cz, ring + (st / 4) * cz,
+                                         mass, w, i + 2 == k ? resid : nullptr, s);
+        if (e != cudaSuccess) return e;
+        st = ring_step2(st);
+    }
+    if (k % 2) {
+        int f0, f1;
+        ring_free(st, f0, f1);
+        cudaError_t e = launch_wave_f32(ring + f0 * cz, ring + (st % 4) * cz, ring + (st / 4) * cz, mass, w, resid, s);
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+
+cudaError_t launch_wave2_f32(float* out1, float* out2, const float* phi, const float* phi_old, const float* mass,
+                             const WaveF32& w, double* resid, cudaStream_t s) {
+    const dim3 block(kT2X, kT2Y);
+    if (w.nx >= 192) {
+        const dim3 grid((w.nx + kT2X - 1) / kT2X, (w.nx + kT2Y - 1) / kT2Y, (w.nx + 31) / 32);
+        wave2_f32_kernel<32><<<grid, block, 0, s>>>(out1, out2, phi, phi_old, mass, w, resid);
+    } else {
+        const dim3 grid((w.nx + kT2X - 1) / kT2X, (w.nx + kT2Y - 1) / kT2Y, (w.nx + 15) / 16);
+        wave2_f32_kernel<16><<<grid, block, 0, s>>>(out1, out2, phi, phi_old, mass, w, resid);
     }
     return cudaGetLastError();
 }

@@ -281,7 +281,7 @@ khrr_status khrr_wave_solve(khrr_ctx* c, const khrr_wave_params* p, double tol, 
             cudaGraphDestroy(kv.second.graph);
         }
         c->wave_graphs.clear();
-        if ((st = c->cuda(c->wave_phi.ensure(3 * cz), "alloc")) != KHRR_OK) return st;
+        if ((st = c->cuda(c->wave_phi.ensure(4 * cz), "alloc")) != KHRR_OK) return st;
         if ((st = c->cuda(c->wave_mass.ensure(cz), "alloc")) != KHRR_OK) return st;
         if ((st = c->cuda(c->wave_tab.ensure(3 * static_cast<size_t>(nx)), "alloc")) != KHRR_OK) return st;
         if ((st = c->cuda(c->wave_resid.ensure(2), "alloc")) != KHRR_OK) return st;
@@ -295,11 +295,11 @@ khrr_status khrr_wave_solve(khrr_ctx* c, const khrr_wave_params* p, double tol, 
         return st;
     if ((st = c->cuda(launch_to_float(c->cell_mass.p, c->wave_mass.p, C, s), "mass to float")) != KHRR_OK) return st;
     if (cold || !c->wave_warm) {
-        cudaMemsetAsync(c->wave_phi.p, 0, 3 * cz * sizeof(float), s);
-        c->wave_rot = 0;
+        cudaMemsetAsync(c->wave_phi.p, 0, 4 * cz * sizeof(float), s);
+        c->wave_rot = kRingStart;
     }
     const WaveF32 w = wave_f32(p, c->wave_tab.p);
-    // Graph of one chunk of `check_every` iterations starting at a rotation;
+    // Graph of one chunk of `check_every` iterations starting at a ring state;
     // the last iteration of the chunk reduces the residual.
     auto chunk_graph = [&](int k, int rot, StepGraph** out) -> khrr_status {
         const auto key = std::make_pair(k, rot);
@@ -312,14 +312,7 @@ khrr_status khrr_wave_solve(khrr_ctx* c, const khrr_wave_params* p, double tol, 
         khrr_status e = c->cuda(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "begin capture");
         if (e != KHRR_OK) return e;
         cudaMemsetAsync(c->wave_resid.p, 0, 2 * sizeof(double), s);
-        int r = rot;
-        for (int i = 0; i < k; ++i) {
-            float* old = c->wave_phi.p + static_cast<size_t>(r) * cz;
-            float* cur = c->wave_phi.p + static_cast<size_t>((r + 1) % 3) * cz;
-            float* nxt = c->wave_phi.p + static_cast<size_t>((r + 2) % 3) * cz;
-            launch_wave_f32(nxt, cur, old, c->wave_mass.p, w, i == k - 1 ? c->wave_resid.p : nullptr, s);
-            r = (r + 1) % 3;
-        }
+        enqueue_wave_f32(c->wave_phi.p, C, c->wave_mass.p, w, k, rot, c->wave_resid.p, s);
         cudaGraph_t graph = nullptr;
         if ((e = c->cuda(cudaStreamEndCapture(s, &graph), "end capture")) != KHRR_OK) return e;
         g.graph = graph;
@@ -349,7 +342,7 @@ khrr_status khrr_wave_solve(khrr_ctx* c, const khrr_wave_params* p, double tol, 
             return st;
         if ((st = c->cuda(cudaStreamSynchronize(s), "wave sync")) != KHRR_OK) return st;
         done += k;
-        c->wave_rot = (c->wave_rot + k) % 3;
+        c->wave_rot = ring_after_f32(c->wave_rot, k);
         rel = r2[1] > 0.0 ? std::sqrt(r2[0] / r2[1]) : (r2[0] > 0.0 ? INFINITY : 0.0);
         if (rel < tol) break;
     }
@@ -357,7 +350,7 @@ khrr_status khrr_wave_solve(khrr_ctx* c, const khrr_wave_params* p, double tol, 
     if (iters) *iters = done;
     if (resid) *resid = rel;
     if (phi_out) {
-        const float* cur = c->wave_phi.p + static_cast<size_t>((c->wave_rot + 1) % 3) * cz;
+        const float* cur = c->wave_phi.p + static_cast<size_t>(c->wave_rot % 4) * cz;
         if ((st = c->cuda(cudaMemcpyAsync(phi_out, cur, cz * sizeof(float), cudaMemcpyDeviceToHost, s), "download")) !=
             KHRR_OK)
             return st;
@@ -449,9 +442,9 @@ khrr_status khrr_set_mesh_solver(khrr_ctx* c, const khrr_mesh_solver* p) {
     if ((st = c->cuda(M.cell_mass.ensure(cz), "alloc")) != KHRR_OK) return st;
     if ((st = c->cuda(M.cell_acc.ensure(3 * cz), "alloc")) != KHRR_OK) return st;
     if (p->fp64) {
-        if ((st = c->cuda(M.phi64.ensure(3 * cz), "alloc")) != KHRR_OK) return st;
+        if ((st = c->cuda(M.phi64.ensure(4 * cz), "alloc")) != KHRR_OK) return st;
     } else {
-        if ((st = c->cuda(M.phi32.ensure(3 * cz), "alloc")) != KHRR_OK) return st;
+        if ((st = c->cuda(M.phi32.ensure(4 * cz), "alloc")) != KHRR_OK) return st;
         if ((st = c->cuda(M.mass32.ensure(cz), "alloc")) != KHRR_OK) return st;
         if ((st = c->cuda(M.tab.ensure(3 * static_cast<size_t>(nx)), "alloc")) != KHRR_OK) return st;
         std::vector<float> tab;
@@ -464,11 +457,11 @@ khrr_status khrr_set_mesh_solver(khrr_ctx* c, const khrr_mesh_solver* p) {
     M.cfg = *p;
     M.geom = g;
     M.cells = C;
-    M.rot = 0;
+    M.rot = kRingStart;
     M.on = true;
     // The field starts at zero, as the reference's freshly allocated arrays.
-    if (p->fp64) cudaMemsetAsync(M.phi64.p, 0, 3 * cz * sizeof(double), c->stream);
-    else cudaMemsetAsync(M.phi32.p, 0, 3 * cz * sizeof(float), c->stream);
+    if (p->fp64) cudaMemsetAsync(M.phi64.p, 0, 4 * cz * sizeof(double), c->stream);
+    else cudaMemsetAsync(M.phi32.p, 0, 4 * cz * sizeof(float), c->stream);
     return khrr_synchronize(c);
 }
 
@@ -477,7 +470,7 @@ khrr_status khrr_mesh_solver_phi(khrr_ctx* c, double* cell_phi) {
     MeshSolver& M = c->msolver;
     if (!M.on) return c->fail(KHRR_ERR_STATE, "no mesh solver set");
     const size_t cz = static_cast<size_t>(M.cells);
-    const size_t cur = static_cast<size_t>((M.rot + 1) % 3) * cz;
+    const size_t cur = static_cast<size_t>(M.rot % 4) * cz;
     khrr_status st;
     if (M.cfg.fp64) {
         st = c->cuda(cudaMemcpyAsync(cell_phi, M.phi64.p + cur, cz * sizeof(double), cudaMemcpyDeviceToHost, c->stream),
@@ -520,7 +513,7 @@ khrr_status khrr_ctx::mesh_ensure_layout() {
 }
 
 // calc_acceleration_by_grid (nbody.cu:183-285) at positions x: deposit, `iters`
-// stencil iterations from ring rotation rot0, gradient, gather into M.part.
+// stencil iterations from ring state rot0, gradient, gather into M.part.
 khrr_status khrr_ctx::mesh_enqueue_force(const double* x, int iters, int rot0) {
     MeshSolver& M = msolver;
     const khrr_mesh_solver& P = M.cfg;
@@ -539,13 +532,15 @@ khrr_status khrr_ctx::mesh_enqueue_force(const double* x, int iters, int rot0) {
     int r = rot0;
     if (P.fp64) {
         const WaveConsts w = wave_consts(&P.wave);
-        for (int i = 0; i < iters; ++i, r = (r + 1) % 3) {
-            double* old = M.phi64.p + static_cast<size_t>(r) * cz;
-            double* cur = M.phi64.p + static_cast<size_t>((r + 1) % 3) * cz;
-            double* nxt = M.phi64.p + static_cast<size_t>((r + 2) % 3) * cz;
+        for (int i = 0; i < iters; ++i, r = ring_step1(r)) {
+            int f0, f1;
+            ring_free(r, f0, f1);
+            double* old = M.phi64.p + static_cast<size_t>(r / 4) * cz;
+            double* cur = M.phi64.p + static_cast<size_t>(r % 4) * cz;
+            double* nxt = M.phi64.p + static_cast<size_t>(f0) * cz;
             if ((st = cuda(launch_wave_f64(nxt, cur, old, M.cell_mass.p, w, s), "wave")) != KHRR_OK) return st;
         }
-        const double* cur = M.phi64.p + static_cast<size_t>((r + 1) % 3) * cz;
+        const double* cur = M.phi64.p + static_cast<size_t>(r % 4) * cz;
         if ((st = cuda(launch_acc_field(M.cell_acc.p, nullptr, cur, nx, P.wave.dx, s), "acc_field")) != KHRR_OK)
             return st;
         for (size_t k = 0; k < cnt.size(); ++k) {
@@ -559,13 +554,10 @@ khrr_status khrr_ctx::mesh_enqueue_force(const double* x, int iters, int rot0) {
     }
     if ((st = cuda(launch_to_float(M.cell_mass.p, M.mass32.p, M.cells, s), "mass to float")) != KHRR_OK) return st;
     const WaveF32 w = wave_f32(&P.wave, M.tab.p);
-    for (int i = 0; i < iters; ++i, r = (r + 1) % 3) {
-        float* old = M.phi32.p + static_cast<size_t>(r) * cz;
-        float* cur = M.phi32.p + static_cast<size_t>((r + 1) % 3) * cz;
-        float* nxt = M.phi32.p + static_cast<size_t>((r + 2) % 3) * cz;
-        if ((st = cuda(launch_wave_f32(nxt, cur, old, M.mass32.p, w, nullptr, s), "wave")) != KHRR_OK) return st;
-    }
-    const float* cur = M.phi32.p + static_cast<size_t>((r + 1) % 3) * cz;
+    if ((st = cuda(enqueue_wave_f32(M.phi32.p, M.cells, M.mass32.p, w, iters, r, nullptr, s), "wave")) != KHRR_OK)
+        return st;
+    r = ring_after_f32(r, iters);
+    const float* cur = M.phi32.p + static_cast<size_t>(r % 4) * cz;
     if ((st = cuda(launch_acc_field_f32(M.cell_acc.p, cur, nx, P.wave.dx, s), "acc_field")) != KHRR_OK) return st;
     for (size_t k = 0; k < cnt.size(); ++k) {
         const int64_t o = poff[k];
@@ -609,10 +601,10 @@ khrr_status khrr_ctx::mesh_forces(int flags) {
     khrr_status st = mesh_ensure_layout();
     if (st != KHRR_OK) return st;
     const size_t cz = static_cast<size_t>(M.cells);
-    if (M.cfg.fp64) cudaMemsetAsync(M.phi64.p, 0, 3 * cz * sizeof(double), stream);
-    else cudaMemsetAsync(M.phi32.p, 0, 3 * cz * sizeof(float), stream);
-    if ((st = mesh_enqueue_force(pos.p, M.cfg.setup_iters, 0)) != KHRR_OK) return st;
-    M.rot = M.cfg.setup_iters % 3;
+    if (M.cfg.fp64) cudaMemsetAsync(M.phi64.p, 0, 4 * cz * sizeof(double), stream);
+    else cudaMemsetAsync(M.phi32.p, 0, 4 * cz * sizeof(float), stream);
+    if ((st = mesh_enqueue_force(pos.p, M.cfg.setup_iters, kRingStart)) != KHRR_OK) return st;
+    M.rot = M.cfg.fp64 ? ring_after_f64(kRingStart, M.cfg.setup_iters) : ring_after_f32(kRingStart, M.cfg.setup_iters);
     StepArgs sa = mesh_step_args(this, 0.0);
     sa.want_phi = (flags & KHRR_PHI) ? 1 : 0;
     if ((st = cuda(launch_collect(sa, (flags & KHRR_ACC) != 0, false, stream), "collect")) != KHRR_OK) return st;
@@ -667,7 +659,7 @@ khrr_status khrr_ctx::mesh_step(double dt, int nsteps, int flags) {
             it = M.graphs.emplace(key, g).first;
         }
         if ((st = cuda(cudaGraphLaunch(it->second.exec, stream), "graph launch")) != KHRR_OK) return st;
-        M.rot = (M.rot + iters) % 3;
+        M.rot = M.cfg.fp64 ? ring_after_f64(M.rot, iters) : ring_after_f32(M.rot, iters);
     }
     predicted = true;
     pred_dt = dt;

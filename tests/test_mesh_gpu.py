@@ -226,3 +226,30 @@ def test_wave_solve_fp32_matches_restatement_and_converges(ctx, oracle):
     assert res3 < res2
     it4, res4, _ = ctx.wave_solve(W, tol=res3 * 1.5, max_iter=100000, check_every=10)
     assert res4 < res3 * 1.5 and it4 < 100000
+
+
+@pytest.mark.parametrize("nx,max_iter,check_every", [(37, 7, 3), (40, 6, 6), (200, 5, 5)])
+def test_wave_solve_pairs_and_singles_bit_exact(ctx, oracle, nx, max_iter, check_every):
+    """Iterations run in pairs through the two-step kernel and, for an odd
+    count, one single step: the field equals the oracle's FP32 restatement
+    bit for bit (meshes that are not multiples of the 32 x 8 x TZ tile, and
+    the TZ = 32 shape from nx = 192 up), and the residual of the last
+    iteration matches the FP64 norm of the oracle's last step."""
+    import khrr
+    pos, vel, mass, eps2 = galaxy_state(2048, 4096, 18)
+    L = 3.0
+    dx = 2 * L / nx
+    ctx.upload(pos, vel, mass, eps2)
+    b = ctx.bin((-L,) * 3, (dx,) * 3, (nx, nx, nx))
+    W = khrr.WaveParams.make(nx, dx)
+    it, res, phi = ctx.wave_solve(W, tol=0.0, max_iter=max_iter, check_every=check_every, cold=True)
+    assert it == max_iter
+    Wo = oracle.wave_params(nx, dx)
+    m32 = b["cell_mass"].astype(np.float32)
+    prev, cur = np.zeros(nx ** 3, np.float32), np.zeros(nx ** 3, np.float32)
+    for _ in range(max_iter):
+        prev, cur = cur, oracle.wave_iter_f32(Wo, cur, prev, m32)
+    assert np.array_equal(phi, cur)
+    d = cur.astype(np.float64) - prev.astype(np.float64)
+    want = np.sqrt((d * d).sum() / (cur.astype(np.float64) ** 2).sum())
+    assert abs(res - want) <= 1e-12 * want
