@@ -60,7 +60,7 @@ khrr_status khrr_ctx::check_device_flag() {
     if (e != cudaSuccess) return cuda(e, "device error flag");
     if (flag & kErrTimeout) {
         cudaMemsetAsync(errflag.p, 0, sizeof(unsigned), stream);
-        return fail(KHRR_ERR_TIMEOUT, "a force kernel gave up waiting for a tile copy (bounded wait)");
+        return fail(KHRR_ERR_TIMEOUT, "a kernel gave up waiting for an asynchronous copy (bounded wait)");
     }
     return KHRR_OK;
 }

@@ -2,6 +2,7 @@
 // runtime (*.cpp) of libkhrr.  Not part of the public ABI (include/khrr.h).
 #pragma once
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -210,10 +211,24 @@ inline int ring_after_f64(int st, int k) {
     for (int i = 0; i < k; ++i) st = ring_step1(st);
     return st;
 }
+// Tensor maps (40 x 12 x 1 float boxes) of the four ring buffers and the
+// FP32 mass of one nx^3 mesh, for the tensor-copy stencil; ok is false when
+// they do not exist (nx % 4 != 0, or no driver entry point), and the stencil
+// then loads through the cache instead.
+struct WaveMaps {
+    CUtensorMap ring[4];
+    CUtensorMap mass;
+    bool ok = false;
+};
+// The two-step stencil fed by tensor copies (see wave2_tma_kernel).
+cudaError_t launch_wave2_tma(float* out1, float* out2, const CUtensorMap& phi, const CUtensorMap& phi_old,
+                             const CUtensorMap& mass, const WaveF32& w, double* resid, unsigned* err, cudaStream_t s);
 // Enqueues k FP32 iterations on the ring (4 buffers of cells floats) from
-// state st; resid (may be NULL) is reduced by the last one.
+// state st; resid (may be NULL) is reduced by the last one.  With maps (ok)
+// the pairs run through the tensor-copy kernel, whose bounded waits report
+// into err.
 cudaError_t enqueue_wave_f32(float* ring, int64_t cells, const float* mass, const WaveF32& w, int k, int st,
-                             double* resid, cudaStream_t s);
+                             double* resid, cudaStream_t s, const WaveMaps* maps = nullptr, unsigned* err = nullptr);
 cudaError_t launch_acc_field(double* cell_acc, double* cell_acc_abs, const double* phi, int nx, double dx,
                              cudaStream_t s);
 cudaError_t launch_apply(double* pacc, double* pval, const double* cacc, const double* cval, const int2* pci,

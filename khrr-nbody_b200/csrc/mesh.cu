@@ -25,6 +25,7 @@
 #include <cmath>
 #include <cstdint>
 
+#include "async_copy.cuh"
 #include "khrr_internal.h"
 
 namespace khrr {
@@ -572,6 +573,147 @@ __global__ void __launch_bounds__(kT2X * kT2Y) wave2_f32_kernel(float* __restric
     }
 }
 
+// The same two steps fed by tensor copies.  Thread 0 streams, plane by
+// plane, three 40 x 12 boxes (phi^n, phi^{n-1}, mass at x0-4 .. x0+35,
+// y0-2 .. y0+9; outside the mesh they read as zero) into a kTmaD-stage
+// shared-memory ring on mbarriers, up to kTmaD planes ahead of the stencil;
+// the stencil then reads only shared memory.  Plane q of a CTA is z0-2+q;
+// step 1 at plane zs = z0-1+j reads planes j, j+1, j+2 and step 2 at zs-1
+// reads plane j, so after iteration j's barrier plane j-1 is free and its
+// stage takes plane j-1+kTmaD.  Needs nx % 4 == 0 (16-byte row strides).
+constexpr int kTmaD = 7;
+constexpr int kTmaBX = 40, kTmaBY = 12;
+constexpr unsigned kTmaBoxBytes = kTmaBX * kTmaBY * 4u;
+
+template <int TZ>
+__global__ void __launch_bounds__(kT2X * kT2Y) wave2_tma_kernel(float* __restrict__ out1, float* __restrict__ out2,
+                                                               const __grid_constant__ CUtensorMap tp0,
+                                                               const __grid_constant__ CUtensorMap tpm,
+                                                               const __grid_constant__ CUtensorMap tms,
+                                                               const WaveF32 W, double* __restrict__ resid,
+                                                               unsigned* __restrict__ err) {
+    __shared__ alignas(128) float ring[kTmaD][3][kTmaBY][kTmaBX];
+    __shared__ float s1[3][kT2EY][kT2EX];
+    __shared__ alignas(8) uint64_t full[kTmaD];
+    const int NX = W.nx;
+    const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * kT2X + tx;
+    const int x0 = blockIdx.x * kT2X, y0 = blockIdx.y * kT2Y, z0 = blockIdx.z * TZ;
+    const int zend = min(z0 + TZ, NX);
+    const int P = zend - z0 + 4;  // planes z0-2 .. zend+1
+
+    if (tid == 0) {
+        for (int s = 0; s < kTmaD; ++s) mbar_init(&full[s], 1);
+        fence_mbar_init();
+    }
+    __syncthreads();
+    auto issue = [&](int q) {
+        const int s = q % kTmaD, z = z0 - 2 + q;
+        mbar_arrive_expect_tx(&full[s], 3 * kTmaBoxBytes);
+        tensor_copy_3d_g2s(&ring[s][0][0][0], &tp0, x0 - 4, y0 - 2, z, &full[s]);
+        tensor_copy_3d_g2s(&ring[s][1][0][0], &tpm, x0 - 4, y0 - 2, z, &full[s]);
+        tensor_copy_3d_g2s(&ring[s][2][0][0], &tms, x0 - 4, y0 - 2, z, &full[s]);
+    };
+    if (tid == 0)
+        for (int q = 0; q < kTmaD && q < P; ++q) issue(q);
+
+    const int ox = x0 + tx, oy = y0 + ty;
+    const bool own_in = ox < NX && oy < NX;
+    const bool has_ring = (tid % 3 == 0) && (tid / 3 < kT2Ring);
+    int rex = 0, rey = 0;
+    if (has_ring) {
+        const int r = tid / 3;
+        if (r < kT2EX) rex = r, rey = 0;
+        else if (r < 2 * kT2EX) rex = r - kT2EX, rey = kT2EY - 1;
+        else if (r < 2 * kT2EX + kT2Y) rex = 0, rey = r - 2 * kT2EX + 1;
+        else rex = kT2EX - 1, rey = r - 2 * kT2EX - kT2Y + 1;
+    }
+    const int rx = x0 - 1 + rex, ry = y0 - 1 + rey;
+    auto edge = [&](int gx, int gy) { return gx <= 0 || gx >= NX - 1 || gy <= 0 || gy >= NX - 1; };
+    auto sxy_of = [&](int gx, int gy) {
+        const int cx = min(max(gx, 0), NX - 1), cy = min(max(gy, 0), NX - 1);
+        return (W.diss_base + W.sx[cx]) + W.sy[cy];
+    };
+    const bool own_edge = edge(ox, oy), ring_edge = edge(rx, ry);
+    const float own_sxy = sxy_of(ox, oy), ring_sxy = sxy_of(rx, ry);
+    // Box coordinates: extended-tile point (ex, ey) sits at (ex + 3, ey + 1).
+    const int oxi = tx + 4, oyi = ty + 2, rxi = rex + 3, ryi = rey + 1;
+
+    bool ok = mbar_wait_bounded(&full[0], 0u) && mbar_wait_bounded(&full[1 % kTmaD], 0u);
+    float o1m = 0.0f, o1c = 0.0f;
+    double d2 = 0.0, n2 = 0.0;
+    for (int j = 0; j + 2 < P; ++j) {
+        const int zs = z0 - 1 + j;
+        const int q2 = j + 2;
+        if (ok) ok = mbar_wait_bounded(&full[q2 % kTmaD], static_cast<unsigned>((q2 / kTmaD) & 1));
+        float o1 = 0.0f;
+        if (ok) {
+            const float(*a)[kTmaBX] = ring[j % kTmaD][0];        // phi^n at zs - 1
+            const float(*b)[kTmaBX] = ring[(j + 1) % kTmaD][0];  // phi^n at zs
+            const float(*c)[kTmaBX] = ring[q2 % kTmaD][0];       // phi^n at zs + 1
+            const float(*pm)[kTmaBX] = ring[(j + 1) % kTmaD][1];
+            const float(*ms)[kTmaBX] = ring[(j + 1) % kTmaD][2];
+            o1 = wave1_point(W, own_sxy, own_edge, zs, b[oyi][oxi - 1], b[oyi][oxi + 1], b[oyi - 1][oxi],
+                             b[oyi + 1][oxi], a[oyi][oxi], b[oyi][oxi], c[oyi][oxi], pm[oyi][oxi], ms[oyi][oxi]);
+            s1[j % 3][ty + 1][tx + 1] = o1;
+            if (has_ring)
+                s1[j % 3][rey][rex] = wave1_point(W, ring_sxy, ring_edge, zs, b[ryi][rxi - 1], b[ryi][rxi + 1],
+                                                  b[ryi - 1][rxi], b[ryi + 1][rxi], a[ryi][rxi], b[ryi][rxi],
+                                                  c[ryi][rxi], pm[ryi][rxi], ms[ryi][rxi]);
+        }
+        if (__syncthreads_or(!ok)) {
+            if (tid == 0) {
+                atomicOr(err, kErrTimeout);
+                // Let copies still in flight into this CTA's ring land:
+                // planes [0, issued) have been issued so far.
+                const int issued = min(P, max(kTmaD, j - 1 + kTmaD));
+                for (int q = j; q < issued; ++q)
+                    (void)mbar_wait_bounded(&full[q % kTmaD], static_cast<unsigned>((q / kTmaD) & 1));
+            }
+            return;
+        }
+        // Plane j - 1 was last read before this barrier: refill its stage.
+        if (tid == 0 && j >= 1 && j - 1 + kTmaD < P) {
+            fence_proxy_async();
+            issue(j - 1 + kTmaD);
+        }
+        const int k = zs - 1;
+        if (j >= 2 && own_in) {
+            const float(*pl)[kT2EX] = s1[(j + 2) % 3];  // phi^{n+1} at k
+            float o2 = 0.0f;
+            if (!(own_edge || k <= 0 || k >= NX - 1)) {
+                const float old = ring[j % kTmaD][0][oyi][oxi], mk = ring[j % kTmaD][2][oyi][oxi];
+                const float nb = ((pl[ty + 1][tx] + pl[ty + 1][tx + 2]) + (pl[ty][tx + 1] + pl[ty + 2][tx + 1])) +
+                                 (o1m + o1);
+                const float diss = own_sxy + W.sz[k];
+                const float Q = diss * W.cdt_half;
+                const float w = 1.0f / (1.0f + Q);
+                o2 = fmaf(nb, W.K * w, fmaf(o1c, W.A * w, fmaf(old, (Q - 1.0f) * w, mk * (W.S * w))));
+            }
+            const int64_t at = k * static_cast<int64_t>(NX) * NX + static_cast<int64_t>(oy) * NX + ox;
+            out1[at] = o1c;
+            out2[at] = o2;
+            if (resid) {
+                const double dd = static_cast<double>(o2) - static_cast<double>(o1c);
+                d2 += dd * dd;
+                n2 += static_cast<double>(o2) * static_cast<double>(o2);
+            }
+        }
+        o1m = o1c;
+        o1c = o1;
+    }
+    if (resid) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            d2 += __shfl_xor_sync(0xffffffffu, d2, o);
+            n2 += __shfl_xor_sync(0xffffffffu, n2, o);
+        }
+        if (tx == 0) {
+            atomicAdd(&resid[0], d2);
+            atomicAdd(&resid[1], n2);
+        }
+    }
+}
+
 // acc_field (p2mesh-kernel.cuh:169-225) with a 3-D launch over the mesh.
 __global__ void acc_field_kernel(double* __restrict__ cell_acc, double* __restrict__ cell_acc_abs,
                                  const double* __restrict__ phi, int NX, double DX) {
@@ -834,13 +976,17 @@ cudaError_t launch_wave_f32(float* phi_new, const float* phi, const float* phi_o
 }
 
 cudaError_t enqueue_wave_f32(float* ring, int64_t cells, const float* mass, const WaveF32& w, int k, int st,
-                             double* resid, cudaStream_t s) {
+                             double* resid, cudaStream_t s, const WaveMaps* maps, unsigned* err) {
     const size_t cz = static_cast<size_t>(cells);
+    const bool tma = maps && maps->ok && err;
     for (int i = 0; i + 1 < k; i += 2) {
         int f0, f1;
         ring_free(st, f0, f1);
-        cudaError_t e = launch_wave2_f32(ring + f0 * cz, ring + f1 * cz, ring + (st % 4) * cz, ring + (st / 4) * cz,
-                                         mass, w, i + 2 == k ? resid : nullptr, s);
+        double* r = i + 2 == k ? resid : nullptr;
+        cudaError_t e = tma ? launch_wave2_tma(ring + f0 * cz, ring + f1 * cz, maps->ring[st % 4], maps->ring[st / 4],
+                                               maps->mass, w, r, err, s)
+                            : launch_wave2_f32(ring + f0 * cz, ring + f1 * cz, ring + (st % 4) * cz,
+                                               ring + (st / 4) * cz, mass, w, r, s);
         if (e != cudaSuccess) return e;
         st = ring_step2(st);
     }
@@ -851,6 +997,19 @@ cudaError_t enqueue_wave_f32(float* ring, int64_t cells, const float* mass, cons
         if (e != cudaSuccess) return e;
     }
     return cudaSuccess;
+}
+
+cudaError_t launch_wave2_tma(float* out1, float* out2, const CUtensorMap& phi, const CUtensorMap& phi_old,
+                             const CUtensorMap& mass, const WaveF32& w, double* resid, unsigned* err, cudaStream_t s) {
+    const dim3 block(kT2X, kT2Y);
+    if (w.nx >= 192) {
+        const dim3 grid((w.nx + kT2X - 1) / kT2X, (w.nx + kT2Y - 1) / kT2Y, (w.nx + 31) / 32);
+        wave2_tma_kernel<32><<<grid, block, 0, s>>>(out1, out2, phi, phi_old, mass, w, resid, err);
+    } else {
+        const dim3 grid((w.nx + kT2X - 1) / kT2X, (w.nx + kT2Y - 1) / kT2Y, (w.nx + 15) / 16);
+        wave2_tma_kernel<16><<<grid, block, 0, s>>>(out1, out2, phi, phi_old, mass, w, resid, err);
+    }
+    return cudaGetLastError();
 }
 
 cudaError_t launch_wave2_f32(float* out1, float* out2, const float* phi, const float* phi_old, const float* mass,

@@ -1,10 +1,12 @@
 // C ABI of the p2mesh path: kernel-level entry points (the reference's
 // pointers and layouts) and the context-level pipeline khrr_bin /
 // khrr_wave_solve.
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <vector>
 
@@ -77,6 +79,52 @@ void sponge_tables(const khrr_wave_params* p, std::vector<float>& t) {
         t[nx + i] = static_cast<float>(sy);
         t[2 * nx + i] = static_cast<float>(sy);  // the z test is the y test
     }
+}
+
+// cuTensorMapEncodeTiled through the runtime's driver entry point (the
+// library does not link libcuda directly).
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+    static const PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            p = nullptr;
+        return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    }();
+    return fn;
+}
+
+// One nx^3 float field as a 3-D tensor with 40 x 12 x 1 boxes (the planes the
+// tensor-copy stencil streams); outside coordinates read as zero.
+bool make_box_map(CUtensorMap* m, const float* base, int nx) {
+    const auto enc = tensor_map_encoder();
+    if (!enc) return false;
+    const cuuint64_t n = static_cast<cuuint64_t>(nx);
+    const cuuint64_t dims[3] = {n, n, n};
+    const cuuint64_t strides[2] = {n * 4, n * n * 4};
+    const cuuint32_t box[3] = {40, 12, 1};
+    const cuuint32_t elem[3] = {1, 1, 1};
+    return enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<float*>(base), dims, strides, box, elem,
+               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// Maps of the four ring buffers and the mass.  The tensor-copy stencil needs
+// 16-byte row strides (nx % 4 == 0) and a mesh at least one box wide;
+// KHRR_WAVE_TMA=0 in the environment turns it off.
+void make_wave_maps(WaveMaps* w, float* ring, const float* mass, int nx) {
+    w->ok = false;
+    static const bool enabled = [] {
+        const char* e = std::getenv("KHRR_WAVE_TMA");
+        return !(e && e[0] == '0');
+    }();
+    if (!enabled || nx % 4 != 0 || nx < 40) return;
+    const size_t cz = static_cast<size_t>(nx) * nx * nx;
+    for (int b = 0; b < 4; ++b)
+        if (!make_box_map(&w->ring[b], ring + b * cz, nx)) return;
+    if (!make_box_map(&w->mass, mass, nx)) return;
+    w->ok = true;
 }
 
 WaveF32 wave_f32(const khrr_wave_params* p, const float* tab) {
@@ -299,6 +347,7 @@ khrr_status khrr_wave_solve(khrr_ctx* c, const khrr_wave_params* p, double tol, 
         c->wave_rot = kRingStart;
     }
     const WaveF32 w = wave_f32(p, c->wave_tab.p);
+    make_wave_maps(&c->wave_maps, c->wave_phi.p, c->wave_mass.p, p->nx);
     // Graph of one chunk of `check_every` iterations starting at a ring state;
     // the last iteration of the chunk reduces the residual.
     auto chunk_graph = [&](int k, int rot, StepGraph** out) -> khrr_status {
@@ -312,7 +361,8 @@ khrr_status khrr_wave_solve(khrr_ctx* c, const khrr_wave_params* p, double tol, 
         khrr_status e = c->cuda(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "begin capture");
         if (e != KHRR_OK) return e;
         cudaMemsetAsync(c->wave_resid.p, 0, 2 * sizeof(double), s);
-        enqueue_wave_f32(c->wave_phi.p, C, c->wave_mass.p, w, k, rot, c->wave_resid.p, s);
+        enqueue_wave_f32(c->wave_phi.p, C, c->wave_mass.p, w, k, rot, c->wave_resid.p, s, &c->wave_maps,
+                         c->errflag.p);
         cudaGraph_t graph = nullptr;
         if ((e = c->cuda(cudaStreamEndCapture(s, &graph), "end capture")) != KHRR_OK) return e;
         g.graph = graph;
@@ -341,6 +391,7 @@ khrr_status khrr_wave_solve(khrr_ctx* c, const khrr_wave_params* p, double tol, 
             KHRR_OK)
             return st;
         if ((st = c->cuda(cudaStreamSynchronize(s), "wave sync")) != KHRR_OK) return st;
+        if ((st = c->check_device_flag()) != KHRR_OK) return st;
         done += k;
         c->wave_rot = ring_after_f32(c->wave_rot, k);
         rel = r2[1] > 0.0 ? std::sqrt(r2[0] / r2[1]) : (r2[0] > 0.0 ? INFINITY : 0.0);
@@ -453,6 +504,7 @@ khrr_status khrr_set_mesh_solver(khrr_ctx* c, const khrr_mesh_solver* p) {
                                           c->stream),
                           "upload")) != KHRR_OK)
             return st;
+        make_wave_maps(&M.maps, M.phi32.p, M.mass32.p, nx);
     }
     M.cfg = *p;
     M.geom = g;
@@ -554,7 +606,8 @@ khrr_status khrr_ctx::mesh_enqueue_force(const double* x, int iters, int rot0) {
     }
     if ((st = cuda(launch_to_float(M.cell_mass.p, M.mass32.p, M.cells, s), "mass to float")) != KHRR_OK) return st;
     const WaveF32 w = wave_f32(&P.wave, M.tab.p);
-    if ((st = cuda(enqueue_wave_f32(M.phi32.p, M.cells, M.mass32.p, w, iters, r, nullptr, s), "wave")) != KHRR_OK)
+    if ((st = cuda(enqueue_wave_f32(M.phi32.p, M.cells, M.mass32.p, w, iters, r, nullptr, s, &M.maps, errflag.p),
+                   "wave")) != KHRR_OK)
         return st;
     r = ring_after_f32(r, iters);
     const float* cur = M.phi32.p + static_cast<size_t>(r % 4) * cz;
