@@ -174,12 +174,6 @@ cudaError_t launch_wave_f64(double* phi_new, const double* phi, const double* ph
                             const WaveConsts& w, cudaStream_t s);
 cudaError_t launch_wave_f32(float* phi_new, const float* phi, const float* phi_old, const float* mass,
                             const WaveF32& w, double* resid, cudaStream_t s);
-// Two FP32 iterations in one launch: out1 = phi^{n+1}, out2 = phi^{n+2}
-// (bit-identical to two launch_wave_f32 calls); resid (may be NULL) sums
-// (phi^{n+2} - phi^{n+1})^2 and (phi^{n+2})^2.  out1 and out2 must differ
-// from phi and phi_old.
-cudaError_t launch_wave2_f32(float* out1, float* out2, const float* phi, const float* phi_old, const float* mass,
-                             const WaveF32& w, double* resid, cudaStream_t s);
 // The four-buffer field ring of the FP32 solver: state = 4 * old + cur; a
 // single iteration writes the lower free buffer (state -> 4 * cur + f0), a
 // pair writes f0 and f1 (state -> 4 * f0 + f1).
@@ -220,7 +214,10 @@ struct WaveMaps {
     CUtensorMap mass;
     bool ok = false;
 };
-// The two-step stencil fed by tensor copies (see wave2_tma_kernel).
+// Two FP32 iterations in one launch fed by tensor copies (wave2_tma_kernel):
+// out1 = phi^{n+1}, out2 = phi^{n+2}, bit-identical to two launch_wave_f32
+// calls; resid (may be NULL) sums (phi^{n+2} - phi^{n+1})^2 and (phi^{n+2})^2.
+// out1 and out2 must differ from the buffers of phi and phi_old.
 cudaError_t launch_wave2_tma(float* out1, float* out2, const CUtensorMap& phi, const CUtensorMap& phi_old,
                              const CUtensorMap& mass, const WaveF32& w, double* resid, unsigned* err, cudaStream_t s);
 // Enqueues k FP32 iterations on the ring (4 buffers of cells floats) from

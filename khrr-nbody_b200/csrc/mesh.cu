@@ -389,7 +389,7 @@ __global__ void __launch_bounds__(kWX * kWY) wave_f32_kernel(float* __restrict__
                 const float nb = ((xm[u] + xp[u]) + (ym[u] + yp[u])) + (c[u] + c[u + 2]);
                 const float diss = sxy + W.sz[z];
                 const float Q = diss * W.cdt_half;
-                const float w = 1.0f / (1.0f + Q);
+                const float w = __frcp_rn(1.0f + Q);  // correctly rounded: the bits of 1.0f / (1.0f + Q)
                 out = fmaf(nb, W.K * w, fmaf(c[u + 1], W.A * w, fmaf(po[u], (Q - 1.0f) * w, ms[u] * (W.S * w))));
             }
             phi_new[at] = out;
@@ -413,46 +413,31 @@ __global__ void __launch_bounds__(kWX * kWY) wave_f32_kernel(float* __restrict__
     }
 }
 
-// Two leap-frog steps per launch (temporal blocking).  A CTA owns a 32 x 8
-// column tile and TZ planes of it and marches up in z.  At each plane it
-// first computes phi^{n+1} on the tile extended by one cell in x and y
-// (34 x 10: its own 256 points plus an 84-point ring spread over every third
-// thread) into a 3-plane shared-memory ring, then phi^{n+2} one plane below
-// from those values (x/y neighbours from shared memory, z neighbours from
-// registers).  Per cell the arithmetic is exactly wave_f32_kernel's, so two
+// Two leap-frog steps per launch (temporal blocking), fed by tensor copies.
+// A CTA owns a 32 x 8 column tile and TZ planes of it and marches up in z.
+// Thread 0 streams, plane by plane, three 40 x 12 boxes (phi^n, phi^{n-1},
+// mass at x0-4 .. x0+35, y0-2 .. y0+9; outside the mesh they read as zero)
+// into a kTmaD-stage shared-memory ring on mbarriers, up to kTmaD planes ahead
+// of the stencil, which then reads only shared memory.  At each plane the
+// CTA first computes phi^{n+1} on the tile extended by one cell in x and y
+// (34 x 10 = 340 points, one per thread and a second for threads 0..83) into
+// a 4-plane shared ring, then phi^{n+2} one plane below on its own 32 x 8
+// points.  Per cell the arithmetic is exactly wave_f32_kernel's, so two
 // launches of that kernel and one of this give identical bits.  It reads
-// phi^n, phi^{n-1} and the mass once and writes phi^{n+1} (inner tile) and
+// phi^n, phi^{n-1} and the mass once and writes phi^{n+1} (own tile) and
 // phi^{n+2}: 20 bytes per cell for two iterations instead of 32.  out1 and
 // out2 must be buffers this launch does not read (neighbouring CTAs still
-// read phi^{n-1} and phi^n).  Loads for the next plane are issued before the
-// barrier so they overlap the second step.
+// read phi^{n-1} and phi^n).  Plane q of a CTA is z0-2+q; step 1 at plane
+// zs = z0-1+j reads planes j, j+1, j+2 and step 2 at zs-1 reads plane j, so
+// after iteration j's barrier plane j-1 is free and its stage takes plane
+// j-1+kTmaD.  Needs nx % 4 == 0 (16-byte row strides) and nx >= 40.
 constexpr int kT2X = 32, kT2Y = 8;
 constexpr int kT2EX = kT2X + 2, kT2EY = kT2Y + 2;
-constexpr int kT2Ring = 2 * kT2EX + 2 * kT2Y;  // 84 border points of the extended plane
-
-// Inputs of one first-step point at one plane (gathered one plane ahead).
-struct Wave1In {
-    float xm, xp, ym, yp, zp2, po, ms;
-};
-
-__device__ __forceinline__ Wave1In wave1_load(const float* __restrict__ p0, const float* __restrict__ pm,
-                                              const float* __restrict__ mass, int gx, int gy, int z, int NX) {
-    // Coordinates clamped into the mesh: every load is in bounds; values of
-    // points outside the mesh are never used (faces are zero).
-    const int cx = min(max(gx, 0), NX - 1), cy = min(max(gy, 0), NX - 1);
-    const int cz = min(max(z, 0), NX - 1), cz2 = min(max(z + 1, 0), NX - 1);
-    const int64_t sy = NX, sz = static_cast<int64_t>(NX) * NX;
-    const int64_t at = cz * sz + cy * sy + cx;
-    Wave1In r;
-    r.xm = p0[at - (cx > 0 ? 1 : 0)];
-    r.xp = p0[at + (cx < NX - 1 ? 1 : 0)];
-    r.ym = p0[at - (cy > 0 ? sy : 0)];
-    r.yp = p0[at + (cy < NX - 1 ? sy : 0)];
-    r.zp2 = p0[cz2 * sz + cy * sy + cx];  // phi^n one plane above z (the march's next value)
-    r.po = pm[at];
-    r.ms = mass[at];
-    return r;
-}
+constexpr int kT2E = kT2EX * kT2EY;           // 340 first-step points per plane
+constexpr int kT2Threads = kT2X * kT2Y;       // 256
+constexpr int kTmaD = 6;
+constexpr int kTmaBX = 40, kTmaBY = 12;
+constexpr unsigned kTmaBoxBytes = kTmaBX * kTmaBY * 4u;
 
 // One stencil update (wave_f32_kernel's expression) or 0 on faces and
 // outside the mesh.
@@ -462,141 +447,51 @@ __device__ __forceinline__ float wave1_point(const WaveF32& W, float sxy, bool e
     const float nb = ((xm + xp) + (ym + yp)) + (zm + zp);
     const float diss = sxy + W.sz[z];
     const float Q = diss * W.cdt_half;
-    const float w = 1.0f / (1.0f + Q);
+    const float w = __frcp_rn(1.0f + Q);  // correctly rounded: the bits of 1.0f / (1.0f + Q)
     return fmaf(nb, W.K * w, fmaf(c, W.A * w, fmaf(po, (Q - 1.0f) * w, ms * (W.S * w))));
 }
 
-template <int TZ>
-__global__ void __launch_bounds__(kT2X * kT2Y) wave2_f32_kernel(float* __restrict__ out1, float* __restrict__ out2,
-                                                               const float* __restrict__ p0,
-                                                               const float* __restrict__ pm,
-                                                               const float* __restrict__ mass, const WaveF32 W,
-                                                               double* __restrict__ resid) {
-    __shared__ float s1[3][kT2EY][kT2EX];
+// A first-step point of the extended tile: its box offset, sponge and edge flag.
+struct Wave2Pt {
+    int box;  // offset in a 40 x 12 box
+    int e;    // index in the 34 x 10 extended plane
+    float sxy;
+    bool edge;
+};
+
+__device__ __forceinline__ Wave2Pt wave2_point(const WaveF32& W, int e, int x0, int y0) {
     const int NX = W.nx;
-    const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * kT2X + tx;
-    const int x0 = blockIdx.x * kT2X, y0 = blockIdx.y * kT2Y, z0 = blockIdx.z * TZ;
-    const int64_t sz = static_cast<int64_t>(NX) * NX;
-
-    // Own point (inner tile) and, for every third thread, one ring point.
-    const int ox = x0 + tx, oy = y0 + ty;
-    const bool own_in = ox < NX && oy < NX;
-    const bool has_ring = (tid % 3 == 0) && (tid / 3 < kT2Ring);
-    int rex = 0, rey = 0;
-    if (has_ring) {
-        const int r = tid / 3;
-        if (r < kT2EX) rex = r, rey = 0;
-        else if (r < 2 * kT2EX) rex = r - kT2EX, rey = kT2EY - 1;
-        else if (r < 2 * kT2EX + kT2Y) rex = 0, rey = r - 2 * kT2EX + 1;
-        else rex = kT2EX - 1, rey = r - 2 * kT2EX - kT2Y + 1;
-    }
-    const int rx = x0 - 1 + rex, ry = y0 - 1 + rey;
-    auto edge = [&](int gx, int gy) { return gx <= 0 || gx >= NX - 1 || gy <= 0 || gy >= NX - 1; };
-    auto sxy_of = [&](int gx, int gy) {
-        const int cx = min(max(gx, 0), NX - 1), cy = min(max(gy, 0), NX - 1);
-        return (W.diss_base + W.sx[cx]) + W.sy[cy];
-    };
-    const bool own_edge = edge(ox, oy), ring_edge = edge(rx, ry);
-    const float own_sxy = sxy_of(ox, oy), ring_sxy = sxy_of(rx, ry);
-
-    // phi^n march registers (planes zs - 1, zs, zs + 1) of both points.
-    auto colv = [&](int gx, int gy, int z) {
-        const int cx = min(max(gx, 0), NX - 1), cy = min(max(gy, 0), NX - 1), cz = min(max(z, 0), NX - 1);
-        return p0[cz * sz + static_cast<int64_t>(cy) * NX + cx];
-    };
-    int zs = z0 - 1;  // first first-step plane
-    float oa0 = colv(ox, oy, zs - 1), oa1 = colv(ox, oy, zs);
-    float ra0 = has_ring ? colv(rx, ry, zs - 1) : 0.0f, ra1 = has_ring ? colv(rx, ry, zs) : 0.0f;
-    Wave1In oin = wave1_load(p0, pm, mass, ox, oy, zs, NX);
-    Wave1In rin = has_ring ? wave1_load(p0, pm, mass, rx, ry, zs, NX) : Wave1In{};
-
-    float o1m = 0.0f, o1c = 0.0f;   // own phi^{n+1} at planes zs - 2, zs - 1
-    float om_prev = 0.0f;           // own mass at plane zs - 1
-    float oa_prev = 0.0f;           // own phi^n at plane zs - 1 (before the shift below)
-    double d2 = 0.0, n2 = 0.0;
-    const int zend = min(z0 + TZ, NX);  // last output plane + 1
-    for (int j = 0; zs <= zend; ++j, ++zs) {
-        // First step at plane zs.
-        const float oa2 = oin.zp2, ra2 = rin.zp2;
-        const float o1 = wave1_point(W, own_sxy, own_edge, zs, oin.xm, oin.xp, oin.ym, oin.yp, oa0, oa1, oa2, oin.po,
-                                     oin.ms);
-        s1[j % 3][ty + 1][tx + 1] = o1;
-        if (has_ring)
-            s1[j % 3][rey][rex] = wave1_point(W, ring_sxy, ring_edge, zs, rin.xm, rin.xp, rin.ym, rin.yp, ra0, ra1, ra2,
-                                              rin.po, rin.ms);
-        const float om_cur = oin.ms;
-        oa_prev = oa0;
-        oa0 = oa1, oa1 = oa2;
-        ra0 = ra1, ra1 = ra2;
-        // The next plane's inputs, in flight across the barrier and the second step.
-        if (zs + 1 <= zend) {
-            oin = wave1_load(p0, pm, mass, ox, oy, zs + 1, NX);
-            if (has_ring) rin = wave1_load(p0, pm, mass, rx, ry, zs + 1, NX);
-        }
-        __syncthreads();
-        // Second step at plane k = zs - 1 (needs first-step planes zs - 2 .. zs).
-        const int k = zs - 1;
-        if (j >= 2 && own_in && k < zend) {
-            const float(&pl)[kT2EY][kT2EX] = s1[(j + 2) % 3];  // plane k
-            float o2 = 0.0f;
-            if (!(own_edge || k <= 0 || k >= NX - 1)) {
-                const float nb = ((pl[ty + 1][tx] + pl[ty + 1][tx + 2]) + (pl[ty][tx + 1] + pl[ty + 2][tx + 1])) +
-                                 (o1m + o1);
-                const float diss = own_sxy + W.sz[k];
-                const float Q = diss * W.cdt_half;
-                const float w = 1.0f / (1.0f + Q);
-                o2 = fmaf(nb, W.K * w, fmaf(o1c, W.A * w, fmaf(oa_prev, (Q - 1.0f) * w, om_prev * (W.S * w))));
-            }
-            const int64_t at = k * sz + static_cast<int64_t>(oy) * NX + ox;
-            out1[at] = o1c;
-            out2[at] = o2;
-            if (resid) {
-                const double dd = static_cast<double>(o2) - static_cast<double>(o1c);
-                d2 += dd * dd;
-                n2 += static_cast<double>(o2) * static_cast<double>(o2);
-            }
-        }
-        o1m = o1c;
-        o1c = o1;
-        om_prev = om_cur;
-    }
-    if (resid) {
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-            d2 += __shfl_xor_sync(0xffffffffu, d2, o);
-            n2 += __shfl_xor_sync(0xffffffffu, n2, o);
-        }
-        if (tx == 0) {
-            atomicAdd(&resid[0], d2);
-            atomicAdd(&resid[1], n2);
-        }
-    }
+    const int ex = e % kT2EX, ey = e / kT2EX;
+    const int gx = x0 - 1 + ex, gy = y0 - 1 + ey;
+    const int cx = min(max(gx, 0), NX - 1), cy = min(max(gy, 0), NX - 1);
+    Wave2Pt p;
+    p.box = (ey + 1) * kTmaBX + (ex + 3);  // extended point (ex, ey) sits at box (ex + 3, ey + 1)
+    p.e = e;
+    p.sxy = (W.diss_base + W.sx[cx]) + W.sy[cy];
+    p.edge = gx <= 0 || gx >= NX - 1 || gy <= 0 || gy >= NX - 1;
+    return p;
 }
 
-// The same two steps fed by tensor copies.  Thread 0 streams, plane by
-// plane, three 40 x 12 boxes (phi^n, phi^{n-1}, mass at x0-4 .. x0+35,
-// y0-2 .. y0+9; outside the mesh they read as zero) into a kTmaD-stage
-// shared-memory ring on mbarriers, up to kTmaD planes ahead of the stencil;
-// the stencil then reads only shared memory.  Plane q of a CTA is z0-2+q;
-// step 1 at plane zs = z0-1+j reads planes j, j+1, j+2 and step 2 at zs-1
-// reads plane j, so after iteration j's barrier plane j-1 is free and its
-// stage takes plane j-1+kTmaD.  Needs nx % 4 == 0 (16-byte row strides).
-constexpr int kTmaD = 7;
-constexpr int kTmaBX = 40, kTmaBY = 12;
-constexpr unsigned kTmaBoxBytes = kTmaBX * kTmaBY * 4u;
+__device__ __forceinline__ float wave2_step1(const WaveF32& W, const Wave2Pt& p, int zs, const float* __restrict__ a,
+                                             const float* __restrict__ b, const float* __restrict__ c,
+                                             const float* __restrict__ pm, const float* __restrict__ ms) {
+    const int o = p.box;
+    return wave1_point(W, p.sxy, p.edge, zs, b[o - 1], b[o + 1], b[o - kTmaBX], b[o + kTmaBX], a[o], b[o], c[o],
+                       pm[o], ms[o]);
+}
 
 template <int TZ>
-__global__ void __launch_bounds__(kT2X * kT2Y) wave2_tma_kernel(float* __restrict__ out1, float* __restrict__ out2,
-                                                               const __grid_constant__ CUtensorMap tp0,
-                                                               const __grid_constant__ CUtensorMap tpm,
-                                                               const __grid_constant__ CUtensorMap tms,
-                                                               const WaveF32 W, double* __restrict__ resid,
-                                                               unsigned* __restrict__ err) {
-    __shared__ alignas(128) float ring[kTmaD][3][kTmaBY][kTmaBX];
-    __shared__ float s1[3][kT2EY][kT2EX];
+__global__ void __launch_bounds__(kT2Threads) wave2_tma_kernel(float* __restrict__ out1, float* __restrict__ out2,
+                                                              const __grid_constant__ CUtensorMap tp0,
+                                                              const __grid_constant__ CUtensorMap tpm,
+                                                              const __grid_constant__ CUtensorMap tms,
+                                                              const WaveF32 W, double* __restrict__ resid,
+                                                              unsigned* __restrict__ err) {
+    __shared__ alignas(128) float ring[kTmaD][3][kTmaBY * kTmaBX];
+    __shared__ float s1[4][kT2E];
     __shared__ alignas(8) uint64_t full[kTmaD];
     const int NX = W.nx;
-    const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * kT2X + tx;
+    const int tid = threadIdx.x;
     const int x0 = blockIdx.x * kT2X, y0 = blockIdx.y * kT2Y, z0 = blockIdx.z * TZ;
     const int zend = min(z0 + TZ, NX);
     const int P = zend - z0 + 4;  // planes z0-2 .. zend+1
@@ -609,56 +504,44 @@ __global__ void __launch_bounds__(kT2X * kT2Y) wave2_tma_kernel(float* __restric
     auto issue = [&](int q) {
         const int s = q % kTmaD, z = z0 - 2 + q;
         mbar_arrive_expect_tx(&full[s], 3 * kTmaBoxBytes);
-        tensor_copy_3d_g2s(&ring[s][0][0][0], &tp0, x0 - 4, y0 - 2, z, &full[s]);
-        tensor_copy_3d_g2s(&ring[s][1][0][0], &tpm, x0 - 4, y0 - 2, z, &full[s]);
-        tensor_copy_3d_g2s(&ring[s][2][0][0], &tms, x0 - 4, y0 - 2, z, &full[s]);
+        tensor_copy_3d_g2s(ring[s][0], &tp0, x0 - 4, y0 - 2, z, &full[s]);
+        tensor_copy_3d_g2s(ring[s][1], &tpm, x0 - 4, y0 - 2, z, &full[s]);
+        tensor_copy_3d_g2s(ring[s][2], &tms, x0 - 4, y0 - 2, z, &full[s]);
     };
     if (tid == 0)
         for (int q = 0; q < kTmaD && q < P; ++q) issue(q);
 
+    // First-step points of this thread (the second one for tid < 84).
+    const Wave2Pt p1 = wave2_point(W, tid, x0, y0);
+    const bool has2 = tid + kT2Threads < kT2E;
+    const Wave2Pt p2 = wave2_point(W, has2 ? tid + kT2Threads : tid, x0, y0);
+    // Own second-step point.
+    const int tx = tid % kT2X, ty = tid / kT2X;
     const int ox = x0 + tx, oy = y0 + ty;
     const bool own_in = ox < NX && oy < NX;
-    const bool has_ring = (tid % 3 == 0) && (tid / 3 < kT2Ring);
-    int rex = 0, rey = 0;
-    if (has_ring) {
-        const int r = tid / 3;
-        if (r < kT2EX) rex = r, rey = 0;
-        else if (r < 2 * kT2EX) rex = r - kT2EX, rey = kT2EY - 1;
-        else if (r < 2 * kT2EX + kT2Y) rex = 0, rey = r - 2 * kT2EX + 1;
-        else rex = kT2EX - 1, rey = r - 2 * kT2EX - kT2Y + 1;
-    }
-    const int rx = x0 - 1 + rex, ry = y0 - 1 + rey;
-    auto edge = [&](int gx, int gy) { return gx <= 0 || gx >= NX - 1 || gy <= 0 || gy >= NX - 1; };
-    auto sxy_of = [&](int gx, int gy) {
-        const int cx = min(max(gx, 0), NX - 1), cy = min(max(gy, 0), NX - 1);
-        return (W.diss_base + W.sx[cx]) + W.sy[cy];
-    };
-    const bool own_edge = edge(ox, oy), ring_edge = edge(rx, ry);
-    const float own_sxy = sxy_of(ox, oy), ring_sxy = sxy_of(rx, ry);
-    // Box coordinates: extended-tile point (ex, ey) sits at (ex + 3, ey + 1).
-    const int oxi = tx + 4, oyi = ty + 2, rxi = rex + 3, ryi = rey + 1;
+    const bool own_edge = ox <= 0 || ox >= NX - 1 || oy <= 0 || oy >= NX - 1;
+    const float own_sxy =
+        (W.diss_base + W.sx[min(max(ox, 0), NX - 1)]) + W.sy[min(max(oy, 0), NX - 1)];
+    const int oe = (ty + 1) * kT2EX + (tx + 1);  // own point in the extended plane
+    const int ob = (ty + 2) * kTmaBX + (tx + 4);  // and in a box
+    const int64_t col = static_cast<int64_t>(oy) * NX + ox;
+    const int64_t plane = static_cast<int64_t>(NX) * NX;
 
     bool ok = mbar_wait_bounded(&full[0], 0u) && mbar_wait_bounded(&full[1 % kTmaD], 0u);
-    float o1m = 0.0f, o1c = 0.0f;
     double d2 = 0.0, n2 = 0.0;
     for (int j = 0; j + 2 < P; ++j) {
         const int zs = z0 - 1 + j;
         const int q2 = j + 2;
         if (ok) ok = mbar_wait_bounded(&full[q2 % kTmaD], static_cast<unsigned>((q2 / kTmaD) & 1));
-        float o1 = 0.0f;
         if (ok) {
-            const float(*a)[kTmaBX] = ring[j % kTmaD][0];        // phi^n at zs - 1
-            const float(*b)[kTmaBX] = ring[(j + 1) % kTmaD][0];  // phi^n at zs
-            const float(*c)[kTmaBX] = ring[q2 % kTmaD][0];       // phi^n at zs + 1
-            const float(*pm)[kTmaBX] = ring[(j + 1) % kTmaD][1];
-            const float(*ms)[kTmaBX] = ring[(j + 1) % kTmaD][2];
-            o1 = wave1_point(W, own_sxy, own_edge, zs, b[oyi][oxi - 1], b[oyi][oxi + 1], b[oyi - 1][oxi],
-                             b[oyi + 1][oxi], a[oyi][oxi], b[oyi][oxi], c[oyi][oxi], pm[oyi][oxi], ms[oyi][oxi]);
-            s1[j % 3][ty + 1][tx + 1] = o1;
-            if (has_ring)
-                s1[j % 3][rey][rex] = wave1_point(W, ring_sxy, ring_edge, zs, b[ryi][rxi - 1], b[ryi][rxi + 1],
-                                                  b[ryi - 1][rxi], b[ryi + 1][rxi], a[ryi][rxi], b[ryi][rxi],
-                                                  c[ryi][rxi], pm[ryi][rxi], ms[ryi][rxi]);
+            const float* a = ring[j % kTmaD][0];        // phi^n at zs - 1
+            const float* b = ring[(j + 1) % kTmaD][0];  // phi^n at zs
+            const float* c = ring[q2 % kTmaD][0];       // phi^n at zs + 1
+            const float* pm = ring[(j + 1) % kTmaD][1];
+            const float* ms = ring[(j + 1) % kTmaD][2];
+            float* dst = s1[j % 4];
+            dst[p1.e] = wave2_step1(W, p1, zs, a, b, c, pm, ms);
+            if (has2) dst[p2.e] = wave2_step1(W, p2, zs, a, b, c, pm, ms);
         }
         if (__syncthreads_or(!ok)) {
             if (tid == 0) {
@@ -676,30 +559,31 @@ __global__ void __launch_bounds__(kT2X * kT2Y) wave2_tma_kernel(float* __restric
             fence_proxy_async();
             issue(j - 1 + kTmaD);
         }
+        // Second step at plane k = zs - 1 from first-step planes k-1, k, k+1.
         const int k = zs - 1;
         if (j >= 2 && own_in) {
-            const float(*pl)[kT2EX] = s1[(j + 2) % 3];  // phi^{n+1} at k
+            const float* lo = s1[(j + 2) % 4];  // plane k - 1
+            const float* pl = s1[(j + 3) % 4];  // plane k
+            const float* hi = s1[j % 4];        // plane k + 1
+            const float c1 = pl[oe];
             float o2 = 0.0f;
             if (!(own_edge || k <= 0 || k >= NX - 1)) {
-                const float old = ring[j % kTmaD][0][oyi][oxi], mk = ring[j % kTmaD][2][oyi][oxi];
-                const float nb = ((pl[ty + 1][tx] + pl[ty + 1][tx + 2]) + (pl[ty][tx + 1] + pl[ty + 2][tx + 1])) +
-                                 (o1m + o1);
+                const float old = ring[j % kTmaD][0][ob], mk = ring[j % kTmaD][2][ob];
+                const float nb = ((pl[oe - 1] + pl[oe + 1]) + (pl[oe - kT2EX] + pl[oe + kT2EX])) + (lo[oe] + hi[oe]);
                 const float diss = own_sxy + W.sz[k];
                 const float Q = diss * W.cdt_half;
-                const float w = 1.0f / (1.0f + Q);
-                o2 = fmaf(nb, W.K * w, fmaf(o1c, W.A * w, fmaf(old, (Q - 1.0f) * w, mk * (W.S * w))));
+                const float w = __frcp_rn(1.0f + Q);
+                o2 = fmaf(nb, W.K * w, fmaf(c1, W.A * w, fmaf(old, (Q - 1.0f) * w, mk * (W.S * w))));
             }
-            const int64_t at = k * static_cast<int64_t>(NX) * NX + static_cast<int64_t>(oy) * NX + ox;
-            out1[at] = o1c;
+            const int64_t at = k * plane + col;
+            out1[at] = c1;
             out2[at] = o2;
             if (resid) {
-                const double dd = static_cast<double>(o2) - static_cast<double>(o1c);
+                const double dd = static_cast<double>(o2) - static_cast<double>(c1);
                 d2 += dd * dd;
                 n2 += static_cast<double>(o2) * static_cast<double>(o2);
             }
         }
-        o1m = o1c;
-        o1c = o1;
     }
     if (resid) {
 #pragma unroll
@@ -707,7 +591,7 @@ __global__ void __launch_bounds__(kT2X * kT2Y) wave2_tma_kernel(float* __restric
             d2 += __shfl_xor_sync(0xffffffffu, d2, o);
             n2 += __shfl_xor_sync(0xffffffffu, n2, o);
         }
-        if (tx == 0) {
+        if ((tid & 31) == 0) {
             atomicAdd(&resid[0], d2);
             atomicAdd(&resid[1], n2);
         }
@@ -983,10 +867,15 @@ cudaError_t enqueue_wave_f32(float* ring, int64_t cells, const float* mass, cons
         int f0, f1;
         ring_free(st, f0, f1);
         double* r = i + 2 == k ? resid : nullptr;
-        cudaError_t e = tma ? launch_wave2_tma(ring + f0 * cz, ring + f1 * cz, maps->ring[st % 4], maps->ring[st / 4],
-                                               maps->mass, w, r, err, s)
-                            : launch_wave2_f32(ring + f0 * cz, ring + f1 * cz, ring + (st % 4) * cz,
-                                               ring + (st / 4) * cz, mass, w, r, s);
+        cudaError_t e;
+        if (tma) {
+            e = launch_wave2_tma(ring + f0 * cz, ring + f1 * cz, maps->ring[st % 4], maps->ring[st / 4], maps->mass, w,
+                                 r, err, s);
+        } else {  // two single steps
+            e = launch_wave_f32(ring + f0 * cz, ring + (st % 4) * cz, ring + (st / 4) * cz, mass, w, nullptr, s);
+            if (e == cudaSuccess)
+                e = launch_wave_f32(ring + f1 * cz, ring + f0 * cz, ring + (st % 4) * cz, mass, w, r, s);
+        }
         if (e != cudaSuccess) return e;
         st = ring_step2(st);
     }
@@ -1001,26 +890,13 @@ cudaError_t enqueue_wave_f32(float* ring, int64_t cells, const float* mass, cons
 
 cudaError_t launch_wave2_tma(float* out1, float* out2, const CUtensorMap& phi, const CUtensorMap& phi_old,
                              const CUtensorMap& mass, const WaveF32& w, double* resid, unsigned* err, cudaStream_t s) {
-    const dim3 block(kT2X, kT2Y);
+    const dim3 block(kT2Threads);
     if (w.nx >= 192) {
         const dim3 grid((w.nx + kT2X - 1) / kT2X, (w.nx + kT2Y - 1) / kT2Y, (w.nx + 31) / 32);
         wave2_tma_kernel<32><<<grid, block, 0, s>>>(out1, out2, phi, phi_old, mass, w, resid, err);
     } else {
         const dim3 grid((w.nx + kT2X - 1) / kT2X, (w.nx + kT2Y - 1) / kT2Y, (w.nx + 15) / 16);
         wave2_tma_kernel<16><<<grid, block, 0, s>>>(out1, out2, phi, phi_old, mass, w, resid, err);
-    }
-    return cudaGetLastError();
-}
-
-cudaError_t launch_wave2_f32(float* out1, float* out2, const float* phi, const float* phi_old, const float* mass,
-                             const WaveF32& w, double* resid, cudaStream_t s) {
-    const dim3 block(kT2X, kT2Y);
-    if (w.nx >= 192) {
-        const dim3 grid((w.nx + kT2X - 1) / kT2X, (w.nx + kT2Y - 1) / kT2Y, (w.nx + 31) / 32);
-        wave2_f32_kernel<32><<<grid, block, 0, s>>>(out1, out2, phi, phi_old, mass, w, resid);
-    } else {
-        const dim3 grid((w.nx + kT2X - 1) / kT2X, (w.nx + kT2Y - 1) / kT2Y, (w.nx + 15) / 16);
-        wave2_f32_kernel<16><<<grid, block, 0, s>>>(out1, out2, phi, phi_old, mass, w, resid);
     }
     return cudaGetLastError();
 }
