@@ -210,10 +210,17 @@ inline int ring_after_f64(int st, int k) {
 // they do not exist (nx % 4 != 0, or no driver entry point), and the stencil
 // then loads through the cache instead.
 struct WaveMaps {
-    CUtensorMap ring[4];
+    CUtensorMap ring[4];             // 40 x 12 boxes (two-step kernel)
     CUtensorMap mass;
+    CUtensorMap halo[4];             // 40 x 10 boxes: phi with its x/y halo (one-step kernel)
+    CUtensorMap tile[4], tile_mass;  // 32 x 8 boxes: phi^{n-1} and mass (one-step kernel)
     bool ok = false;
+    bool two_step = false;           // pairs of iterations through the two-step kernel
 };
+// One FP32 iteration fed by tensor copies (wave1_tma_kernel), bit-identical
+// to launch_wave_f32.
+cudaError_t launch_wave1_tma(float* phi_new, const CUtensorMap& phi, const CUtensorMap& phi_old,
+                             const CUtensorMap& mass, const WaveF32& w, double* resid, unsigned* err, cudaStream_t s);
 // Two FP32 iterations in one launch fed by tensor copies (wave2_tma_kernel):
 // out1 = phi^{n+1}, out2 = phi^{n+2}, bit-identical to two launch_wave_f32
 // calls; resid (may be NULL) sums (phi^{n+2} - phi^{n+1})^2 and (phi^{n+2})^2.

@@ -598,6 +598,122 @@ __global__ void __launch_bounds__(kT2Threads) wave2_tma_kernel(float* __restrict
     }
 }
 
+// One leap-frog step fed by tensor copies, warp-specialised.  A CTA owns a
+// 32 x 8 column tile and TZ planes of it.  Warp 8 (one lane) is the
+// producer: plane by plane it copies phi^n with its x/y halo (a 40 x 10 box
+// at x0-4, y0-1), phi^{n-1} and the mass (32 x 8 boxes at x0, y0) into a
+// kW1D-stage ring, waiting on each stage's "empty" barrier before reuse.
+// Warps 0..7 are consumers, one output point per thread: output plane z
+// reads phi^n at z-1, z, z+1 (stages i, i+1, i+2 for z = z0+i) and
+// phi^{n-1}, mass at z (stage i+1), then releases stage i.  No CTA-wide
+// barrier after set-up: warps drift up to kW1D planes apart and each waits
+// only for its data.  Per cell the arithmetic is wave_f32_kernel's (same
+// bits).  Needs nx % 4 == 0 and nx >= 40.
+constexpr int kW1D = 8;
+constexpr int kW1Consumers = 8;                 // warps
+constexpr int kW1PhiFloats = 40 * 10;           // phi box
+constexpr int kW1PhiPad = 416;                  // 1664 bytes: keeps the next box 128-byte aligned
+constexpr int kW1TileFloats = 32 * 8;           // phi^{n-1} and mass boxes
+constexpr int kW1StageFloats = kW1PhiPad + 2 * kW1TileFloats;
+constexpr unsigned kW1StageBytes = (kW1PhiFloats + 2 * kW1TileFloats) * 4u;
+
+template <int TZ>
+__global__ void __launch_bounds__((kW1Consumers + 1) * 32) wave1_tma_kernel(float* __restrict__ phi_new,
+                                                                           const __grid_constant__ CUtensorMap tphi,
+                                                                           const __grid_constant__ CUtensorMap told,
+                                                                           const __grid_constant__ CUtensorMap tmass,
+                                                                           const WaveF32 W, double* __restrict__ resid,
+                                                                           unsigned* __restrict__ err) {
+    __shared__ alignas(128) float ring[kW1D][kW1StageFloats];
+    __shared__ alignas(8) uint64_t full[kW1D], empty[kW1D];
+    const int NX = W.nx;
+    const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
+    const int x0 = blockIdx.x * 32, y0 = blockIdx.y * 8, z0 = blockIdx.z * TZ;
+    const int zend = min(z0 + TZ, NX);
+    const int P = zend - z0 + 2;  // planes z0-1 .. zend: plane q is z0-1+q
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < kW1D; ++s) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], kW1Consumers);
+        }
+        fence_mbar_init();
+    }
+    __syncthreads();
+
+    if (warp == kW1Consumers) {  // producer
+        if (lane != 0) return;
+        bool ok = true;
+        int issued = 0;
+        for (int q = 0; q < P; ++q) {
+            const int s = q % kW1D;
+            if (q >= kW1D) {
+                ok = mbar_wait_bounded(&empty[s], static_cast<unsigned>((q / kW1D - 1) & 1));
+                if (!ok) break;
+                fence_proxy_async();
+            }
+            const int z = z0 - 1 + q;
+            float* st = ring[s];
+            mbar_arrive_expect_tx(&full[s], kW1StageBytes);
+            tensor_copy_3d_g2s(st, &tphi, x0 - 4, y0 - 1, z, &full[s]);
+            tensor_copy_3d_g2s(st + kW1PhiPad, &told, x0, y0, z, &full[s]);
+            tensor_copy_3d_g2s(st + kW1PhiPad + kW1TileFloats, &tmass, x0, y0, z, &full[s]);
+            issued = q + 1;
+        }
+        if (!ok) atomicOr(err, kErrTimeout);
+        // No copy may still be in flight when the CTA exits.
+        for (int q = max(0, issued - kW1D); q < issued; ++q)
+            (void)mbar_wait_bounded(&full[q % kW1D], static_cast<unsigned>((q / kW1D) & 1));
+        return;
+    }
+
+    // Consumers: thread (lane, warp) owns point (x0 + lane, y0 + warp).
+    const int ox = x0 + lane, oy = y0 + warp;
+    const bool own_in = ox < NX && oy < NX;
+    const bool edge_xy = ox <= 0 || ox >= NX - 1 || oy <= 0 || oy >= NX - 1;
+    const float sxy = (W.diss_base + W.sx[min(max(ox, 0), NX - 1)]) + W.sy[min(max(oy, 0), NX - 1)];
+    const int pb = (warp + 1) * 40 + (lane + 4);  // point in the phi box
+    const int tb = warp * 32 + lane;              // point in the 32 x 8 boxes
+    const int64_t plane = static_cast<int64_t>(NX) * NX;
+    const int64_t col = static_cast<int64_t>(oy) * NX + ox;
+    double d2 = 0.0, n2 = 0.0;
+    bool ok = mbar_wait_bounded(&full[0], 0u) && mbar_wait_bounded(&full[1], 0u);
+    for (int i = 0; ok && i + 2 < P; ++i) {
+        const int q2 = i + 2;
+        ok = mbar_wait_bounded(&full[q2 % kW1D], static_cast<unsigned>((q2 / kW1D) & 1));
+        if (!ok) break;
+        const int z = z0 + i;
+        const float* a = ring[i % kW1D];
+        const float* b = ring[(i + 1) % kW1D];
+        const float* c = ring[q2 % kW1D];
+        const float cc = b[pb];
+        const float out = wave1_point(W, sxy, edge_xy, z, b[pb - 1], b[pb + 1], b[pb - 40], b[pb + 40], a[pb], cc,
+                                      c[pb], b[kW1PhiPad + tb], b[kW1PhiPad + kW1TileFloats + tb]);
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&empty[i % kW1D]);  // this warp is done with plane i
+        if (own_in) {
+            phi_new[z * plane + col] = out;
+            if (resid) {
+                const double dd = static_cast<double>(out) - static_cast<double>(cc);
+                d2 += dd * dd;
+                n2 += static_cast<double>(out) * static_cast<double>(out);
+            }
+        }
+    }
+    if (!ok) atomicOr(err, kErrTimeout);
+    if (resid) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            d2 += __shfl_xor_sync(0xffffffffu, d2, o);
+            n2 += __shfl_xor_sync(0xffffffffu, n2, o);
+        }
+        if (lane == 0) {
+            atomicAdd(&resid[0], d2);
+            atomicAdd(&resid[1], n2);
+        }
+    }
+}
+
 // acc_field (p2mesh-kernel.cuh:169-225) with a 3-D launch over the mesh.
 __global__ void acc_field_kernel(double* __restrict__ cell_acc, double* __restrict__ cell_acc_abs,
                                  const double* __restrict__ phi, int NX, double DX) {
@@ -863,18 +979,23 @@ cudaError_t enqueue_wave_f32(float* ring, int64_t cells, const float* mass, cons
                              double* resid, cudaStream_t s, const WaveMaps* maps, unsigned* err) {
     const size_t cz = static_cast<size_t>(cells);
     const bool tma = maps && maps->ok && err;
+    // One iteration: buffer `out` from phi^n in `cur` and phi^{n-1} in `old`.
+    auto single = [&](int old, int cur, int out, double* r) {
+        if (tma)
+            return launch_wave1_tma(ring + out * cz, maps->halo[cur], maps->tile[old], maps->tile_mass, w, r, err, s);
+        return launch_wave_f32(ring + out * cz, ring + cur * cz, ring + old * cz, mass, w, r, s);
+    };
     for (int i = 0; i + 1 < k; i += 2) {
         int f0, f1;
         ring_free(st, f0, f1);
         double* r = i + 2 == k ? resid : nullptr;
         cudaError_t e;
-        if (tma) {
+        if (tma && maps->two_step) {
             e = launch_wave2_tma(ring + f0 * cz, ring + f1 * cz, maps->ring[st % 4], maps->ring[st / 4], maps->mass, w,
                                  r, err, s);
-        } else {  // two single steps
-            e = launch_wave_f32(ring + f0 * cz, ring + (st % 4) * cz, ring + (st / 4) * cz, mass, w, nullptr, s);
-            if (e == cudaSuccess)
-                e = launch_wave_f32(ring + f1 * cz, ring + f0 * cz, ring + (st % 4) * cz, mass, w, r, s);
+        } else {  // two single steps: phi^{n+1} into f0, phi^{n+2} into f1
+            e = single(st / 4, st % 4, f0, nullptr);
+            if (e == cudaSuccess) e = single(st % 4, f0, f1, r);
         }
         if (e != cudaSuccess) return e;
         st = ring_step2(st);
@@ -882,10 +1003,23 @@ cudaError_t enqueue_wave_f32(float* ring, int64_t cells, const float* mass, cons
     if (k % 2) {
         int f0, f1;
         ring_free(st, f0, f1);
-        cudaError_t e = launch_wave_f32(ring + f0 * cz, ring + (st % 4) * cz, ring + (st / 4) * cz, mass, w, resid, s);
+        cudaError_t e = single(st / 4, st % 4, f0, resid);
         if (e != cudaSuccess) return e;
     }
     return cudaSuccess;
+}
+
+cudaError_t launch_wave1_tma(float* phi_new, const CUtensorMap& phi, const CUtensorMap& phi_old,
+                             const CUtensorMap& mass, const WaveF32& w, double* resid, unsigned* err, cudaStream_t s) {
+    const dim3 block((kW1Consumers + 1) * 32);
+    if (w.nx >= 192) {
+        const dim3 grid((w.nx + 31) / 32, (w.nx + 7) / 8, (w.nx + 31) / 32);
+        wave1_tma_kernel<32><<<grid, block, 0, s>>>(phi_new, phi, phi_old, mass, w, resid, err);
+    } else {
+        const dim3 grid((w.nx + 31) / 32, (w.nx + 7) / 8, (w.nx + 15) / 16);
+        wave1_tma_kernel<16><<<grid, block, 0, s>>>(phi_new, phi, phi_old, mass, w, resid, err);
+    }
+    return cudaGetLastError();
 }
 
 cudaError_t launch_wave2_tma(float* out1, float* out2, const CUtensorMap& phi, const CUtensorMap& phi_old,

@@ -95,35 +95,41 @@ PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
     return fn;
 }
 
-// One nx^3 float field as a 3-D tensor with 40 x 12 x 1 boxes (the planes the
-// tensor-copy stencil streams); outside coordinates read as zero.
-bool make_box_map(CUtensorMap* m, const float* base, int nx) {
+// One nx^3 float field as a 3-D tensor with bx x by x 1 boxes (the planes the
+// tensor-copy stencils stream); outside coordinates read as zero.
+bool make_box_map(CUtensorMap* m, const float* base, int nx, unsigned bx, unsigned by) {
     const auto enc = tensor_map_encoder();
     if (!enc) return false;
     const cuuint64_t n = static_cast<cuuint64_t>(nx);
     const cuuint64_t dims[3] = {n, n, n};
     const cuuint64_t strides[2] = {n * 4, n * n * 4};
-    const cuuint32_t box[3] = {40, 12, 1};
+    const cuuint32_t box[3] = {bx, by, 1};
     const cuuint32_t elem[3] = {1, 1, 1};
     return enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<float*>(base), dims, strides, box, elem,
                CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
-// Maps of the four ring buffers and the mass.  The tensor-copy stencil needs
-// 16-byte row strides (nx % 4 == 0) and a mesh at least one box wide;
-// KHRR_WAVE_TMA=0 in the environment turns it off.
+// Maps of the four ring buffers and the mass for both tensor-copy stencils.
+// They need 16-byte row strides (nx % 4 == 0) and a mesh at least one box
+// wide.  KHRR_WAVE_TMA=0 in the environment turns them off (cache-fed
+// kernel); KHRR_WAVE_TMA=2 runs pairs of iterations through the two-step
+// kernel instead of the one-step one.
 void make_wave_maps(WaveMaps* w, float* ring, const float* mass, int nx) {
     w->ok = false;
-    static const bool enabled = [] {
+    static const int mode = [] {
         const char* e = std::getenv("KHRR_WAVE_TMA");
-        return !(e && e[0] == '0');
+        return e ? std::atoi(e) : 1;
     }();
-    if (!enabled || nx % 4 != 0 || nx < 40) return;
+    if (mode == 0 || nx % 4 != 0 || nx < 40) return;
     const size_t cz = static_cast<size_t>(nx) * nx * nx;
     for (int b = 0; b < 4; ++b)
-        if (!make_box_map(&w->ring[b], ring + b * cz, nx)) return;
-    if (!make_box_map(&w->mass, mass, nx)) return;
+        if (!make_box_map(&w->ring[b], ring + b * cz, nx, 40, 12) ||
+            !make_box_map(&w->halo[b], ring + b * cz, nx, 40, 10) ||
+            !make_box_map(&w->tile[b], ring + b * cz, nx, 32, 8))
+            return;
+    if (!make_box_map(&w->mass, mass, nx, 40, 12) || !make_box_map(&w->tile_mass, mass, nx, 32, 8)) return;
+    w->two_step = mode == 2;
     w->ok = true;
 }
 
