@@ -110,18 +110,18 @@ bool make_box_map(CUtensorMap* m, const float* base, int nx, unsigned bx, unsign
                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
-// Maps of the four ring buffers and the mass for both tensor-copy stencils.
-// They need 16-byte row strides (nx % 4 == 0) and a mesh at least one box
-// wide.  KHRR_WAVE_TMA=0 in the environment turns them off (cache-fed
-// kernel); KHRR_WAVE_TMA=2 runs pairs of iterations through the two-step
-// kernel instead of the one-step one.
+// Maps of the four ring buffers and the mass for the tensor-copy stencils,
+// made only when KHRR_WAVE_TMA selects one (read at every solve set-up):
+// 1 = the warp-specialised one-step kernel, 2 = the two-step kernel for
+// pairs of iterations; unset or 0 = the cache-fed one-step kernel, which
+// measured fastest on the 128^3 mesh (10.4 us per iteration against 16.4 and
+// 13.1) and within noise of both on 256^3.  The tensor-copy kernels need
+// 16-byte row strides (nx % 4 == 0) and a mesh at least one box wide.
 void make_wave_maps(WaveMaps* w, float* ring, const float* mass, int nx) {
     w->ok = false;
-    static const int mode = [] {
-        const char* e = std::getenv("KHRR_WAVE_TMA");
-        return e ? std::atoi(e) : 1;
-    }();
-    if (mode == 0 || nx % 4 != 0 || nx < 40) return;
+    const char* e = std::getenv("KHRR_WAVE_TMA");
+    const int mode = e ? std::atoi(e) : 0;
+    if ((mode != 1 && mode != 2) || nx % 4 != 0 || nx < 40) return;
     const size_t cz = static_cast<size_t>(nx) * nx * nx;
     for (int b = 0; b < 4; ++b)
         if (!make_box_map(&w->ring[b], ring + b * cz, nx, 40, 12) ||
