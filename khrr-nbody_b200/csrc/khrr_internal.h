@@ -178,12 +178,7 @@ cudaError_t launch_wave_f32(float* phi_new, const float* phi, const float* phi_o
 // single iteration writes the lower free buffer (state -> 4 * cur + f0), a
 // pair writes f0 and f1 (state -> 4 * f0 + f1).
 constexpr int kRingStart = 1;  // old = buffer 0, cur = buffer 1
-#ifdef __CUDACC__
-#define KHRR_HD __host__ __device__
-#else
-#define KHRR_HD
-#endif
-KHRR_HD inline void ring_free(int st, int& f0, int& f1) {
+inline void ring_free(int st, int& f0, int& f1) {
     const int o = st / 4, c = st % 4;
     int f[2], n = 0;
     for (int b = 0; b < 4; ++b)
@@ -191,12 +186,12 @@ KHRR_HD inline void ring_free(int st, int& f0, int& f1) {
     f0 = f[0];
     f1 = f[1];
 }
-KHRR_HD inline int ring_step1(int st) {
+inline int ring_step1(int st) {
     int f0, f1;
     ring_free(st, f0, f1);
     return 4 * (st % 4) + f0;
 }
-KHRR_HD inline int ring_step2(int st) {
+inline int ring_step2(int st) {
     int f0, f1;
     ring_free(st, f0, f1);
     return 4 * f0 + f1;
@@ -221,18 +216,7 @@ struct WaveMaps {
     CUtensorMap tile[4], tile_mass;  // 32 x 8 boxes: phi^{n-1} and mass (one-step kernel)
     bool ok = false;
     bool two_step = false;           // pairs of iterations through the two-step kernel
-    // Persistent stencil (all iterations of a call in one cooperative
-    // launch): co-resident grid, 0 when not used, and its barrier words.
-    int persist_grid = 0;
-    unsigned* bar = nullptr;
 };
-// Co-resident grid of the persistent stencil for an nx^3 mesh on the current
-// device, or 0 when it is not used there (working sets beyond kPersistMaxCells
-// cells, which are HBM-bound and gain nothing from fewer launches; devices
-// without cooperative launches; KHRR_WAVE_PERSIST=0).  Host only, outside
-// stream captures.
-constexpr int64_t kPersistMaxCells = 5000000;
-int wave_persist_grid(int nx);
 // One FP32 iteration fed by tensor copies (wave1_tma_kernel), bit-identical
 // to launch_wave_f32.
 cudaError_t launch_wave1_tma(float* phi_new, const CUtensorMap& phi, const CUtensorMap& phi_old,

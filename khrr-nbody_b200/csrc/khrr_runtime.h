@@ -78,8 +78,7 @@ struct MeshSolver {
     DevBuf<float> mass32, phi32, tab;           // C, 4 C (field ring), 3 nx
     DevBuf<int2> pci;                           // npad
     DevBuf<double4> part;                       // npad: {acc, -phi} per body
-    WaveMaps maps;                              // stencil launch set-up (tensor maps, persistent grid)
-    DevBuf<unsigned> bar;                       // grid-barrier words of the persistent stencil
+    WaveMaps maps;                              // tensor maps of phi32 / mass32
     DevBuf<unsigned char> ns;                   // npad: 1 for real bodies, 0 for ghosts
     std::vector<int64_t> layout_poff, layout_cnt;  // the layout pci/part/ns were sized for
     int rot = kRingStart;                       // ring state: 4 * (phi^{n-1} buffer) + phi^n buffer
@@ -139,8 +138,7 @@ struct khrr_ctx {
     khrr::DevBuf<float> wave_phi, wave_mass, wave_tab;   // 4 C (field ring), C, 3 nx
     int wave_nx = 0;
     int wave_rot = khrr::kRingStart;                     // ring state: 4 * (phi^{n-1} buffer) + phi^n buffer
-    khrr::WaveMaps wave_maps;                            // stencil launch set-up of wave_phi / wave_mass
-    khrr::DevBuf<unsigned> wave_bar;                     // grid-barrier words of the persistent stencil
+    khrr::WaveMaps wave_maps;                            // tensor maps of wave_phi / wave_mass
     bool wave_warm = false;
     std::map<std::pair<int, int>, khrr::StepGraph> wave_graphs;  // (chunk, rotation)
 

@@ -24,7 +24,6 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdint>
-#include <cstdlib>
 
 #include "async_copy.cuh"
 #include "khrr_internal.h"
@@ -345,86 +344,6 @@ __global__ void wave_f64_kernel(double* __restrict__ phi_new, const double* __re
 // large meshes, 4 on small ones (more CTAs).
 constexpr int kWX = 32, kWY = 8;
 
-// Field loads: through L1 by default; L2 only (ld.global.cg) where other CTAs
-// rewrite the buffers during the kernel (the persistent kernel below), so no
-// stale L1 line is ever read.
-template <bool CG>
-__device__ __forceinline__ float ld_field(const float* p) {
-    if constexpr (CG) return __ldcg(p);
-    else return *p;
-}
-
-// One 32 x 8 x kWZ tile of the FP32 step for the persistent kernel (tile
-// coordinates bx, by, bz; thread tx, ty), wave_f32_kernel's arithmetic;
-// residual terms are added into d2 and n2 when resid is set.
-template <int kWZ, bool CG>
-__device__ __forceinline__ void wave_tile(float* __restrict__ phi_new, const float* __restrict__ phi,
-                                          const float* __restrict__ phi_old, const float* __restrict__ mass,
-                                          const WaveF32& W, int bx, int by, int bz, int tx, int ty, bool resid,
-                                          double& d2, double& n2) {
-    const int NX = W.nx;
-    const int ix = bx * kWX + tx, iy = by * kWY + ty;
-    const int zb = bz * kWZ;
-    const int64_t sy = NX, sz = static_cast<int64_t>(NX) * NX;
-    if (ix >= NX || iy >= NX) return;
-    const int64_t col = static_cast<int64_t>(iy) * NX + ix;
-    // Neighbour offsets clamped into the mesh, so every load below is
-    // unconditional and in bounds (face cells discard their values).
-    const int64_t dxm = ix > 0 ? 1 : 0, dxp = ix < NX - 1 ? 1 : 0;
-    const int64_t dym = iy > 0 ? sy : 0, dyp = iy < NX - 1 ? sy : 0;
-    float c[kWZ + 2];  // phi at z = zb - 1 .. zb + kWZ (clamped into the mesh)
-    float xm[kWZ], xp[kWZ], ym[kWZ], yp[kWZ], po[kWZ], ms[kWZ];
-#pragma unroll
-    for (int u = 0; u < kWZ + 2; ++u) {
-        const int z = min(max(zb - 1 + u, 0), NX - 1);
-        c[u] = ld_field<CG>(phi + z * sz + col);
-    }
-#pragma unroll
-    for (int u = 0; u < kWZ; ++u) {
-        const int64_t at = min(zb + u, NX - 1) * sz + col;
-        xm[u] = ld_field<CG>(phi + at - dxm);
-        xp[u] = ld_field<CG>(phi + at + dxp);
-        ym[u] = ld_field<CG>(phi + at - dym);
-        yp[u] = ld_field<CG>(phi + at + dyp);
-        po[u] = ld_field<CG>(phi_old + at);
-        ms[u] = mass[at];
-    }
-    const bool edge_xy = ix == 0 || ix == NX - 1 || iy == 0 || iy == NX - 1;
-    const float sxy = (W.diss_base + W.sx[ix]) + W.sy[iy];
-#pragma unroll
-    for (int u = 0; u < kWZ; ++u) {
-        const int z = zb + u;
-        if (z >= NX) break;
-        const int64_t at = z * sz + col;
-        float out = 0.0f;
-        if (!(edge_xy || z == 0 || z == NX - 1)) {
-            const float nb = ((xm[u] + xp[u]) + (ym[u] + yp[u])) + (c[u] + c[u + 2]);
-            const float diss = sxy + W.sz[z];
-            const float Q = diss * W.cdt_half;
-            const float w = __frcp_rn(1.0f + Q);  // correctly rounded: the bits of 1.0f / (1.0f + Q)
-            out = fmaf(nb, W.K * w, fmaf(c[u + 1], W.A * w, fmaf(po[u], (Q - 1.0f) * w, ms[u] * (W.S * w))));
-        }
-        phi_new[at] = out;
-        if (resid) {
-            const double dd = static_cast<double>(out) - static_cast<double>(c[u + 1]);
-            d2 += dd * dd;
-            n2 += static_cast<double>(out) * static_cast<double>(out);
-        }
-    }
-}
-
-__device__ __forceinline__ void resid_reduce(double d2, double n2, double* resid) {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        d2 += __shfl_xor_sync(0xffffffffu, d2, o);
-        n2 += __shfl_xor_sync(0xffffffffu, n2, o);
-    }
-    if ((threadIdx.x & 31) == 0) {
-        atomicAdd(&resid[0], d2);
-        atomicAdd(&resid[1], n2);
-    }
-}
-
 template <int kWZ>
 __global__ void __launch_bounds__(kWX * kWY) wave_f32_kernel(float* __restrict__ phi_new, const float* __restrict__ phi,
                                                              const float* __restrict__ phi_old,
@@ -481,87 +400,17 @@ __global__ void __launch_bounds__(kWX * kWY) wave_f32_kernel(float* __restrict__
             }
         }
     }
-    if (resid) resid_reduce(d2, n2, resid);
-}
-
-// Grid-wide barrier of a cooperative launch: bar[0] counts arrivals, bar[1]
-// is the generation (both zero before the launch).  Each wait gives up after
-// ~2 s or as soon as another CTA has raised the error flag; it then returns
-// false and the caller ends the kernel.
-__device__ __forceinline__ bool grid_barrier(unsigned* bar, unsigned nblocks, unsigned* err) {
-    __shared__ int s_ok;
-    __syncthreads();
-    if (threadIdx.x == 0 && threadIdx.y == 0) {
-        volatile unsigned* vgen = bar + 1;
-        volatile unsigned* verr = err;
-        const unsigned g = *vgen;
-        int ok = 1;
-        __threadfence();  // this CTA's field writes before its arrival
-        if (atomicAdd(&bar[0], 1u) == nblocks - 1) {
-            atomicExch(&bar[0], 0u);
-            __threadfence();
-            atomicAdd(&bar[1], 1u);
-        } else {
-            const uint64_t t0 = global_ns();
-            while (*vgen == g) {
-                if (*verr) {
-                    ok = 0;
-                    break;
-                }
-                if (global_ns() - t0 > 2000000000ull) {
-                    atomicOr(err, kErrTimeout);
-                    ok = 0;
-                    break;
-                }
-                __nanosleep(64);
-            }
+    if (resid) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            d2 += __shfl_xor_sync(0xffffffffu, d2, o);
+            n2 += __shfl_xor_sync(0xffffffffu, n2, o);
         }
-        __threadfence();
-        s_ok = ok;
-    }
-    __syncthreads();
-    return s_ok != 0;
-}
-
-// `iters` FP32 steps in one cooperative launch (working sets that stay in
-// L2, where a launch per step costs more than the step).  The grid strides
-// over the 32 x 8 x 4 tiles; a grid barrier separates steps.  Buffers follow
-// enqueue_wave_f32's ring sequence: pairs write the two free buffers in
-// order (f0 then f1), an odd last step writes f0.  Per cell the arithmetic is
-// wave_f32_kernel's (same bits).
-constexpr int kPZ = 4;
-
-__global__ void __launch_bounds__(kWX * kWY, 3) wave_persist_kernel(float* __restrict__ ring, const float* __restrict__ mass,
-                                                                const WaveF32 W, int iters, int st0,
-                                                                double* __restrict__ resid, unsigned* __restrict__ bar,
-                                                                unsigned* __restrict__ err) {
-    const int NX = W.nx;
-    const int gx = (NX + kWX - 1) / kWX, gy = (NX + kWY - 1) / kWY, gz = (NX + kPZ - 1) / kPZ;
-    const int ntiles = gx * gy * gz;
-    const size_t cz = static_cast<size_t>(NX) * NX * NX;
-    double d2 = 0.0, n2 = 0.0;
-    int st = st0;
-    for (int it = 0; it < iters; ++it) {
-        // Steps go in pairs (it, it + 1) from the pair's starting state st:
-        // the first (or an odd last step) writes f0 from (old, cur), the
-        // second writes f1 from (cur, f0).
-        int f0, f1;
-        ring_free(st, f0, f1);
-        const bool second = it & 1;
-        const int o = second ? st % 4 : st / 4;
-        const int c = second ? f0 : st % 4;
-        const int out = second ? f1 : f0;
-        const bool last = it == iters - 1;
-        for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
-            const int bx = t % gx, by = (t / gx) % gy, bz = t / (gx * gy);
-            wave_tile<kPZ, true>(ring + out * cz, ring + c * cz, ring + o * cz, mass, W, bx, by, bz, threadIdx.x,
-                                 threadIdx.y, last && resid, d2, n2);
+        if (threadIdx.x == 0) {
+            atomicAdd(&resid[0], d2);
+            atomicAdd(&resid[1], n2);
         }
-        if (second) st = ring_step2(st);
-        else if (last) st = ring_step1(st);
-        if (!last && !grid_barrier(bar, gridDim.x, err)) return;
     }
-    if (resid) resid_reduce(d2, n2, resid);
 }
 
 // Two leap-frog steps per launch (temporal blocking), fed by tensor copies.
@@ -1129,21 +978,6 @@ cudaError_t launch_wave_f32(float* phi_new, const float* phi, const float* phi_o
 cudaError_t enqueue_wave_f32(float* ring, int64_t cells, const float* mass, const WaveF32& w, int k, int st,
                              double* resid, cudaStream_t s, const WaveMaps* maps, unsigned* err) {
     const size_t cz = static_cast<size_t>(cells);
-    // The persistent kernel, unless a tensor-copy kernel was asked for.
-    if (maps && !maps->ok && maps->persist_grid > 0 && maps->bar && err && k > 0) {
-        cudaError_t e = cudaMemsetAsync(maps->bar, 0, 2 * sizeof(unsigned), s);
-        if (e != cudaSuccess) return e;
-        cudaLaunchConfig_t cfg = {};
-        cfg.gridDim = dim3(static_cast<unsigned>(maps->persist_grid));
-        cfg.blockDim = dim3(kWX, kWY);
-        cfg.stream = s;
-        cudaLaunchAttribute attr[1];
-        attr[0].id = cudaLaunchAttributeCooperative;
-        attr[0].val.cooperative = 1;
-        cfg.attrs = attr;
-        cfg.numAttrs = 1;
-        return cudaLaunchKernelEx(&cfg, wave_persist_kernel, ring, mass, w, k, st, resid, maps->bar, err);
-    }
     const bool tma = maps && maps->ok && err;
     // One iteration: buffer `out` from phi^n in `cur` and phi^{n-1} in `old`.
     auto single = [&](int old, int cur, int out, double* r) {
@@ -1173,22 +1007,6 @@ cudaError_t enqueue_wave_f32(float* ring, int64_t cells, const float* mass, cons
         if (e != cudaSuccess) return e;
     }
     return cudaSuccess;
-}
-
-int wave_persist_grid(int nx) {
-    const char* e = std::getenv("KHRR_WAVE_PERSIST");
-    if (e && e[0] == '0') return 0;
-    const int64_t cells = static_cast<int64_t>(nx) * nx * nx;
-    if (cells > kPersistMaxCells) return 0;
-    int dev = 0, sms = 0, coop = 0, occ = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess ||
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
-        cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev) != cudaSuccess || !coop)
-        return 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, wave_persist_kernel, kWX * kWY, 0) != cudaSuccess || occ < 1)
-        return 0;
-    const int64_t ntiles = static_cast<int64_t>((nx + kWX - 1) / kWX) * ((nx + kWY - 1) / kWY) * ((nx + kPZ - 1) / kPZ);
-    return static_cast<int>(std::min<int64_t>(ntiles, static_cast<int64_t>(occ) * sms));
 }
 
 cudaError_t launch_wave1_tma(float* phi_new, const CUtensorMap& phi, const CUtensorMap& phi_old,

@@ -354,9 +354,6 @@ khrr_status khrr_wave_solve(khrr_ctx* c, const khrr_wave_params* p, double tol, 
     }
     const WaveF32 w = wave_f32(p, c->wave_tab.p);
     make_wave_maps(&c->wave_maps, c->wave_phi.p, c->wave_mass.p, p->nx);
-    if ((st = c->cuda(c->wave_bar.ensure(2), "alloc")) != KHRR_OK) return st;
-    c->wave_maps.bar = c->wave_bar.p;
-    c->wave_maps.persist_grid = wave_persist_grid(p->nx);
     // Graph of one chunk of `check_every` iterations starting at a ring state;
     // the last iteration of the chunk reduces the residual.
     auto chunk_graph = [&](int k, int rot, StepGraph** out) -> khrr_status {
@@ -514,9 +511,6 @@ khrr_status khrr_set_mesh_solver(khrr_ctx* c, const khrr_mesh_solver* p) {
                           "upload")) != KHRR_OK)
             return st;
         make_wave_maps(&M.maps, M.phi32.p, M.mass32.p, nx);
-        if ((st = c->cuda(M.bar.ensure(2), "alloc")) != KHRR_OK) return st;
-        M.maps.bar = M.bar.p;
-        M.maps.persist_grid = wave_persist_grid(nx);
     }
     M.cfg = *p;
     M.geom = g;

@@ -228,24 +228,19 @@ def test_wave_solve_fp32_matches_restatement_and_converges(ctx, oracle):
     assert res4 < res3 * 1.5 and it4 < 100000
 
 
-@pytest.mark.parametrize("kernel", ["persistent", "0", "1", "2"])
+@pytest.mark.parametrize("kernel", ["0", "1", "2"])
 @pytest.mark.parametrize("nx,max_iter,check_every", [(37, 7, 3), (40, 6, 6), (200, 5, 5)])
 def test_wave_solve_pairs_and_singles_bit_exact(ctx, oracle, nx, max_iter, check_every, kernel, monkeypatch):
-    """Every FP32 stencil kernel: the persistent one (all iterations of a
-    chunk in one cooperative launch, meshes up to 5 M cells; larger ones use
-    the cache-fed kernel), KHRR_WAVE_TMA 0 the cache-fed one-step kernel
-    launched per step (persistent kernel off), 1 the tensor-copy one-step
-    kernel, 2 pairs through the tensor-copy two-step kernel (meshes the
-    tensor-copy kernels cannot take, nx = 37, fall back); odd counts too: the
-    field equals
+    """Every FP32 stencil kernel (KHRR_WAVE_TMA: 0 the cache-fed one-step
+    kernel, 1 the tensor-copy one-step kernel, 2 pairs through the
+    tensor-copy two-step kernel; meshes the tensor-copy kernels cannot take,
+    nx = 37, fall back to the cache-fed one) and odd counts: the field equals
     the oracle's FP32 restatement bit for bit (meshes that are not multiples
     of the 32 x 8 x TZ tile, and the TZ = 32 shape from nx = 192 up), and the
     residual of the last iteration matches the FP64 norm of the oracle's last
     step."""
     import khrr
-    if kernel != "persistent":
-        monkeypatch.setenv("KHRR_WAVE_TMA", kernel)
-        monkeypatch.setenv("KHRR_WAVE_PERSIST", "0")
+    monkeypatch.setenv("KHRR_WAVE_TMA", kernel)
     pos, vel, mass, eps2 = galaxy_state(2048, 4096, 18)
     L = 3.0
     dx = 2 * L / nx
