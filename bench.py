@@ -345,6 +345,24 @@ def mesh_leg(khrr, device, torch, hbm_gbs, iter_cap=0):
     return out
 
 
+def max_over_ranks(dist, values, device="cpu"):
+    """Element-wise maximum of per-rank timings over all ranks (the identity
+    without a process group).  Every rank calls it at the same point."""
+    if not dist:
+        return [float(v) for v in values]
+    import torch
+    t = torch.tensor([float(v) for v in values], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(v) for v in t.tolist()]
+
+
+def replica_rate(world, pairs_per_step, steps, ms_max):
+    """Whole-job interactions per second (G/s) of `world` independent
+    replicas, each doing `steps` steps of `pairs_per_step` pairs, timed as the
+    slowest rank's `ms_max`."""
+    return world * pairs_per_step * steps / (ms_max * 1e-3) / 1e9
+
+
 def run_khrr(args):
     import torch
     import khrr
@@ -410,13 +428,9 @@ def run_khrr(args):
     if launches < 1 or force_ms <= 0.0:
         raise RuntimeError("force-kernel timing events recorded nothing")
     barrier()
-    ms_max = ms
-    if dist:
-        t = torch.tensor([ms], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms_max = float(t.item())
+    (ms_max,) = max_over_ranks(dist, [ms], device="cuda")
     pairs_step = float(n) * n
-    value = world * pairs_step * args.steps / (ms_max * 1e-3) / 1e9
+    value = replica_rate(world, pairs_step, args.steps, ms_max)
 
     # end to end through the C ABI: pinned host inputs -> step -> host outputs
     pin = lambda shape: torch.empty(shape, dtype=torch.float64, pin_memory=True).numpy()
@@ -436,12 +450,8 @@ def run_khrr(args):
         e1.synchronize()
         if k >= args.warmup:
             e2e_ms.append(e0.elapsed_time(e1))
-    e2e_total = sum(e2e_ms)
-    if dist:
-        t = torch.tensor([e2e_total], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_total = float(t.item())
-    e2e_value = world * pairs_step * args.steps / (e2e_total * 1e-3) / 1e9
+    (e2e_total,) = max_over_ranks(dist, [sum(e2e_ms)], device="cuda")
+    e2e_value = replica_rate(world, pairs_step, args.steps, e2e_total)
 
     peaks = measured_peaks()
     sm_max = float(peaks.get("sm_max_mhz", 1965.0))
