@@ -391,6 +391,15 @@ khrr_status khrr_pair_count(khrr_ctx* ctx, double* pairs);
 /* FP32 FMA throughput probe: a dependent-chain FMA kernel on all SMs;
  * returns TFLOP/s (2 flops per FMA) measured with CUDA events. */
 khrr_status khrr_fp32_probe(khrr_ctx* ctx, double* tflops);
+/* Failure-path check (the reference has no failure detection; main only
+ * catches host exceptions, nbody.cu:1713-1721): runs one kernel that waits,
+ * through the same bounded wait as the force and stencil kernels, on a
+ * barrier nothing completes.  It gives up after `seconds` (0 < s <= 10),
+ * raises the context's device error flag and returns; this call then reports
+ * KHRR_ERR_TIMEOUT with the message a stalled copy gives, and clears the
+ * flag.  The context stays usable.  No fault, trap or unbounded loop is
+ * involved. */
+khrr_status khrr_probe_bounded_wait(khrr_ctx* ctx, double seconds);
 
 #ifdef __cplusplus
 }

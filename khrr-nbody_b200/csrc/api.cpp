@@ -868,4 +868,15 @@ khrr_status khrr_fp32_probe(khrr_ctx* c, double* tflops) {
     return KHRR_OK;
 }
 
+khrr_status khrr_probe_bounded_wait(khrr_ctx* c, double seconds) {
+    if (!c) return KHRR_ERR_INVALID_ARG;
+    if (!(seconds > 0.0) || seconds > 10.0) return c->fail(KHRR_ERR_INVALID_ARG, "seconds must be in (0, 10]");
+    khrr_status st = c->check_device_flag();  // report (and clear) anything raised earlier first
+    if (st != KHRR_OK) return st;
+    if ((st = c->cuda(launch_wait_probe(c->errflag.p, static_cast<unsigned long long>(seconds * 1e9), c->stream),
+                      "wait probe")) != KHRR_OK)
+        return st;
+    return c->check_device_flag();
+}
+
 }  // extern "C"

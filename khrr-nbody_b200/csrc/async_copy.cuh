@@ -51,14 +51,16 @@ __device__ __forceinline__ uint64_t global_ns() {
     return t;
 }
 
-// Waits for phase `parity` of an mbarrier; gives up after ~2 s of wall time.
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, unsigned parity) {
+// Waits for phase `parity` of an mbarrier; gives up after limit_ns of wall
+// time (~2 s by default) and returns false.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, unsigned parity,
+                                                  uint64_t limit_ns = 2000000000ull) {
     if (mbar_try_wait(bar, parity)) return true;
     const uint64_t t0 = global_ns();
     for (;;) {
         for (int k = 0; k < 256; ++k)
             if (mbar_try_wait(bar, parity)) return true;
-        if (global_ns() - t0 > 2000000000ull) return false;
+        if (global_ns() - t0 > limit_ns) return false;
     }
 }
 

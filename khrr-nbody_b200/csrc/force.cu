@@ -480,6 +480,20 @@ __global__ void reduce_partials_kernel(const double4* __restrict__ part, long lo
     }
 }
 
+// The failure path of the bounded waits, on purpose: one CTA waits on an
+// mbarrier that nothing arrives on (no copy is issued), gives up after
+// limit_ns, raises the error flag and returns like a stalled kernel does.
+__global__ void wait_probe_kernel(unsigned* err, unsigned long long limit_ns) {
+    __shared__ alignas(8) uint64_t bar;
+    if (threadIdx.x == 0) {
+        mbar_init(&bar, 1);
+        fence_mbar_init();
+    }
+    __syncthreads();
+    const bool ok = mbar_wait_bounded(&bar, 0u, limit_ns);
+    if (__syncthreads_or(!ok) && threadIdx.x == 0) atomicOr(err, kErrTimeout);
+}
+
 __global__ void fp32_probe_kernel(float* out, int iters) {
     float a0 = threadIdx.x * 1e-7f, a1 = a0 + 1e-7f, a2 = a0 + 2e-7f, a3 = a0 + 3e-7f;
     float a4 = a0 + 4e-7f, a5 = a0 + 5e-7f, a6 = a0 + 6e-7f, a7 = a0 + 7e-7f;
@@ -591,6 +605,11 @@ cudaError_t launch_reduce_partials(const double4* part, long long npad, int nslo
                                    double* acc, double* phi, bool overwrite, cudaStream_t s) {
     reduce_partials_kernel<<<grid_for(n, 256), 256, 0, s>>>(part, npad, nslots, n, acc, phi,
                                                             overwrite ? 1 : 0);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_wait_probe(unsigned* err, unsigned long long limit_ns, cudaStream_t s) {
+    wait_probe_kernel<<<1, 32, 0, s>>>(err, limit_ns);
     return cudaGetLastError();
 }
 

@@ -92,6 +92,9 @@ cudaError_t launch_pack(const double* pos, const double* mass, const double* eps
 cudaError_t launch_reduce_partials(const double4* part, long long npad, int nslots, int64_t n,
                                    double* acc, double* phi, bool overwrite, cudaStream_t s);
 cudaError_t launch_fp32_probe(float* out, int iters, int grid, int block, cudaStream_t s);
+// One CTA waiting (bounded, limit_ns) on an mbarrier nothing completes: the
+// timeout path of every bounded wait, raising kErrTimeout in *err.
+cudaError_t launch_wait_probe(unsigned* err, unsigned long long limit_ns, cudaStream_t s);
 // FP64 direct sum for sampled targets: tgt[k] is a padded index, [jb[k], je[k])
 // its system's padded body range; out4[k] = (ax, ay, az, phi).
 cudaError_t launch_fp64_sample(const double* pos, const double* mass, const double* eps2,

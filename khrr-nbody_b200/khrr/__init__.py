@@ -143,6 +143,7 @@ def lib(path: pathlib.Path | str | None = None) -> C.CDLL:
         "khrr_wave_solve": ([vp, C.POINTER(WaveParams), d, i, i, i, C.POINTER(i), C.POINTER(d), vp], i),
         "khrr_bin_cell_phi": ([vp, i, vp], i),
         "khrr_accel_noalloc": ([vp, vp, vp, vp, vp, i64, i, vp], i),
+        "khrr_probe_bounded_wait": ([vp, d], i),
         "khrr_cic_deposit": ([vp, vp, vp, i64, C.POINTER(Mesh), vp], i),
         "khrr_cic_gather": ([vp, vp, i64, C.POINTER(Mesh), vp, vp, vp, vp], i),
         "khrr_sort_by_cell": ([vp, vp], i),
@@ -404,6 +405,11 @@ class Context:
             iters_per_step = int(dt / params.dt)
         ms = MeshSolver(params, int(assign), 1 if fp64 else 0, int(iters_per_step), int(setup_iters))
         self._check(self.L.khrr_set_mesh_solver(self.h, C.byref(ms)))
+
+    def probe_bounded_wait(self, seconds=0.2) -> int:
+        """Status of the library's bounded-wait failure path (KHRR_ERR_TIMEOUT
+        = 5 when it works); raises nothing."""
+        return int(self.L.khrr_probe_bounded_wait(self.h, float(seconds)))
 
     def mesh_solver_phi(self, nx):
         out = np.empty(nx ** 3)
