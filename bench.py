@@ -396,6 +396,10 @@ def run_khrr(args):
     err = float(np.sqrt(((acc0[tg] - ref) ** 2).sum() / (ref ** 2).sum()))
     err_max = float(np.max(np.linalg.norm(acc0[tg] - ref, axis=1) / np.linalg.norm(ref, axis=1)))
 
+    # conservation at the start (potentials of the current positions)
+    ctx.forces(khrr.ACC | khrr.PHI)
+    lie0 = ctx.conservation()
+
     stream = torch.cuda.ExternalStream(ctx.stream)
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
     torch.cuda.synchronize()
@@ -427,6 +431,28 @@ def run_khrr(args):
     tuning = ctx.get_tuning()
     if launches < 1 or force_ms <= 0.0:
         raise RuntimeError("force-kernel timing events recorded nothing")
+    # conservation after warm-up + timed steps (one more step, with potentials,
+    # outside the timed region): relative energy and L_z drift over the run
+    ctx.step(DT, 1, khrr.PHI)
+    lie1 = ctx.conservation()
+    drift = {"steps": args.warmup + args.steps + 1,
+             "energy_rel": abs(lie1["E"] / lie0["E"] - 1.0),
+             "lz_rel": abs(lie1["Lz"] / lie0["Lz"] - 1.0) if lie0["Lz"] != 0 else None}
+
+    # the plain path on the same galaxy: the conventional one-body-per-thread
+    # FP32 kernel, one launch per system (CUDA events, outside the timed region)
+    ctx.upload(pos, vel, mass, eps2)
+    ctx.forces(khrr.ACC | khrr.PLAIN)
+    ctx.step(DT, 1, khrr.PLAIN)
+    p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    p0.record(stream)
+    ctx.step(DT, 2, khrr.PLAIN)
+    p1.record(stream)
+    p1.synchronize()
+    plain_ms = p0.elapsed_time(p1) / 2
+    plain = {"value": float(n) * n / (plain_ms * 1e-3) / 1e9, "unit": UNIT, "ms_per_step": plain_ms,
+             "what": "KHRR_PLAIN: one i body per thread, 256-body shared-memory j tiles, one launch per system"}
+
     barrier()
     (ms_max,) = max_over_ranks(dist, [ms], device="cuda")
     pairs_step = float(n) * n
@@ -480,12 +506,15 @@ def run_khrr(args):
         return 0
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+        "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "steps_per_s": 1e3 * args.steps / ms_max,
+        "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32 pair terms (compensated sums), f64 integrator",
         "data": "synthetic (seeded disk-galaxy generator)",
         "config": config(args, {"tuning": tuning}),
         "pct_fp32_peak": 100.0 * achieved / peak_tflops,
         "acc_rel_rms_vs_fp64": err, "acc_rel_max_vs_fp64": err_max, "acc_err_targets": int(len(tg)),
+        "drift": drift,
+        "plain": plain,
         "roofline": {"bound": "fp32", "kernel": "force_kernel", "achieved": achieved, "peak": peak_tflops,
                      "unit": "TFLOP/s", "frac": achieved / peak_tflops,
                      # DRAM read+write of one force launch from the ncu capture on
