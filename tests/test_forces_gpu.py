@@ -319,3 +319,35 @@ def test_timing_counts_force_launches(ctx):
     assert launches1 == 1 and ms1 > 0.0
     assert launches3 == 3 and ms3 > 0.0
     assert pairs3 == 3 * float(len(mass)) ** 2
+
+
+def test_autotuner_picks_a_shape_caches_it_and_keeps_parity(ctx, oracle, tmp_path):
+    """khrr_autotune times the candidate kernel shapes on the uploaded state,
+    keeps the fastest, and caches it per layout; a second context with the same
+    layout takes the cached shape without timing; forces stay within tolerance."""
+    import json
+    import time
+    import khrr
+    candidates = {(128, 2, 1), (128, 4, 1), (256, 2, 1), (256, 4, 1), (128, 4, 0), (128, 8, 0), (256, 4, 0),
+                  (256, 8, 0)}
+    pos, vel, mass, eps2 = galaxy(2048, 4096, seed=61)
+    cache = tmp_path / "tune.json"
+    ctx.upload(pos, vel, mass, eps2)
+    ctx.autotune(cache)
+    t = ctx.get_tuning()
+    assert (t["threads"], t["i_per_thread"], t["packed"]) in candidates
+    entries = json.loads(cache.read_text())
+    assert list(entries.values()) == [[t["threads"], t["i_per_thread"], t["j_tile"], t["j_split"], t["packed"]]]
+    ctx.forces(khrr.ACC)
+    assert rel_rms(ctx.download()["acc"], oracle.accel_f64(pos, mass, eps2)) <= SMALL_N_TOL
+    other = khrr.Context(0)
+    try:
+        other.upload(pos, vel, mass, eps2)
+        other.set_tuning(128, 8, 128, 0, 0)          # something else first
+        t0 = time.perf_counter()
+        other.autotune(cache)
+        assert time.perf_counter() - t0 < 0.5      # read from the cache, nothing timed
+        assert other.get_tuning() == t
+    finally:
+        other.close()
+    ctx.set_tuning()                                 # back to the default shape for later tests
