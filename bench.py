@@ -386,8 +386,9 @@ def run_khrr(args):
     n = len(mass)
     ctx = khrr.Context(local)
     ctx.upload(pos, vel, mass, eps2)
-    # kernel shape picked by the autotuner (timed candidates, cached per layout)
-    ctx.autotune(ROOT / "khrr-nbody_b200" / "build" / "autotune_cache.json")
+    # kernel shape picked by the autotuner (timed candidates, cached per layout;
+    # one cache file per local rank, so replicas never write the same file)
+    ctx.autotune(ROOT / "khrr-nbody_b200" / "build" / f"autotune_cache.{local}.json")
     ctx.forces(khrr.ACC)
 
     # accuracy vs FP64 on 4096 seeded targets (GPU FP64 direct sum)
