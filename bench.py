@@ -345,6 +345,38 @@ def mesh_leg(khrr, device, torch, hbm_gbs, iter_cap=0):
     return out
 
 
+def kick_drift_leg(khrr, ctx, torch, n, hbm_gbs):
+    """The predictor and corrector as the reference launches them
+    (khrr_integ_time = kernelNbody_integTime, nbody-kernel.cuh:144-193) on n
+    bodies in device memory, in achieved GB/s of algorithmic bytes: predictor
+    120 B per body (read acc, pos, vel; write pos_t, vel_t), corrector 168 B
+    (read acc, pos, vel, vel_t; write pos_t, vel_t, acc0)."""
+    g = torch.Generator(device="cuda").manual_seed(3)
+    arr = lambda: torch.randn((n, 3), dtype=torch.float64, device="cuda", generator=g)
+    acc, pos, vel, pos_t, vel_t, acc0 = arr(), arr(), arr(), arr(), arr(), arr()
+    s = torch.cuda.ExternalStream(ctx.stream)
+    torch.cuda.synchronize()
+    out = {}
+    for istep, label, nbytes in ((0, "predictor", 120), (1, "corrector", 168)):
+        call = lambda: ctx.integ_time(acc.data_ptr(), pos_t.data_ptr(), vel_t.data_ptr(), pos.data_ptr(),
+                                      vel.data_ptr(), DT, istep, 0.0, acc0.data_ptr(), n)
+        for _ in range(3):
+            call()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        reps = 20
+        e0.record(s)
+        for _ in range(reps):
+            call()
+        e1.record(s)
+        e1.synchronize()
+        ms = e0.elapsed_time(e1) / reps
+        gbs = nbytes * n / (ms * 1e-3) / 1e9
+        out[label] = {"ms": ms, "gbs": gbs, "frac_of_hbm": gbs / hbm_gbs, "bytes_per_body": nbytes}
+    out["bodies"] = n
+    out["note"] = f"{120 * n / 1e6:.0f}-{168 * n / 1e6:.0f} MB per pass (above the 126 MB L2)"
+    return out
+
+
 def max_over_ranks(dist, values, device="cpu"):
     """Element-wise maximum of per-rank timings over all ranks (the identity
     without a process group).  Every rank calls it at the same point."""
@@ -489,6 +521,9 @@ def run_khrr(args):
     achieved = FLOPS_PER_PAIR * (pairs_timed / max(launches, 1)) / avg_launch_s / 1e12
     probe = ctx.fp32_probe()
 
+    kick = None
+    if rank == 0:
+        kick = kick_drift_leg(khrr, ctx, torch, 4 * n, float(peaks.get("hbm_gbs", 6650.0)))
     ens = None
     if not args.no_ensemble and rank == 0:
         ens = ensemble_leg(khrr, local, torch)
@@ -536,6 +571,7 @@ def run_khrr(args):
                         "khrr_download_state(pos, vel, acc)"},
         "gpu_launches": 2 * args.steps,
         "clocks": clk.summary(),
+        "kick_drift": kick,
         "ensemble": ens,
         "mesh": mesh,
     }
