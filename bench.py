@@ -327,6 +327,28 @@ def mesh_leg(khrr, device, torch, hbm_gbs, iter_cap=0):
                 "cic_bytes_note": "32 B per body (FP64 position, mass) + 16 B per cell (zeroed, summed)",
                 "sort_ms": sort_ms, "sort_gbs": 16.0 * n / (sort_ms * 1e-3) / 1e9,
             }
+            if label == "large_256":
+                # The reference's own FP64 stencil (wave_diss_iteration's
+                # expression, khrr_wave_iteration) on the same mesh: 32 B/cell.
+                f64 = [torch.zeros(ncells, dtype=torch.float64, device=device) for _ in range(3)]
+                m64 = torch.rand(ncells, dtype=torch.float64, device=device) * 1e-4  # timing only: values do not matter
+                torch.cuda.synchronize()
+                k = [0]
+
+                def f64_iter():
+                    o, c, nx_ = f64[k[0] % 3], f64[(k[0] + 1) % 3], f64[(k[0] + 2) % 3]
+                    ctx.wave_iteration(nx_.data_ptr(), c.data_ptr(), o.data_ptr(), m64.data_ptr(), W)
+                    k[0] += 1
+                f64_iter()
+
+                def f64_run():
+                    for _ in range(20):
+                        f64_iter()
+                f64_ms = timed(f64_run, reps=3) / 20
+                out[label].update({"wave_f64_ms_per_iteration": f64_ms,
+                                   "wave_f64_gbs": 32.0 * ncells / (f64_ms * 1e-3) / 1e9,
+                                   "wave_f64_frac_of_hbm": 32.0 * ncells / (f64_ms * 1e-3) / 1e9 / hbm_gbs})
+                del f64, m64
             if label == "encounter_128":
                 # The reference's Wave mode on this mesh: FP32 stencil, CIC,
                 # (int)(dt / dt_wave) iterations per dt = 0.002 step.
