@@ -520,6 +520,7 @@ khrr_status khrr_set_external_field(khrr_ctx* c, const khrr_field_params* p) {
 khrr_status khrr_upload_state(khrr_ctx* c, int64_t n, const double* pos, const double* vel,
                               const double* mass, const double* eps2, int nsys,
                               const int64_t* sys_offsets) {
+    khrr::NvtxRange nvtx_range("khrr_upload_state");
     if (!c) return KHRR_ERR_INVALID_ARG;
     if (n < 1 || !pos || !vel || !mass || !eps2) return c->fail(KHRR_ERR_INVALID_ARG, "bad state arrays");
     if (nsys < 1 || (nsys > 1 && !sys_offsets)) return c->fail(KHRR_ERR_INVALID_ARG, "bad system count");
@@ -673,6 +674,7 @@ khrr_status khrr_accel_fp64_sample(khrr_ctx* c, const int64_t* targets, int64_t 
 }
 
 khrr_status khrr_download_state(khrr_ctx* c, double* pos, double* vel, double* acc, double* phi) {
+    khrr::NvtxRange nvtx_range("khrr_download_state");
     if (!c) return KHRR_ERR_INVALID_ARG;
     if (!c->has_state) return c->fail(KHRR_ERR_STATE, "no state uploaded");
     cudaStream_t s = c->stream;
@@ -690,6 +692,7 @@ khrr_status khrr_download_state(khrr_ctx* c, double* pos, double* vel, double* a
 }
 
 khrr_status khrr_forces(khrr_ctx* c, int flags) {
+    khrr::NvtxRange nvtx_range("khrr_forces");
     if (!c) return KHRR_ERR_INVALID_ARG;
     if (!c->has_state) return c->fail(KHRR_ERR_STATE, "no state uploaded");
     const bool want_acc = (flags & KHRR_ACC) != 0, want_phi = (flags & KHRR_PHI) != 0;
@@ -721,6 +724,7 @@ khrr_status khrr_forces(khrr_ctx* c, int flags) {
 }
 
 khrr_status khrr_step(khrr_ctx* c, double dt, int nsteps, int flags) {
+    khrr::NvtxRange nvtx_range("khrr_step");
     if (!c) return KHRR_ERR_INVALID_ARG;
     if (!c->has_state) return c->fail(KHRR_ERR_STATE, "no state uploaded");
     if (nsteps < 0 || !std::isfinite(dt)) return c->fail(KHRR_ERR_INVALID_ARG, "bad step arguments");
@@ -758,6 +762,7 @@ khrr_status khrr_step(khrr_ctx* c, double dt, int nsteps, int flags) {
 }
 
 khrr_status khrr_conservation(khrr_ctx* c, khrr_lie* out) {
+    khrr::NvtxRange nvtx_range("khrr_conservation");
     if (!c || !out) return KHRR_ERR_INVALID_ARG;
     if (!c->has_state) return c->fail(KHRR_ERR_STATE, "no state uploaded");
     const int nb = conservation_blocks(c->npad);

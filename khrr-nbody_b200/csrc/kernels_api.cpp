@@ -106,6 +106,7 @@ extern "C" {
 
 khrr_status khrr_accel(khrr_ctx* c, double* acc, const double* pos_i, const double* pos_j,
                        const double* mass_j, const double* eps2_j, int64_t n, int flags) {
+    khrr::NvtxRange nvtx_range("khrr_accel");
     if (!c) return KHRR_ERR_INVALID_ARG;
     if (!acc) return c->fail(KHRR_ERR_INVALID_ARG, "null acc");
     const ForceVariant* v = nullptr;
@@ -119,6 +120,7 @@ khrr_status khrr_accel(khrr_ctx* c, double* acc, const double* pos_i, const doub
 
 khrr_status khrr_phi(khrr_ctx* c, double* phi, const double* pos_i, const double* pos_j,
                      const double* mass_j, const double* eps2_j, int64_t n, int flags) {
+    khrr::NvtxRange nvtx_range("khrr_phi");
     if (!c) return KHRR_ERR_INVALID_ARG;
     if (!phi) return c->fail(KHRR_ERR_INVALID_ARG, "null phi");
     const ForceVariant* v = nullptr;
@@ -145,6 +147,7 @@ khrr_status khrr_integ_time(khrr_ctx* c, const double* acc, double* pos_t, doubl
 // uploaded state (automatic j split), the fastest kept; the winner is cached
 // per state key ("npad:nsys:uniform") in a small JSON object file.
 khrr_status khrr_autotune(khrr_ctx* c, const char* cache_path) {
+    khrr::NvtxRange nvtx_range("khrr_autotune");
     if (!c) return KHRR_ERR_INVALID_ARG;
     if (!c->has_state) return c->fail(KHRR_ERR_STATE, "no state uploaded");
     char key[96];

@@ -2,6 +2,7 @@
 #pragma once
 
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include <cstdint>
 #include <map>
@@ -14,6 +15,15 @@
 #include "khrr_internal.h"
 
 namespace khrr {
+
+// An NVTX range over one library call, shown by Nsight Systems as a named
+// phase (header-only NVTX v3; without a tool attached it costs a few ns).
+struct NvtxRange {
+    explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+    ~NvtxRange() { nvtxRangePop(); }
+    NvtxRange(const NvtxRange&) = delete;
+    NvtxRange& operator=(const NvtxRange&) = delete;
+};
 
 // Grow-only device allocation.
 template <class T>

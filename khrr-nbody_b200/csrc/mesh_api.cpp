@@ -225,6 +225,7 @@ khrr_status khrr_apply_cells_to_particles(khrr_ctx* c, double* particle_acc, dou
 
 khrr_status khrr_bin(khrr_ctx* c, const khrr_mesh* mesh, int* cell_id, int* id_in_cell, int* count, int* start,
                      int* start_ref, double* cell_mass) {
+    khrr::NvtxRange nvtx_range("khrr_bin");
     if (!c) return KHRR_ERR_INVALID_ARG;
     if (!c->has_state) return c->fail(KHRR_ERR_STATE, "no state uploaded");
     MeshGeom g;
@@ -294,6 +295,7 @@ khrr_status khrr_bin(khrr_ctx* c, const khrr_mesh* mesh, int* cell_id, int* id_i
 }
 
 khrr_status khrr_bin_cell_phi(khrr_ctx* c, int reset, double* cell_phi) {
+    khrr::NvtxRange nvtx_range("khrr_bin_cell_phi");
     if (!c) return KHRR_ERR_INVALID_ARG;
     if (!c->has_bin) return c->fail(KHRR_ERR_STATE, "no binned bodies (call khrr_bin first)");
     const size_t C = static_cast<size_t>(c->ncells);
@@ -319,6 +321,7 @@ khrr_status khrr_bin_cell_phi(khrr_ctx* c, int reset, double* cell_phi) {
 
 khrr_status khrr_wave_solve(khrr_ctx* c, const khrr_wave_params* p, double tol, int max_iter, int check_every,
                             int cold, int* iters, double* resid, float* phi_out) {
+    khrr::NvtxRange nvtx_range("khrr_wave_solve");
     if (!c) return KHRR_ERR_INVALID_ARG;
     khrr_status st = check_wave(c, p);
     if (st != KHRR_OK) return st;
@@ -435,6 +438,7 @@ khrr_status check_cubic(khrr_ctx* c, const khrr_mesh* m, MeshGeom* g, int64_t* n
 
 khrr_status khrr_cic_deposit(khrr_ctx* c, const double* pos, const double* mass, int64_t n, const khrr_mesh* mesh,
                              double* cell_mass) {
+    khrr::NvtxRange nvtx_range("khrr_cic_deposit");
     if (!c) return KHRR_ERR_INVALID_ARG;
     MeshGeom g;
     int64_t C = 0;
@@ -446,6 +450,7 @@ khrr_status khrr_cic_deposit(khrr_ctx* c, const double* pos, const double* mass,
 
 khrr_status khrr_cic_gather(khrr_ctx* c, const double* pos, int64_t n, const khrr_mesh* mesh, const double* cell_acc,
                             const double* cell_value, double* particle_acc, double* particle_value) {
+    khrr::NvtxRange nvtx_range("khrr_cic_gather");
     if (!c) return KHRR_ERR_INVALID_ARG;
     MeshGeom g;
     int64_t C = 0;
@@ -458,6 +463,7 @@ khrr_status khrr_cic_gather(khrr_ctx* c, const double* pos, int64_t n, const khr
 }
 
 khrr_status khrr_sort_by_cell(khrr_ctx* c, int* order) {
+    khrr::NvtxRange nvtx_range("khrr_sort_by_cell");
     if (!c) return KHRR_ERR_INVALID_ARG;
     if (!c->has_bin) return c->fail(KHRR_ERR_STATE, "no binned bodies (call khrr_bin first)");
     if (c->n > 0x7fffffffLL) return c->fail(KHRR_ERR_INVALID_ARG, "more bodies than int32 indices");
@@ -476,6 +482,7 @@ khrr_status khrr_sort_by_cell(khrr_ctx* c, int* order) {
 }
 
 khrr_status khrr_set_mesh_solver(khrr_ctx* c, const khrr_mesh_solver* p) {
+    khrr::NvtxRange nvtx_range("khrr_set_mesh_solver");
     if (!c) return KHRR_ERR_INVALID_ARG;
     MeshSolver& M = c->msolver;
     M.drop_graphs();
