@@ -108,7 +108,7 @@ khrr_status khrr_synchronize(khrr_ctx* ctx);
 /* ACCEL_kernel (nbody-kernel.cuh:89-142): acc[i] += sum_j m_j d/(d^2 +
  * (eps2_i + eps2_j)/2)^{3/2}, d = pos_j[j] - pos_i[i], over i, j < n
  * (KHRR_OVERWRITE: acc = sum).  pos_*, acc: n double3 (AoS xyz); mass_j,
- * eps2_j: n doubles.  Pair terms in FP32 with compensated sums; any n >= 1
+ * eps2_j: n doubles.  Pair terms in FP32 with compensated sums; any n >= 0 (0: nothing to do)
  * (the reference needs n % 512 == 0). */
 khrr_status khrr_accel(khrr_ctx* ctx, double* acc, const double* pos_i, const double* pos_j,
                        const double* mass_j, const double* eps2_j, int64_t n, int flags);

@@ -108,6 +108,7 @@ khrr_status khrr_accel(khrr_ctx* c, double* acc, const double* pos_i, const doub
                        const double* mass_j, const double* eps2_j, int64_t n, int flags) {
     khrr::NvtxRange nvtx_range("khrr_accel");
     if (!c) return KHRR_ERR_INVALID_ARG;
+    if (n == 0) return KHRR_OK;  // nothing to do, as a launch of zero blocks
     if (!acc) return c->fail(KHRR_ERR_INVALID_ARG, "null acc");
     const ForceVariant* v = nullptr;
     khrr_status st = prepare_kernel_pass(c, pos_i, pos_j, mass_j, eps2_j, n, true, false, &v);
@@ -122,6 +123,7 @@ khrr_status khrr_phi(khrr_ctx* c, double* phi, const double* pos_i, const double
                      const double* mass_j, const double* eps2_j, int64_t n, int flags) {
     khrr::NvtxRange nvtx_range("khrr_phi");
     if (!c) return KHRR_ERR_INVALID_ARG;
+    if (n == 0) return KHRR_OK;
     if (!phi) return c->fail(KHRR_ERR_INVALID_ARG, "null phi");
     const ForceVariant* v = nullptr;
     khrr_status st = prepare_kernel_pass(c, pos_i, pos_j, mass_j, eps2_j, n, false, true, &v);
@@ -137,7 +139,8 @@ khrr_status khrr_integ_time(khrr_ctx* c, const double* acc, double* pos_t, doubl
                             double* acc0, int64_t n) {
     (void)t;  // the reference passes t to dev_fex, which ignores it (static field)
     if (!c) return KHRR_ERR_INVALID_ARG;
-    if (n < 1 || !acc || !pos_t || !vel_t || !pos || !vel || (istep == 1 && !acc0) || (istep != 0 && istep != 1))
+    if (n == 0) return KHRR_OK;
+    if (n < 0 || !acc || !pos_t || !vel_t || !pos || !vel || (istep == 1 && !acc0) || (istep != 0 && istep != 1))
         return c->fail(KHRR_ERR_INVALID_ARG, "bad integrator arguments");
     return c->cuda(launch_integ_time(acc, pos_t, vel_t, pos, vel, dt, istep, acc0, n, c->field, c->stream),
                    "integrator");

@@ -58,19 +58,37 @@ __device__ __forceinline__ int cell_of(const double* __restrict__ p, const MeshG
     return iz * m.g[0] * m.g[1] + iy * m.g[2] + ix;
 }
 
+// kAssignPer bodies per thread (strided by the block size, so loads stay
+// coalesced): their slot atomics are independent and go out back to back,
+// so a thread waits for all of them once instead of once per body.
+constexpr int kAssignPer = 4;
+
 __global__ void assign_kernel(const double* __restrict__ pos, int64_t n, const MeshGeom m, int2* __restrict__ pci,
                               int* __restrict__ counter, int counter_stride, int* __restrict__ count2,
                               int count2_stride, const double* __restrict__ mass, double* __restrict__ cell_mass) {
-    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const int c = cell_of(pos + 3 * i, m);
+    const int64_t base = blockIdx.x * (int64_t)blockDim.x * kAssignPer + threadIdx.x;
+    int c[kAssignPer], slot[kAssignPer];
+#pragma unroll
+    for (int k = 0; k < kAssignPer; ++k) {
+        const int64_t i = base + static_cast<int64_t>(k) * blockDim.x;
+        c[k] = i < n ? cell_of(pos + 3 * i, m) : 0;
+    }
     // One atomic per body, as the reference does: bodies arrive in no
     // spatial order, so warp-level aggregation finds almost no shared cells
     // and its match/shuffle traffic costs more than it saves.
-    const int slot = atomicAdd(&counter[static_cast<int64_t>(c) * counter_stride], 1);
-    if (count2) atomicAdd(&count2[static_cast<int64_t>(c) * count2_stride], 1);
-    pci[i] = make_int2(c, slot);
-    if (cell_mass) atomicAdd(&cell_mass[c], mass[i]);
+#pragma unroll
+    for (int k = 0; k < kAssignPer; ++k) {
+        const int64_t i = base + static_cast<int64_t>(k) * blockDim.x;
+        slot[k] = i < n ? atomicAdd(&counter[static_cast<int64_t>(c[k]) * counter_stride], 1) : 0;
+    }
+#pragma unroll
+    for (int k = 0; k < kAssignPer; ++k) {
+        const int64_t i = base + static_cast<int64_t>(k) * blockDim.x;
+        if (i >= n) continue;
+        if (count2) atomicAdd(&count2[static_cast<int64_t>(c[k]) * count2_stride], 1);
+        pci[i] = make_int2(c[k], slot[k]);
+        if (cell_mass) atomicAdd(&cell_mass[c[k]], mass[i]);
+    }
 }
 
 // Cells and the NGP mass deposit only (the mesh-force step needs no slots).
@@ -971,8 +989,8 @@ cudaError_t launch_assign(const double* pos, int64_t n, const MeshGeom& m, int2*
                           int counter_stride, int* count2, int count2_stride, const double* mass, double* cell_mass,
                           cudaStream_t s) {
     if (n < 1) return cudaSuccess;
-    assign_kernel<<<static_cast<unsigned>((n + 255) / 256), 256, 0, s>>>(pos, n, m, pci, counter, counter_stride,
-                                                                           count2, count2_stride, mass, cell_mass);
+    assign_kernel<<<static_cast<unsigned>((n + 256 * kAssignPer - 1) / (256 * kAssignPer)), 256, 0, s>>>(
+        pos, n, m, pci, counter, counter_stride, count2, count2_stride, mass, cell_mass);
     return cudaGetLastError();
 }
 

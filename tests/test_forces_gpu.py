@@ -351,3 +351,26 @@ def test_autotuner_picks_a_shape_caches_it_and_keeps_parity(ctx, oracle, tmp_pat
     finally:
         other.close()
     ctx.set_tuning()                                 # back to the default shape for later tests
+
+
+def test_empty_inputs_are_no_ops(ctx, torch_cuda):
+    """n = 0 does nothing and succeeds, as a reference launch of zero blocks
+    does: kernel-level forces, potentials, the integrator, binning, the CIC
+    deposit and the gathers leave their outputs untouched."""
+    import khrr
+    torch = torch_cuda
+    sentinel = torch.full((8, 3), 7.0, dtype=torch.float64, device="cuda")
+    one = torch.ones(8, dtype=torch.float64, device="cuda")
+    ints = torch.full((16,), 5, dtype=torch.int32, device="cuda")
+    torch.cuda.synchronize()
+    p = sentinel.data_ptr()
+    ctx.accel(p, p, p, one.data_ptr(), one.data_ptr(), 0, khrr.OVERWRITE)
+    ctx.phi(one.data_ptr(), p, p, one.data_ptr(), one.data_ptr(), 0, khrr.OVERWRITE)
+    ctx.integ_time(p, p, p, p, p, 0.002, 1, 0.0, p, 0)
+    mesh = khrr.Mesh.make((-1,) * 3, (0.5,) * 3, (4, 4, 4))
+    ctx.assign_particles_to_cells(p, 0, mesh, ints.data_ptr(), ints.data_ptr(), None, None, None)
+    ctx.cic_deposit(p, one.data_ptr(), 0, mesh, one.data_ptr())
+    ctx.cic_gather(p, 0, mesh, p, one.data_ptr(), p, one.data_ptr())
+    ctx.apply_cells_to_particles(p, one.data_ptr(), p, one.data_ptr(), ints.data_ptr(), 0)
+    ctx.synchronize()
+    assert bool((sentinel == 7.0).all()) and bool((one == 1.0).all()) and bool((ints == 5).all())
