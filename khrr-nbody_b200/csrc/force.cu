@@ -114,8 +114,18 @@ struct TileAcc<K, false> {
     __device__ __forceinline__ float p(int k) const { return pp[k]; }
 };
 
+// Residency floor per shape: the potential variants of the 128-thread,
+// K <= 4 shapes are held to three CTAs per SM (168 registers; they would take
+// 172 and fit two): 260 -> 249 ms for a force + potential pass at 786k
+// bodies.  The acceleration-only variants are faster left unbounded.
+template <int NT, int K, unsigned F>
+constexpr int force_min_blocks() {
+    if (kThreadsPerSm > 0) return kThreadsPerSm / NT;
+    return ((F & kPhi) && NT == 128 && K <= 4) ? 3 : 1;
+}
+
 template <int NT, int K, int JT, int STAGES, unsigned F>
-__global__ void __launch_bounds__(NT, (kThreadsPerSm > 0 ? kThreadsPerSm / NT : 1)) force_kernel(const ForceArgs a) {
+__global__ void __launch_bounds__(NT, (force_min_blocks<NT, K, F>())) force_kernel(const ForceArgs a) {
     using S = ForceShape<NT, K, JT, STAGES, F>;
     constexpr bool UNIF = S::UNIF, ACC = S::ACC, PHI = S::PHI, TMASS = S::TMASS;
     constexpr bool PACKED = F & kPacked;
