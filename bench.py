@@ -578,8 +578,8 @@ def run_khrr(args):
         "roofline": {"bound": "fp32", "kernel": "force_kernel", "achieved": achieved, "peak": peak_tflops,
                      "unit": "TFLOP/s", "frac": achieved / peak_tflops,
                      # DRAM read+write of one force launch from the ncu capture on
-                     # 131,072 bodies (2.30 MB), scaled by the bodies processed.
-                     "traffic": 2.30e6 * n / 131072,
+                     # 131,072 bodies (2.80 MB), scaled by the bodies processed.
+                     "traffic": 2.80e6 * n / 131072,
                      "flops_per_pair": FLOPS_PER_PAIR, "pairs_per_launch": pairs_timed / max(launches, 1),
                      "avg_launch_ms": avg_launch_s * 1e3,
                      "peak_basis": f"nominal FP32: {SMS} SMs x {FP32_LANES} lanes x 2 flops x {sm_max:.0f} MHz "
