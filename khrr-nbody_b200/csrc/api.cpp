@@ -76,9 +76,25 @@ int khrr_ctx::resident_ctas(const ForceVariant* v) {
     return occ * sm_count;
 }
 
-// The state's kernel: the tile-mass form where the layout allows it and the
-// shape has one, else the general form.
+// The pair kernel's partials take 16 bytes per body and slot; layouts whose
+// largest system would need more than this fall back to the one-sided kernel.
+constexpr int64_t kPairPartBudget = int64_t(32) << 30;
+
+bool khrr_ctx::pair_mode() const {
+    if (tuning.packed != 2 || !has_state) return false;
+    return pair_slots_bound(poff) * npad * 16 <= kPairPartBudget;
+}
+
+// The state's kernel: the symmetric pair kernel when the tuning asks for it
+// (packed = 2) and the layout admits it; else the tile-mass form where the
+// layout allows it and the shape has one, else the general form.
 const ForceVariant* khrr_ctx::variant(bool unif, bool acc, bool phi) const {
+    if (tuning.packed == 2) {
+        if (pair_mode()) return find_pair_variant(unif, acc, phi, block_uniform_mass);
+        if (tile_uniform_mass)
+            if (const ForceVariant* v = find_force_variant(128, 4, 128, true, unif, acc, phi, true)) return v;
+        return find_force_variant(128, 4, 128, true, unif, acc, phi, false);
+    }
     const bool packed = tuning.packed != 0;
     if (tile_uniform_mass)
         if (const ForceVariant* v =
@@ -172,6 +188,59 @@ void plan_force_items(const std::vector<int64_t>& poff, const std::vector<int64_
     }
 }
 
+int64_t pair_slots_bound(const std::vector<int64_t>& poff) {
+    int64_t nb = 1;
+    for (size_t k = 0; k + 1 < poff.size(); ++k)
+        nb = std::max(nb, (poff[k + 1] - poff[k] + kPairBlock - 1) / kPairBlock);
+    return nb;
+}
+
+// Block row b of a system with nb blocks holds the block pairs (b, J), J >= b,
+// cut into chunks of C blocks.  A body of block b receives nb_b = b + chunks(b)
+// partials: the reactions of blocks 0..b-1 (slots 0..b-1) and its own row's
+// chunk sums (slots b..).  C is the largest chunk (up to 32 blocks) that still
+// gives the persistent grid about 16 items per CTA; items run costliest first.
+void plan_pair_items(const std::vector<int64_t>& poff, const std::vector<int64_t>& cnt, int ctas, int chunk,
+                     ForcePlan& out, std::vector<unsigned short>& nsplit) {
+    out.pair_items.clear();
+    const size_t nsys = cnt.size();
+    nsplit.assign(static_cast<size_t>(poff[nsys]), 0);
+    double block_pairs = 0.0;
+    for (size_t k = 0; k < nsys; ++k) {
+        const double nb = static_cast<double>((poff[k + 1] - poff[k] + kPairBlock - 1) / kPairBlock);
+        block_pairs += nb * (nb + 1.0) / 2.0;
+    }
+    int C = chunk;
+    if (C <= 0) C = static_cast<int>(std::clamp(block_pairs / (16.0 * std::max(ctas, 1)), 1.0, 32.0));
+    out.nslots = 1;
+    for (size_t k = 0; k < nsys; ++k) {
+        const int64_t P = poff[k], np = poff[k + 1] - poff[k], real_end = poff[k] + cnt[k];
+        const int64_t nb = (np + kPairBlock - 1) / kPairBlock;
+        for (int64_t b = 0; b < nb; ++b) {
+            const int64_t ib = P + b * kPairBlock, ie = std::min(ib + kPairBlock, P + np);
+            const int64_t nch = (nb - b + C - 1) / C;
+            for (int64_t u = 0; u < nch; ++u) {
+                const int64_t Jb = b + u * C, Je = std::min(Jb + C, nb);
+                PairItem it{};
+                it.i_begin = static_cast<int>(ib);
+                it.i_end = static_cast<int>(ie);
+                it.j_begin = static_cast<int>(P + Jb * kPairBlock);
+                it.j_end = static_cast<int>(std::min(P + Je * kPairBlock, P + np));
+                it.diag_end = u == 0 ? it.i_end : it.j_begin;
+                it.slot_i = static_cast<int>(b + u);
+                it.slot_j = static_cast<int>(b);
+                it.cost = static_cast<int>((ie - ib) * (it.j_end - it.j_begin) / kPairBlock);
+                out.pair_items.push_back(it);
+            }
+            const int64_t ns = b + nch;
+            for (int64_t i = ib; i < std::min(ie, real_end); ++i) nsplit[i] = static_cast<unsigned short>(ns);
+            out.nslots = std::max<int>(out.nslots, static_cast<int>(ns));
+        }
+    }
+    std::stable_sort(out.pair_items.begin(), out.pair_items.end(),
+                     [](const PairItem& a, const PairItem& b) { return a.cost > b.cost; });
+}
+
 }  // namespace khrr
 
 khrr_status khrr_ctx::ensure_plan(bool plain) {
@@ -181,16 +250,43 @@ khrr_status khrr_ctx::ensure_plan(bool plain) {
     const ForceVariant* v = variant(uniform, true, false);
     if (!v) return fail(KHRR_ERR_INVALID_ARG, "no force kernel for the current tuning");
     const int ctas = resident_ctas(v);
-    if (p.valid && p.threads == v->threads && p.ipt == v->i_per_thread && p.jt == v->j_tile &&
+    khrr_status st;
+    if (!plain && v->pair) {
+        if (p.valid && p.pair && p.split_req == tuning.j_split && p.ctas == ctas) return KHRR_OK;
+        std::vector<unsigned short> ns;
+        plan_pair_items(poff, cnt, ctas, tuning.j_split, p, ns);
+        p.pair = true;
+        p.threads = v->threads;
+        p.ipt = v->i_per_thread;
+        p.jt = v->j_tile;
+        p.split_req = tuning.j_split;
+        p.ctas = ctas;
+        if ((st = cuda(p.d_pair_items.ensure(p.pair_items.size()), "alloc items")) != KHRR_OK) return st;
+        if ((st = cuda(cudaMemcpyAsync(p.d_pair_items.p, p.pair_items.data(), p.pair_items.size() * sizeof(PairItem),
+                                       cudaMemcpyHostToDevice, stream),
+                       "upload items")) != KHRR_OK)
+            return st;
+        if ((st = cuda(p.d_nsplit4.ensure(ns.size()), "alloc nsplit")) != KHRR_OK) return st;
+        if ((st = cuda(cudaMemcpyAsync(p.d_nsplit4.p, ns.data(), ns.size() * sizeof(unsigned short),
+                                       cudaMemcpyHostToDevice, stream),
+                       "upload nsplit")) != KHRR_OK)
+            return st;
+        if ((st = cuda(part4.ensure(static_cast<size_t>(p.nslots) * npad), "alloc partials")) != KHRR_OK) return st;
+        if ((st = cuda(cudaStreamSynchronize(stream), "plan sync")) != KHRR_OK) return st;
+        p.valid = true;
+        drop_graphs();
+        return KHRR_OK;
+    }
+    if (p.valid && !p.pair && p.threads == v->threads && p.ipt == v->i_per_thread && p.jt == v->j_tile &&
         p.split_req == tuning.j_split && p.ctas == ctas)
         return KHRR_OK;
     plan_force_items(poff, cnt, v->threads * v->i_per_thread, v->j_tile, ctas, tuning.j_split, plain, p);
+    p.pair = false;
     p.threads = v->threads;
     p.ipt = v->i_per_thread;
     p.jt = v->j_tile;
     p.split_req = tuning.j_split;
     p.ctas = ctas;
-    khrr_status st;
     if ((st = cuda(p.d_items.ensure(p.items.size()), "alloc items")) != KHRR_OK) return st;
     if ((st = cuda(cudaMemcpyAsync(p.d_items.p, p.items.data(), p.items.size() * sizeof(WorkItem),
                                    cudaMemcpyHostToDevice, stream),
@@ -271,6 +367,21 @@ khrr_status khrr_ctx::enqueue_force(bool plain, bool acc, bool phi, bool events)
                            "plain force kernel")) != KHRR_OK)
                 return st;
         }
+    } else if (p.pair) {
+        if (!v->pair) return fail(KHRR_ERR_INVALID_ARG, "no pair kernel for this output set");
+        if ((st = cuda(cudaMemsetAsync(queue.p, 0, sizeof(unsigned), stream), "queue reset")) != KHRR_OK) return st;
+        PairArgs a{};
+        a.sh = shadow();
+        a.items = p.d_pair_items.p;
+        a.n_items = static_cast<int>(p.pair_items.size());
+        a.queue = queue.p;
+        a.part = part4.p;
+        a.npad = npad;
+        a.h_uniform = h_uniform;
+        a.tile_mass = tile_mass.p;
+        a.err = errflag.p;
+        if ((st = cuda(launch_pair(v, a, std::min(a.n_items, ctas), stream), "pair force kernel")) != KHRR_OK)
+            return st;
     } else {
         if ((st = cuda(cudaMemsetAsync(queue.p, 0, sizeof(unsigned), stream), "queue reset")) != KHRR_OK) return st;
         const int e = static_cast<int>(p.items.size());
@@ -296,6 +407,8 @@ StepArgs khrr_ctx::step_args(const ForcePlan& p, double dt) {
     a.part = part.p;
     a.npad = npad;
     a.nsplit = p.d_nsplit.p;
+    a.part4 = p.pair ? part4.p : nullptr;
+    a.nsplit4 = p.pair ? p.d_nsplit4.p : nullptr;
     a.n = npad;
     a.dt = dt;
     a.field = field;
@@ -449,8 +562,8 @@ khrr_status khrr_create(int device, khrr_ctx** out) {
     c->stream = c->own;
     cudaMemset(c->queue.p, 0, sizeof(unsigned));
     cudaMemset(c->errflag.p, 0, sizeof(unsigned));
-    for (int i = 0; i < force_variant_count(); ++i) {
-        const ForceVariant* v = force_variant(i);
+    for (int i = 0; i < force_variant_count() + pair_variant_count(); ++i) {
+        const ForceVariant* v = i < force_variant_count() ? force_variant(i) : pair_variant(i - force_variant_count());
         if (cudaFuncSetAttribute(v->fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  static_cast<int>(v->smem)) != cudaSuccess) {
             khrr_destroy(c);
@@ -591,6 +704,16 @@ khrr_status khrr_upload_state(khrr_ctx* c, int64_t n, const double* pos, const d
     }
     if (tile_uniform != c->tile_uniform_mass) c->drop_graphs();
     c->tile_uniform_mass = tile_uniform;
+    // The pair kernel's block-mass form: whole 1024 blocks of one mass each.
+    bool block_uniform = tile_uniform;
+    for (int k = 0; k < nsys && block_uniform; ++k) {
+        if (c->cnt[k] % kPairBlock) block_uniform = false;
+        for (int64_t b = 0; b < c->cnt[k] && block_uniform; b += kPairBlock)
+            for (int64_t q = kPad; q < kPairBlock; q += kPad)
+                if (tm[(c->poff[k] + b + q) / kPad] != tm[(c->poff[k] + b) / kPad]) block_uniform = false;
+    }
+    if (block_uniform != c->block_uniform_mass) c->drop_graphs();
+    c->block_uniform_mass = block_uniform;
     if ((st = c->cuda(c->tile_mass.ensure(tm.size()), "alloc tile masses")) != KHRR_OK) return st;
     st = c->cuda(cudaMemcpyAsync(c->tile_mass.p, tm.data(), tm.size() * sizeof(float), cudaMemcpyHostToDevice, s),
                  "upload");
@@ -796,7 +919,13 @@ khrr_status khrr_set_tuning(khrr_ctx* c, const khrr_tuning* t) {
     if (!c || !t) return KHRR_ERR_INVALID_ARG;
     khrr_tuning n = *t;
     if (n.j_tile == 0) n.j_tile = 128;
-    if (!find_force_variant(n.threads, n.i_per_thread, n.j_tile, n.packed != 0, false, true, false))
+    if (n.packed == 2) {
+        if (n.threads != kPairThreads || n.i_per_thread != kPairBodies || n.j_tile != kPairTile)
+            return c->fail(KHRR_ERR_INVALID_ARG, "the pair kernel (packed=2) has threads=%d i_per_thread=%d j_tile=%d",
+                           kPairThreads, kPairBodies, kPairTile);
+    } else if (n.packed != 0 && n.packed != 1) {
+        return c->fail(KHRR_ERR_INVALID_ARG, "packed must be 0, 1 or 2");
+    } else if (!find_force_variant(n.threads, n.i_per_thread, n.j_tile, n.packed != 0, false, true, false))
         return c->fail(KHRR_ERR_INVALID_ARG,
                        "no compiled force kernel with threads=%d i_per_thread=%d j_tile=%d packed=%d", n.threads,
                        n.i_per_thread, n.j_tile, n.packed);

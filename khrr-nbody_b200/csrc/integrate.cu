@@ -107,6 +107,17 @@ __global__ void predictor_kernel(const StepArgs a) {
 __device__ __forceinline__ void sum_partials(const StepArgs& a, int64_t i, d3& s, double& sp) {
     s = d3{0.0, 0.0, 0.0};
     sp = 0.0;
+    if (a.part4) {
+        const int ns = a.nsplit4[i];
+        for (int k = 0; k < ns; ++k) {
+            const float4 p = a.part4[k * a.npad + i];
+            s.x += static_cast<double>(p.x);
+            s.y += static_cast<double>(p.y);
+            s.z += static_cast<double>(p.z);
+            sp += static_cast<double>(p.w);
+        }
+        return;
+    }
     const int ns = a.nsplit[i];
     for (int k = 0; k < ns; ++k) {
         const double4 p = a.part[k * a.npad + i];

@@ -27,11 +27,15 @@ khrr_status prepare_kernel_pass(khrr_ctx* c, const double* pos_i, const double* 
                                 bool phi, const ForceVariant** vout) {
     if (n < 1 || n > (int64_t(1) << 30)) return c->fail(KHRR_ERR_INVALID_ARG, "n out of range");
     if (!pos_i || !pos_j || !mass_j || !eps2_j) return c->fail(KHRR_ERR_INVALID_ARG, "null device pointer");
+    // These entry points run the one-sided kernel (i and j may be different
+    // sets); the pair tuning maps to its packed 128 x 4 shape.
+    const bool pair_tuning = c->tuning.packed == 2;
+    const int threads = pair_tuning ? 128 : c->tuning.threads;
+    const int ipt = pair_tuning ? 4 : c->tuning.i_per_thread;
+    const int jt = pair_tuning ? 128 : c->tuning.j_tile;
     const bool packed = c->tuning.packed != 0;
-    const ForceVariant* v =
-        find_force_variant(c->tuning.threads, c->tuning.i_per_thread, c->tuning.j_tile, packed, false, acc, phi);
-    const ForceVariant* vplan =
-        find_force_variant(c->tuning.threads, c->tuning.i_per_thread, c->tuning.j_tile, packed, false, true, false);
+    const ForceVariant* v = find_force_variant(threads, ipt, jt, packed, false, acc, phi);
+    const ForceVariant* vplan = find_force_variant(threads, ipt, jt, packed, false, true, false);
     if (!v || !vplan) return c->fail(KHRR_ERR_INVALID_ARG, "no force kernel for the current tuning");
     const int64_t npad = round_up(n, kPad);
     khrr_status st;
@@ -176,9 +180,9 @@ khrr_status khrr_autotune(khrr_ctx* c, const char* cache_path) {
     const khrr_tuning keep = c->tuning;
     khrr_tuning best = keep;
     double best_ms = 1e300;
-    // {threads, i bodies per thread, packed}
-    const int shapes[][3] = {{128, 2, 1}, {128, 4, 1}, {256, 2, 1}, {256, 4, 1},
-                             {128, 4, 0}, {128, 8, 0}, {256, 4, 0}, {256, 8, 0}};
+    // {threads, i bodies per thread, packed}; packed 2 is the symmetric pair kernel
+    const int shapes[][3] = {{128, 8, 2}, {128, 2, 1}, {128, 4, 1}, {256, 2, 1}, {256, 4, 1},
+                             {128, 4, 0},  {128, 8, 0}, {256, 4, 0}, {256, 8, 0}};
     for (const auto& sh : shapes) {
         khrr_tuning t{sh[0], sh[1], 128, 0, sh[2]};
         if (khrr_set_tuning(c, &t) != KHRR_OK) continue;

@@ -57,13 +57,54 @@ struct ForceArgs {
     unsigned* err;           // device error flag word
 };
 
-// One compiled force-kernel instance.
+// One compiled force-kernel instance.  pair: the symmetric kernel (pair.cu),
+// launched with PairArgs; its tile_mass means one mass per kPairBlock block.
 struct ForceVariant {
     int threads, i_per_thread, j_tile, stages;
     bool packed, uniform_eps, acc, phi, tile_mass;
     const void* fn;
     size_t smem;
+    bool pair = false;
 };
+
+// ---- the symmetric pair kernel (pair.cu) --------------------------------------
+constexpr int kPairThreads = 128;                          // threads per CTA
+constexpr int kPairBodies = 8;                             // i bodies per thread
+constexpr int kPairBlock = kPairThreads * kPairBodies;     // bodies per block (1024)
+constexpr int kPairTile = 128;                             // j bodies per shared-memory tile
+
+// One unit of symmetric work: the i block [i_begin, i_end) against the j
+// bodies [j_begin, j_end) of later blocks of the same system (the first
+// chunk of a row starts with the i block itself, [j_begin, diag_end), which
+// is evaluated one-sided).  Padded device indices; j bounds are multiples of
+// kPairTile.
+struct PairItem {
+    int i_begin;
+    int i_end;
+    int j_begin;
+    int j_end;
+    int diag_end;  // == j_begin when the chunk holds no tile of the i block
+    int slot_i;    // slot of the i block's sums over this chunk
+    int slot_j;    // slot of the reactions on the chunk's bodies (the i block's index)
+    int cost;      // planner's estimate (i bodies x j bodies / 1024)
+};
+
+struct PairArgs {
+    Shadow sh;               // the bodies (i and j are the same set)
+    const PairItem* items;
+    int n_items;
+    unsigned* queue;         // next-item counter (zeroed before each launch)
+    float4* part;            // partial sums [slot][npad]: ax, ay, az, sum m/r
+    long long npad;          // slot stride
+    float h_uniform;         // 0.5 * eps2 when every body shares it
+    const float* tile_mass;  // mass per 128-body tile (block-mass kernels)
+    unsigned* err;           // device error flag word
+};
+
+int pair_variant_count();
+const ForceVariant* pair_variant(int idx);
+const ForceVariant* find_pair_variant(bool unif, bool acc, bool phi, bool block_mass);
+cudaError_t launch_pair(const ForceVariant* v, const PairArgs& a, int grid, cudaStream_t s);
 
 // Derived constants of the analytic halo/bulge field (dev_fex operands).
 struct FieldConsts {
@@ -115,6 +156,8 @@ struct StepArgs {
     const double4* part;  // force partials [slot][npad]
     long long npad;
     const unsigned char* nsplit;  // partial slots per body
+    const float4* part4;          // the pair kernel's FP32 partials [slot][npad] (replaces part when set)
+    const unsigned short* nsplit4;  // their slot count per body
     int64_t n;            // padded count
     double dt;
     FieldConsts field;

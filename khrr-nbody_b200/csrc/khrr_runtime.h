@@ -63,6 +63,11 @@ struct ForcePlan {
     int nslots = 1;
     DevBuf<WorkItem> d_items;
     DevBuf<unsigned char> d_nsplit;
+    // The symmetric pair kernel's queue (pair plans only) and slot counts.
+    bool pair = false;
+    std::vector<PairItem> pair_items;
+    DevBuf<PairItem> d_pair_items;
+    DevBuf<unsigned short> d_nsplit4;
     ForcePlan() = default;
     ForcePlan(const ForcePlan&) = delete;
     ForcePlan& operator=(const ForcePlan&) = delete;
@@ -70,6 +75,14 @@ struct ForcePlan {
 
 void plan_force_items(const std::vector<int64_t>& poff, const std::vector<int64_t>& cnt, int itile,
                       int jt, int ctas, int forced_split, bool plain, ForcePlan& out);
+// The symmetric pair kernel's items: block rows cut into chunks of
+// `chunk` blocks (0 = chosen from the CTA count); nsplit gets the slot count
+// of every padded body (0 for ghosts).
+void plan_pair_items(const std::vector<int64_t>& poff, const std::vector<int64_t>& cnt, int ctas, int chunk,
+                     ForcePlan& out, std::vector<unsigned short>& nsplit);
+// Upper bound of the pair kernel's slot count for a layout (the largest
+// system's block count).
+int64_t pair_slots_bound(const std::vector<int64_t>& poff);
 
 struct StepGraph {
     cudaGraph_t graph = nullptr;
@@ -117,12 +130,14 @@ struct khrr_ctx {
     khrr::DevBuf<double> pos, vel, acc, post, velt, acct, mass, eps2, phi;
     khrr::DevBuf<float> shadow_buf;  // SoA FP32 shadow, 5 x npad
     khrr::DevBuf<double4> part;
+    khrr::DevBuf<float4> part4;         // the pair kernel's FP32 partials
     khrr::DevBuf<unsigned> queue, errflag;
     khrr::DevBuf<double> cons_blocks, scratch;
     bool uniform = false;
     float h_uniform = 0.0f;
     bool tile_uniform_mass = false;     // every 128-body tile of the layout has one mass
     khrr::DevBuf<float> tile_mass;      // that mass per tile (FP32)
+    bool block_uniform_mass = false;    // every system a whole number of 1024 blocks, one mass each
     khrr::FieldConsts field{};
     khrr_tuning tuning{128, 4, 128, 0, 1};
     khrr::ForcePlan plan_batched, plan_plain;
@@ -169,6 +184,7 @@ struct khrr_ctx {
     khrr_status check_device_flag();
     int resident_ctas(const khrr::ForceVariant* v);
     const khrr::ForceVariant* variant(bool unif, bool acc, bool phi) const;
+    bool pair_mode() const;  // the tuning asks for the pair kernel and the layout admits it
     khrr_status ensure_plan(bool plain);
     void drop_graphs();
     khrr::ForceArgs force_args(const khrr::ForcePlan& p, int item_begin, int item_end);
