@@ -21,24 +21,26 @@
 // B + (chunks of row B) slots in FP64.  Every slot is written exactly once per
 // pass: no atomics, and the result is bitwise reproducible.
 //
-// The reaction sum across a warp.  In a 32-body sub-chunk of the tile, lane l
-// evaluates j = (l + s) mod 32 at step s against its 8 i bodies, adds the
-// result to the running reaction it holds for that j and hands the reaction
-// to lane l - 1 (one shuffle per component); after 32 steps lane l holds the
-// reaction of j = l summed over the warp's 256 i bodies.  The four warps' sums
-// meet in shared memory (double-buffered by tile parity) and one thread per j
-// body adds them and writes the partial.
+// The reaction sum across a warp.  The tile's 128 j bodies form four 32-body
+// sub-chunks, taken two at a time.  At step s (0..31) lane l evaluates body
+// r = (l + s) mod 32 of both sub-chunks against its 8 i bodies, adds the
+// results to the pair of running reactions it holds for those two bodies and
+// hands the pair to lane l - 1 (shuffles); after 32 steps lane l holds the
+// reactions of the bodies r = l summed over the warp's 256 i bodies.  The four
+// warps' sums meet in shared memory (double-buffered by tile parity) and one
+// thread per j body adds them and writes the partial.
 //
-// Inner loop: packed f32x2 instructions over pairs of i bodies (k, k + 1)
-// against one j: d (3 add), r^2 (3 fma), two MUFU.RSQ, r^-3 (2 mul), i side
-// (3 fma), j side (3 fma): 14 packed instructions per two pair evaluations,
-// that is 7 FP32 operations per interaction against 11 for the one-sided
-// kernel.  Tile-uniform masses (every 1024 block one mass) are factored out of
-// both sums; otherwise m_j and m_i enter per pair (2 more multiplies).
+// Inner loop: packed f32x2 instructions over the two j bodies of a step
+// against one i body (its coordinates duplicated in both lanes once per
+// item): d (3 add), r^2 (3 fma), two MUFU.RSQ, r^-3 (2 mul), i side (3 fma),
+// j side (3 fma) = 14 FP32 operations per two pair evaluations, 7 per
+// interaction against 11 for the one-sided kernel.  When every 1024 block has
+// one mass (and no ghosts) the masses are factored out of both sums;
+// otherwise m_j and m_i enter per pair (2 more multiplies).
 //
-// Accuracy: i-side tile partials (128 terms) fold into compensated (hi + lo)
-// running sums; a reaction partial is a sum of 1024 terms in three levels
-// (8 i bodies, 32 lanes, 4 warps).
+// Accuracy: the i-side tile partials (two 64-term halves) fold into
+// compensated (hi + lo) running sums kept in shared memory; a reaction partial
+// is a sum of 1024 terms in three levels (8 i bodies, 32 lanes, 4 warps).
 #include <cstdint>
 
 #include "async_copy.cuh"
@@ -63,16 +65,26 @@ __device__ __forceinline__ void two_sum_into(float& hi, float& lo, float p) {
 
 __device__ __forceinline__ float2 f2(float a, float b) { return make_float2(a, b); }
 
+__device__ __forceinline__ float2 shfl2(float2 v, int src) {
+    return f2(__shfl_sync(0xffffffffu, v.x, src), __shfl_sync(0xffffffffu, v.y, src));
+}
+
 constexpr int kBarBytes = 128;
-constexpr int NT = kPairThreads;   // threads per CTA
-constexpr int K = kPairBodies;     // i bodies per thread
-constexpr int KP = K / 2;          // packed i pairs per thread
-constexpr int JT = kPairTile;      // j bodies per tile
+constexpr int NT = kPairThreads;  // threads per CTA
+constexpr int K = kPairBodies;    // i bodies per thread
+constexpr int JT = kPairTile;     // j bodies per tile
 constexpr int STAGES = 3;
-constexpr int W = NT / 32;         // warps
+constexpr int W = NT / 32;        // warps
 static_assert(NT * K == kPairBlock, "block = threads x bodies per thread");
 static_assert(JT == NT, "one thread per j body writes the reaction partials");
-static_assert(JT % 32 == 0 && JT == kPad, "tiles are whole 32-body sub-chunks and padding units");
+static_assert(JT % 64 == 0 && JT == kPad, "tiles are whole sub-chunk pairs and padding units");
+
+// Unroll of the 32-step loop (2 measured best at 786k bodies: 151.2 ms per
+// pass against 152.2 ms for 1 and 153.4 ms for 4).
+#ifndef KHRR_PAIR_UNROLL
+#define KHRR_PAIR_UNROLL 2
+#endif
+constexpr int kSUnroll = KHRR_PAIR_UNROLL;
 
 constexpr unsigned kUnif = 1;   // every body has the same softening: no h array
 constexpr unsigned kAcc = 2;    // accumulate accelerations
@@ -86,19 +98,21 @@ struct PairShape {
     static constexpr int NCOMP = 3 + (BMASS ? 0 : 1) + (UNIF ? 0 : 1);  // x, y, z, [m], [h]
     static constexpr int kOffM = 3, kOffH = BMASS ? 3 : 4;
     static constexpr unsigned kTileBytes = NCOMP * JT * 4u;
-    static constexpr int kJwFloats = W * NC * JT;  // one parity of the reaction buffer
-    static constexpr size_t kSmem = kBarBytes + (size_t)STAGES * kTileBytes + 2 * (size_t)kJwFloats * 4;
+    static constexpr int kJwFloats = W * NC * JT;       // one parity of the reaction buffer
+    static constexpr int kRunFloats = 2 * NC * K * NT;  // (hi, lo) running sums
+    static constexpr size_t kSmem =
+        kBarBytes + (size_t)STAGES * kTileBytes + (2 * (size_t)kJwFloats + kRunFloats) * 4;
 };
 
-// One tile: the lane's 8 i bodies against the tile's 128 j bodies in four
-// 32-body sub-chunks, each visited in the rotated order above.  SYM adds the
-// reactions (written to jw[warp][comp][j]); without it the tile is the i
-// block itself and only the i side is summed.
+// One tile against the lane's K i bodies.  SYM adds the reactions (written
+// to jw[warp][comp][j]); without it the tile is the i block itself and only
+// the i side is summed.  ai[c][k] keeps the i-side sums of the two lanes (the
+// two sub-chunks) apart.
 template <unsigned F, bool SYM>
 __device__ __forceinline__ void pair_tile(const float* __restrict__ tile, float* __restrict__ jw,
-                                          const float2 (&nx)[KP], const float2 (&ny)[KP], const float2 (&nz)[KP],
-                                          const float2 (&hi)[KP], const float2 (&mi)[KP], float2 e2,
-                                          float2 (&ai)[PairShape<F>::NC][KP], int lane, int warp) {
+                                          const float2 (&nx)[K], const float2 (&ny)[K], const float2 (&nz)[K],
+                                          const float2 (&hi)[K], const float2 (&mi)[K], float2 e2,
+                                          float2 (&ai)[PairShape<F>::NC][K], int lane, int warp) {
     using S = PairShape<F>;
     constexpr bool UNIF = S::UNIF, ACC = S::ACC, PHI = S::PHI, BMASS = S::BMASS;
     constexpr int NC = S::NC, CP = NC - 1;  // CP: the potential's component
@@ -107,25 +121,22 @@ __device__ __forceinline__ void pair_tile(const float* __restrict__ tile, float*
     const float* Z = tile + 2 * JT;
     const float* M = tile + S::kOffM * JT;
     const float* H = tile + S::kOffH * JT;
+    const int src = (lane + 1) & 31;
 #pragma unroll 1
-    for (int c = 0; c < JT / 32; ++c) {
-        const int base = c * 32;
-        float rx = 0.f, ry = 0.f, rz = 0.f, rp = 0.f;  // reaction held by this lane
-#pragma unroll 2
+    for (int c0 = 0; c0 < JT / 32; c0 += 2) {
+        float2 rx = f2(0.f, 0.f), ry = rx, rz = rx, rp = rx;  // reactions held by this lane
+#pragma unroll kSUnroll
         for (int s = 0; s < 32; ++s) {
-            const int jj = base + ((lane + s) & 31);
-            const float xj = X[jj], yj = Y[jj], zj = Z[jj];
-            const float mj = BMASS ? 1.f : M[jj];
-            const float hj = UNIF ? 0.f : H[jj];
-            const float2 X2 = f2(xj, xj), Y2 = f2(yj, yj), Z2 = f2(zj, zj);
-            const float2 M2 = f2(mj, mj), H2 = f2(hj, hj);
-            float2 tx = f2(rx, 0.f), ty = f2(ry, 0.f), tz = f2(rz, 0.f), tp = f2(rp, 0.f);
+            const int ja = c0 * 32 + ((lane + s) & 31), jb = ja + 32;
+            const float2 X2 = f2(X[ja], X[jb]), Y2 = f2(Y[ja], Y[jb]), Z2 = f2(Z[ja], Z[jb]);
+            const float2 M2 = BMASS ? f2(1.f, 1.f) : f2(M[ja], M[jb]);
+            const float2 H2 = UNIF ? f2(0.f, 0.f) : f2(H[ja], H[jb]);
 #pragma unroll
-            for (int p = 0; p < KP; ++p) {
-                const float2 dx = __fadd2_rn(X2, nx[p]);
-                const float2 dy = __fadd2_rn(Y2, ny[p]);
-                const float2 dz = __fadd2_rn(Z2, nz[p]);
-                float2 r2 = UNIF ? e2 : __fadd2_rn(H2, hi[p]);
+            for (int k = 0; k < K; ++k) {
+                const float2 dx = __fadd2_rn(X2, nx[k]);
+                const float2 dy = __fadd2_rn(Y2, ny[k]);
+                const float2 dz = __fadd2_rn(Z2, nz[k]);
+                float2 r2 = UNIF ? e2 : __fadd2_rn(H2, hi[k]);
                 r2 = __ffma2_rn(dx, dx, r2);
                 r2 = __ffma2_rn(dy, dy, r2);
                 r2 = __ffma2_rn(dz, dz, r2);
@@ -133,44 +144,53 @@ __device__ __forceinline__ void pair_tile(const float* __restrict__ tile, float*
                 if (ACC) {
                     const float2 i3 = __fmul2_rn(inv, __fmul2_rn(inv, inv));
                     const float2 fi = BMASS ? i3 : __fmul2_rn(M2, i3);
-                    ai[0][p] = __ffma2_rn(dx, fi, ai[0][p]);
-                    ai[1][p] = __ffma2_rn(dy, fi, ai[1][p]);
-                    ai[2][p] = __ffma2_rn(dz, fi, ai[2][p]);
+                    ai[0][k] = __ffma2_rn(dx, fi, ai[0][k]);
+                    ai[1][k] = __ffma2_rn(dy, fi, ai[1][k]);
+                    ai[2][k] = __ffma2_rn(dz, fi, ai[2][k]);
                     if (SYM) {
-                        const float2 fj = BMASS ? i3 : __fmul2_rn(mi[p], i3);
-                        tx = __ffma2_rn(dx, fj, tx);
-                        ty = __ffma2_rn(dy, fj, ty);
-                        tz = __ffma2_rn(dz, fj, tz);
+                        const float2 fj = BMASS ? i3 : __fmul2_rn(mi[k], i3);
+                        rx = __ffma2_rn(dx, fj, rx);
+                        ry = __ffma2_rn(dy, fj, ry);
+                        rz = __ffma2_rn(dz, fj, rz);
                     }
                 }
                 if (PHI) {
-                    ai[CP][p] = BMASS ? __fadd2_rn(ai[CP][p], inv) : __ffma2_rn(M2, inv, ai[CP][p]);
-                    if (SYM) tp = BMASS ? __fadd2_rn(tp, inv) : __ffma2_rn(mi[p], inv, tp);
+                    ai[CP][k] = BMASS ? __fadd2_rn(ai[CP][k], inv) : __ffma2_rn(M2, inv, ai[CP][k]);
+                    if (SYM) rp = BMASS ? __fadd2_rn(rp, inv) : __ffma2_rn(mi[k], inv, rp);
                 }
             }
             if (SYM) {
-                // Hand the reaction of j to the lane that evaluates it next.
-                const int src = (lane + 1) & 31;
+                // Hand the reactions to the lane that evaluates their bodies next.
                 if (ACC) {
-                    rx = __shfl_sync(0xffffffffu, tx.x + tx.y, src);
-                    ry = __shfl_sync(0xffffffffu, ty.x + ty.y, src);
-                    rz = __shfl_sync(0xffffffffu, tz.x + tz.y, src);
+                    rx = shfl2(rx, src);
+                    ry = shfl2(ry, src);
+                    rz = shfl2(rz, src);
                 }
-                if (PHI) rp = __shfl_sync(0xffffffffu, tp.x + tp.y, src);
+                if (PHI) rp = shfl2(rp, src);
             }
         }
         if (SYM) {
-            float* w = jw + warp * NC * JT + base + lane;  // after 32 steps: the reaction of j = base + lane
+            // After 32 steps: the reactions of j = c0 * 32 + lane and of j + 32.
+            float* w = jw + warp * NC * JT + c0 * 32 + lane;
             if (ACC) {
-                w[0] = rx;
-                w[JT] = ry;
-                w[2 * JT] = rz;
+                w[0] = rx.x;
+                w[32] = rx.y;
+                w[JT] = ry.x;
+                w[JT + 32] = ry.y;
+                w[2 * JT] = rz.x;
+                w[2 * JT + 32] = rz.y;
             }
-            if (PHI) w[CP * JT] = rp;
+            if (PHI) {
+                w[CP * JT] = rp.x;
+                w[CP * JT + 32] = rp.y;
+            }
         }
     }
 }
 
+// Resident CTAs per SM the register allocation aims at: three (168
+// registers) for accelerations; the potential variants carry one more
+// accumulator per i body and per reaction and run at two.
 template <unsigned F>
 __global__ void __launch_bounds__(NT, ((F & kPhi) ? 2 : 3)) pair_kernel(const PairArgs a) {
     using S = PairShape<F>;
@@ -182,6 +202,7 @@ __global__ void __launch_bounds__(NT, ((F & kPhi) ? 2 : 3)) pair_kernel(const Pa
     uint64_t* full = reinterpret_cast<uint64_t*>(smem_raw);
     float* ring = reinterpret_cast<float*>(smem_raw + kBarBytes);  // [STAGES][NCOMP][JT]
     float* jwbuf = ring + STAGES * NCOMP * JT;                      // [2][W][NC][JT]
+    float* runs = jwbuf + 2 * S::kJwFloats;                         // [2][NC][K][NT]: hi, lo
     __shared__ int s_item;
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -201,6 +222,9 @@ __global__ void __launch_bounds__(NT, ((F & kPhi) ? 2 : 3)) pair_kernel(const Pa
         if (!BMASS) bulk_copy_g2s(dst + S::kOffM * JT, a.sh.m + jstart, JT * 4u, &full[stage]);
         if (!UNIF) bulk_copy_g2s(dst + S::kOffH * JT, a.sh.h + jstart, JT * 4u, &full[stage]);
     };
+    // The thread's compensated running sums, component c of i body k.
+    auto RH = [&](int c, int k) -> float& { return runs[(c * K + k) * NT + tid]; };
+    auto RL = [&](int c, int k) -> float& { return runs[((NC + c) * K + k) * NT + tid]; };
 
     const float2 e2 = f2(a.h_uniform + a.h_uniform, a.h_uniform + a.h_uniform);
     unsigned consumed = 0;  // tiles this CTA has consumed, over all its items
@@ -216,39 +240,25 @@ __global__ void __launch_bounds__(NT, ((F & kPhi) ? 2 : 3)) pair_kernel(const Pa
             for (int s = 0; s < STAGES && s < ntiles; ++s) issue((consumed + s) % STAGES, w.j_begin + s * JT);
         }
 
-        // i bodies k = 2p, 2p + 1 of this thread: negated coordinates, the eps
-        // term and the mass (0 past the block's end, so those lanes add no
-        // reaction).
-        float2 nx[KP], ny[KP], nz[KP], hi[KP], mi[KP];
+        // The thread's i bodies k (index i_begin + k NT + tid), each duplicated
+        // in both lanes: negated coordinates, the eps term and the mass (0 past
+        // the block's end, so those lanes add no reaction).
+        float2 nx[K], ny[K], nz[K], hi[K], mi[K];
 #pragma unroll
-        for (int p = 0; p < KP; ++p) {
-            float v[2][5];
+        for (int k = 0; k < K; ++k) {
+            const int i = w.i_begin + k * NT + tid;
+            const bool in = i < w.i_end;
+            const float x = in ? -a.sh.x[i] : 0.f, y = in ? -a.sh.y[i] : 0.f, z = in ? -a.sh.z[i] : 0.f;
+            const float h = UNIF ? 0.f : (in ? a.sh.h[i] : 1.f);
+            const float m = BMASS ? 1.f : (in ? a.sh.m[i] : 0.f);
+            nx[k] = f2(x, x);
+            ny[k] = f2(y, y);
+            nz[k] = f2(z, z);
+            hi[k] = f2(h, h);
+            mi[k] = f2(m, m);
 #pragma unroll
-            for (int h = 0; h < 2; ++h) {
-                const int i = w.i_begin + (2 * p + h) * NT + tid;
-                if (i < w.i_end) {
-                    v[h][0] = -a.sh.x[i];
-                    v[h][1] = -a.sh.y[i];
-                    v[h][2] = -a.sh.z[i];
-                    v[h][3] = UNIF ? 0.f : a.sh.h[i];
-                    v[h][4] = BMASS ? 1.f : a.sh.m[i];
-                } else {
-                    v[h][0] = v[h][1] = v[h][2] = 0.f;
-                    v[h][3] = 1.f;
-                    v[h][4] = 0.f;
-                }
-            }
-            nx[p] = f2(v[0][0], v[1][0]);
-            ny[p] = f2(v[0][1], v[1][1]);
-            nz[p] = f2(v[0][2], v[1][2]);
-            hi[p] = f2(v[0][3], v[1][3]);
-            mi[p] = f2(v[0][4], v[1][4]);
+            for (int c = 0; c < NC; ++c) RH(c, k) = RL(c, k) = 0.f;
         }
-        float rh[NC][K], rl[NC][K];  // compensated running i-side sums
-#pragma unroll
-        for (int c = 0; c < NC; ++c)
-#pragma unroll
-            for (int k = 0; k < K; ++k) rh[c][k] = rl[c][k] = 0.f;
         const float mI = BMASS ? a.tile_mass[w.i_begin / JT] : 1.f;
 
         for (int t = 0; t < ntiles; ++t) {
@@ -260,11 +270,11 @@ __global__ void __launch_bounds__(NT, ((F & kPhi) ? 2 : 3)) pair_kernel(const Pa
             const float mt = BMASS ? a.tile_mass[jt0 / JT] : 1.f;
             const bool ok = mbar_wait_bounded(&full[stage], (q / STAGES) & 1u);
 
-            float2 ai[NC][KP];
+            float2 ai[NC][K];
 #pragma unroll
             for (int c = 0; c < NC; ++c)
 #pragma unroll
-                for (int p = 0; p < KP; ++p) ai[c][p] = f2(0.f, 0.f);
+                for (int k = 0; k < K; ++k) ai[c][k] = f2(0.f, 0.f);
             if (ok) {
                 const float* tile = ring + stage * NCOMP * JT;
                 if (sym) pair_tile<F, true>(tile, jw, nx, ny, nz, hi, mi, e2, ai, lane, warp);
@@ -275,9 +285,9 @@ __global__ void __launch_bounds__(NT, ((F & kPhi) ? 2 : 3)) pair_kernel(const Pa
 #pragma unroll
             for (int c = 0; c < NC; ++c)
 #pragma unroll
-                for (int p = 0; p < KP; ++p) {
-                    two_sum_into(rh[c][2 * p], rl[c][2 * p], BMASS ? mt * ai[c][p].x : ai[c][p].x);
-                    two_sum_into(rh[c][2 * p + 1], rl[c][2 * p + 1], BMASS ? mt * ai[c][p].y : ai[c][p].y);
+                for (int k = 0; k < K; ++k) {
+                    const float v = ai[c][k].x + ai[c][k].y;
+                    two_sum_into(RH(c, k), RL(c, k), BMASS ? mt * v : v);
                 }
             // Every thread is done with this stage and its reaction buffer
             // (and all waits ended).
@@ -325,11 +335,11 @@ __global__ void __launch_bounds__(NT, ((F & kPhi) ? 2 : 3)) pair_kernel(const Pa
             if (i < w.i_end) {
                 float4 o = make_float4(0.f, 0.f, 0.f, 0.f);
                 if (ACC) {
-                    o.x = rh[0][k] + rl[0][k];
-                    o.y = rh[1][k] + rl[1][k];
-                    o.z = rh[2][k] + rl[2][k];
+                    o.x = RH(0, k) + RL(0, k);
+                    o.y = RH(1, k) + RL(1, k);
+                    o.z = RH(2, k) + RL(2, k);
                 }
-                if (PHI) o.w = rh[CP][k] + rl[CP][k];
+                if (PHI) o.w = RH(CP, k) + RL(CP, k);
                 out[i] = o;
             }
         }

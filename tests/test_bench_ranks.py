@@ -58,3 +58,15 @@ def test_reference_arm_is_rank_zero_only(monkeypatch):
     monkeypatch.setenv("WORLD_SIZE", "2")
     monkeypatch.setattr(sys, "argv", ["bench.py", "--impl", "reference", "--gpus", "2"])
     assert bench.run_reference(bench.parse()) == 0   # no work, no output on rank 1
+
+
+def test_force_flops_counts_each_kernel_form():
+    """Executed FP32 flops per launch: 17 per ordered pair one-sided, 23 per
+    unordered pair of different 1024-blocks for the pair kernel."""
+    import bench
+    assert bench.force_flops(1000, False) == 17.0 * 1000 * 1000
+    own = 2.0 * 1024 * 1024
+    assert bench.force_flops(2048, True) == 23.0 * (2048.0 ** 2 - own) / 2 + 17.0 * own
+    own = 1024.0 ** 2 + 476.0 ** 2
+    assert bench.force_flops(1500, True) == 23.0 * (1500.0 ** 2 - own) / 2 + 17.0 * own
+    assert bench.force_flops(1024, True) == bench.force_flops(1024, False)
