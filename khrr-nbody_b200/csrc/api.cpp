@@ -76,10 +76,6 @@ int khrr_ctx::resident_ctas(const ForceVariant* v) {
     return occ * sm_count;
 }
 
-// The pair kernel's partials take 16 bytes per body and slot; layouts whose
-// largest system would need more than this fall back to the one-sided kernel.
-constexpr int64_t kPairPartBudget = int64_t(32) << 30;
-
 bool khrr_ctx::pair_mode() const {
     if (tuning.packed != 2 || !has_state) return false;
     return pair_slots_bound(poff) * npad * 16 <= kPairPartBudget;

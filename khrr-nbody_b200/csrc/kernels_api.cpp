@@ -20,15 +20,62 @@ namespace {
 
 int64_t round_up(int64_t v, int64_t m) { return (v + m - 1) / m * m; }
 
+// The pair kernel's plan, slot counts and partials for one system of n
+// bodies (the same set as i and j).
+khrr_status prepare_pair_pass(khrr_ctx* c, int64_t n, int64_t npad, bool acc, bool phi, const ForceVariant** vout) {
+    const ForceVariant* v = find_pair_variant(false, acc, phi, false);
+    const ForceVariant* vplan = find_pair_variant(false, true, false, false);
+    if (!v || !vplan) return c->fail(KHRR_ERR_INVALID_ARG, "no pair kernel for this output set");
+    ForcePlan& p = c->kplan;
+    const int ctas = c->resident_ctas(vplan);
+    khrr_status st;
+    if (!p.valid || !p.pair || c->kplan_n != n || p.split_req != c->tuning.j_split || p.ctas != ctas) {
+        std::vector<int64_t> poff{0, npad}, cnt{n};
+        std::vector<unsigned short> ns;
+        plan_pair_items(poff, cnt, ctas, c->tuning.j_split, p, ns);
+        p.pair = true;
+        p.threads = v->threads;
+        p.ipt = v->i_per_thread;
+        p.jt = v->j_tile;
+        p.split_req = c->tuning.j_split;
+        p.ctas = ctas;
+        if ((st = c->cuda(p.d_pair_items.ensure(p.pair_items.size()), "alloc")) != KHRR_OK) return st;
+        if ((st = c->cuda(cudaMemcpy(p.d_pair_items.p, p.pair_items.data(), p.pair_items.size() * sizeof(PairItem),
+                                     cudaMemcpyHostToDevice),
+                          "upload items")) != KHRR_OK)
+            return st;
+        if ((st = c->cuda(p.d_nsplit4.ensure(ns.size()), "alloc")) != KHRR_OK) return st;
+        if ((st = c->cuda(cudaMemcpy(p.d_nsplit4.p, ns.data(), ns.size() * sizeof(unsigned short),
+                                     cudaMemcpyHostToDevice),
+                          "upload nsplit")) != KHRR_OK)
+            return st;
+        p.valid = true;
+        c->kplan_n = n;
+    }
+    if ((st = c->cuda(c->kpart4.ensure(static_cast<size_t>(p.nslots) * npad), "alloc partials")) != KHRR_OK)
+        return st;
+    *vout = v;
+    return KHRR_OK;
+}
+
 // Shadow + plan + partials for a one-system pass over n bodies given by
-// device pointers; returns the variant to launch.
+// device pointers; returns the variant to launch (the pair kernel when the
+// tuning asks for it and i and j are the same set).
 khrr_status prepare_kernel_pass(khrr_ctx* c, const double* pos_i, const double* pos_j,
                                 const double* mass_j, const double* eps2_j, int64_t n, bool acc,
                                 bool phi, const ForceVariant** vout) {
     if (n < 1 || n > (int64_t(1) << 30)) return c->fail(KHRR_ERR_INVALID_ARG, "n out of range");
     if (!pos_i || !pos_j || !mass_j || !eps2_j) return c->fail(KHRR_ERR_INVALID_ARG, "null device pointer");
-    // These entry points run the one-sided kernel (i and j may be different
-    // sets); the pair tuning maps to its packed 128 x 4 shape.
+    const int64_t npad = round_up(n, kPad);
+    khrr_status st;
+    if (c->tuning.packed == 2 && pos_i == pos_j &&
+        pair_slots_bound({0, npad}) * npad * 16 <= kPairPartBudget) {
+        if ((st = c->cuda(c->kshadow.ensure(5 * static_cast<size_t>(npad)), "alloc")) != KHRR_OK) return st;
+        if ((st = prepare_pair_pass(c, n, npad, acc, phi, vout)) != KHRR_OK) return st;
+        return c->cuda(launch_pack(pos_j, mass_j, eps2_j, n, npad, shadow_at(c->kshadow.p, npad), c->stream), "pack");
+    }
+    // The one-sided kernel (i and j may be different sets); the pair tuning
+    // maps to its packed 128 x 4 shape.
     const bool pair_tuning = c->tuning.packed == 2;
     const int threads = pair_tuning ? 128 : c->tuning.threads;
     const int ipt = pair_tuning ? 4 : c->tuning.i_per_thread;
@@ -37,15 +84,14 @@ khrr_status prepare_kernel_pass(khrr_ctx* c, const double* pos_i, const double* 
     const ForceVariant* v = find_force_variant(threads, ipt, jt, packed, false, acc, phi);
     const ForceVariant* vplan = find_force_variant(threads, ipt, jt, packed, false, true, false);
     if (!v || !vplan) return c->fail(KHRR_ERR_INVALID_ARG, "no force kernel for the current tuning");
-    const int64_t npad = round_up(n, kPad);
-    khrr_status st;
     if ((st = c->cuda(c->kshadow.ensure(5 * static_cast<size_t>(npad)), "alloc")) != KHRR_OK) return st;
     ForcePlan& p = c->kplan;
     const int ctas = c->resident_ctas(vplan);
-    if (!p.valid || c->kplan_n != n || p.threads != v->threads || p.ipt != v->i_per_thread ||
+    if (!p.valid || p.pair || c->kplan_n != n || p.threads != v->threads || p.ipt != v->i_per_thread ||
         p.split_req != c->tuning.j_split || p.ctas != ctas) {
         std::vector<int64_t> poff{0, npad}, cnt{n};
         plan_force_items(poff, cnt, v->threads * v->i_per_thread, v->j_tile, ctas, c->tuning.j_split, false, p);
+        p.pair = false;
         p.threads = v->threads;
         p.ipt = v->i_per_thread;
         p.jt = v->j_tile;
@@ -77,8 +123,33 @@ khrr_status prepare_kernel_pass(khrr_ctx* c, const double* pos_i, const double* 
 
 khrr_status run_kernel_pass(khrr_ctx* c, const ForceVariant* v, bool distinct_i) {
     ForcePlan& p = c->kplan;
-    ForceArgs a{};
     const int64_t npad = round_up(c->kplan_n, kPad);
+    if (v->pair) {
+        PairArgs a{};
+        a.sh = shadow_at(c->kshadow.p, npad);
+        a.items = p.d_pair_items.p;
+        a.n_items = static_cast<int>(p.pair_items.size());
+        a.queue = c->queue.p;
+        a.part = c->kpart4.p;
+        a.npad = npad;
+        a.err = c->errflag.p;
+        cudaStream_t s = c->stream;
+        cudaEvent_t e0 = nullptr, e1 = nullptr;
+        khrr_status st;
+        if (c->timing && (st = c->timing_pair(&e0, &e1)) != KHRR_OK) return st;
+        if ((st = c->cuda(cudaMemsetAsync(c->queue.p, 0, sizeof(unsigned), s), "queue reset")) != KHRR_OK) return st;
+        if (e0) cudaEventRecord(e0, s);
+        if ((st = c->cuda(launch_pair(v, a, std::min(a.n_items, c->resident_ctas(v)), s), "pair force kernel")) !=
+            KHRR_OK)
+            return st;
+        if (e1) cudaEventRecord(e1, s);
+        if (c->timing) {
+            c->timed_launches += 1;
+            c->timed_pairs += static_cast<double>(c->kplan_n) * static_cast<double>(c->kplan_n);
+        }
+        return KHRR_OK;
+    }
+    ForceArgs a{};
     a.j = shadow_at(c->kshadow.p, npad);
     a.i = distinct_i ? shadow_at(c->kishadow.p, npad) : a.j;
     a.items = p.d_items.p;
@@ -118,6 +189,10 @@ khrr_status khrr_accel(khrr_ctx* c, double* acc, const double* pos_i, const doub
     khrr_status st = prepare_kernel_pass(c, pos_i, pos_j, mass_j, eps2_j, n, true, false, &v);
     if (st != KHRR_OK) return st;
     if ((st = run_kernel_pass(c, v, pos_i != pos_j)) != KHRR_OK) return st;
+    if (v->pair)
+        return c->cuda(launch_reduce_pair_partials(c->kpart4.p, round_up(n, kPad), c->kplan.d_nsplit4.p, n, acc,
+                                                   nullptr, (flags & KHRR_OVERWRITE) != 0, c->stream),
+                       "reduce partials");
     return c->cuda(launch_reduce_partials(c->kpart.p, round_up(n, kPad), c->kplan.nslots, n, acc, nullptr,
                                           (flags & KHRR_OVERWRITE) != 0, c->stream),
                    "reduce partials");
@@ -133,6 +208,10 @@ khrr_status khrr_phi(khrr_ctx* c, double* phi, const double* pos_i, const double
     khrr_status st = prepare_kernel_pass(c, pos_i, pos_j, mass_j, eps2_j, n, false, true, &v);
     if (st != KHRR_OK) return st;
     if ((st = run_kernel_pass(c, v, pos_i != pos_j)) != KHRR_OK) return st;
+    if (v->pair)
+        return c->cuda(launch_reduce_pair_partials(c->kpart4.p, round_up(n, kPad), c->kplan.d_nsplit4.p, n,
+                                                   nullptr, phi, (flags & KHRR_OVERWRITE) != 0, c->stream),
+                       "reduce partials");
     return c->cuda(launch_reduce_partials(c->kpart.p, round_up(n, kPad), c->kplan.nslots, n, nullptr, phi,
                                           (flags & KHRR_OVERWRITE) != 0, c->stream),
                    "reduce partials");
@@ -180,11 +259,13 @@ khrr_status khrr_autotune(khrr_ctx* c, const char* cache_path) {
     const khrr_tuning keep = c->tuning;
     khrr_tuning best = keep;
     double best_ms = 1e300;
-    // {threads, i bodies per thread, packed}; packed 2 is the symmetric pair kernel
-    const int shapes[][3] = {{128, 8, 2}, {128, 2, 1}, {128, 4, 1}, {256, 2, 1}, {256, 4, 1},
-                             {128, 4, 0},  {128, 8, 0}, {256, 4, 0}, {256, 8, 0}};
+    // {threads, i bodies per thread, packed, j_split}; packed 2 is the
+    // symmetric pair kernel, whose j_split is its chunk of blocks per item
+    const int shapes[][4] = {{128, 8, 2, 0}, {128, 8, 2, 4}, {128, 8, 2, 12}, {128, 2, 1, 0}, {128, 4, 1, 0},
+                             {256, 2, 1, 0}, {256, 4, 1, 0}, {128, 4, 0, 0},  {128, 8, 0, 0}, {256, 4, 0, 0},
+                             {256, 8, 0, 0}};
     for (const auto& sh : shapes) {
-        khrr_tuning t{sh[0], sh[1], 128, 0, sh[2]};
+        khrr_tuning t{sh[0], sh[1], 128, sh[3], sh[2]};
         if (khrr_set_tuning(c, &t) != KHRR_OK) continue;
         khrr_enable_timing(c, 0);
         khrr_status st = khrr_forces(c, KHRR_ACC);  // warm-up (plans, caches)

@@ -105,6 +105,13 @@ int pair_variant_count();
 const ForceVariant* pair_variant(int idx);
 const ForceVariant* find_pair_variant(bool unif, bool acc, bool phi, bool block_mass);
 cudaError_t launch_pair(const ForceVariant* v, const PairArgs& a, int grid, cudaStream_t s);
+// Pair-kernel partials -> out[i] (+)= sum of the body's nsplit[i] slots (FP64);
+// phi[i] (-)= the potential sums.
+cudaError_t launch_reduce_pair_partials(const float4* part, long long npad, const unsigned short* nsplit, int64_t n,
+                                       double* acc, double* phi, bool overwrite, cudaStream_t s);
+// The pair kernel's partials take 16 bytes per body and slot; layouts whose
+// largest system would need more than this use the one-sided kernel.
+constexpr int64_t kPairPartBudget = int64_t(32) << 30;
 
 // Derived constants of the analytic halo/bulge field (dev_fex operands).
 struct FieldConsts {

@@ -148,6 +148,7 @@ struct khrr_ctx {
     // Kernel-level entry points: their own shadow, partials and plan.
     khrr::DevBuf<float> kshadow, kishadow;
     khrr::DevBuf<double4> kpart;
+    khrr::DevBuf<float4> kpart4;  // the pair kernel's partials (pos_i == pos_j under the pair tuning)
     khrr::ForcePlan kplan;
     int64_t kplan_n = -1;
 

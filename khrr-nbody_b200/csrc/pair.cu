@@ -387,6 +387,37 @@ const PairTable& pair_table() {
     return t;
 }
 
+// Partials -> out[i] (+)= sum over the body's nsplit[i] slots, in FP64
+// (the kernel-level entry points; the state path sums them in the corrector).
+__global__ void reduce_pair_partials_kernel(const float4* __restrict__ part, long long npad,
+                                            const unsigned short* __restrict__ nsplit, int64_t n,
+                                            double* __restrict__ acc, double* __restrict__ phi, int overwrite) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        double sx = 0.0, sy = 0.0, sz = 0.0, sp = 0.0;
+        const int ns = nsplit[i];
+        for (int s = 0; s < ns; ++s) {
+            const float4 p = part[s * npad + i];
+            sx += static_cast<double>(p.x);
+            sy += static_cast<double>(p.y);
+            sz += static_cast<double>(p.z);
+            sp += static_cast<double>(p.w);
+        }
+        if (acc) {
+            if (overwrite) {
+                acc[3 * i] = sx;
+                acc[3 * i + 1] = sy;
+                acc[3 * i + 2] = sz;
+            } else {
+                acc[3 * i] += sx;
+                acc[3 * i + 1] += sy;
+                acc[3 * i + 2] += sz;
+            }
+        }
+        if (phi) phi[i] = overwrite ? -sp : phi[i] - sp;
+    }
+}
+
 }  // namespace
 
 int pair_variant_count() { return pair_table().n; }
@@ -402,6 +433,16 @@ const ForceVariant* find_pair_variant(bool unif, bool acc, bool phi, bool block_
         if (v.uniform_eps == unif && v.acc == acc && v.phi == phi && v.tile_mass == block_mass) return &v;
     }
     return nullptr;
+}
+
+cudaError_t launch_reduce_pair_partials(const float4* part, long long npad, const unsigned short* nsplit, int64_t n,
+                                       double* acc, double* phi, bool overwrite, cudaStream_t s) {
+    int64_t g = (n + 255) / 256;
+    if (g > 148 * 32) g = 148 * 32;
+    if (g < 1) g = 1;
+    reduce_pair_partials_kernel<<<static_cast<unsigned>(g), 256, 0, s>>>(part, npad, nsplit, n, acc, phi,
+                                                                         overwrite ? 1 : 0);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_pair(const ForceVariant* v, const PairArgs& a, int grid, cudaStream_t s) {

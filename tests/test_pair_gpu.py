@@ -201,3 +201,52 @@ def test_tuning_validation(ctx):
     ctx.set_tuning(*PAIR, 0, 2)
     assert ctx.get_tuning()["packed"] == 2
     ctx.set_tuning()
+
+
+def _dev(torch, a):
+    return torch.as_tensor(np.ascontiguousarray(a, np.float64), device="cuda")
+
+
+def test_kernel_level_entry_points_under_the_pair_tuning(ctx, golden, oracle):
+    """khrr_accel / khrr_phi (the reference's call sites) with pos_i == pos_j
+    take the pair kernel under the pair tuning: overwrite and accumulate modes,
+    the potential, a ragged multi-block size; a distinct target set still runs
+    the one-sided kernel."""
+    import torch
+    import khrr
+    g = golden("forces_n1536.npz")
+    ctx.set_tuning(*PAIR, 0, 2)
+    try:
+        for pos, mass, eps2, acc_ref, phi_ref, tol in (
+                (g["pos"], g["mass"], g["eps2"], g["acc_f64"], g["phi"], 1e-6),
+                (*galaxy(2500, 4321, seed=43, eps_d=0.006)[0:1], *galaxy(2500, 4321, seed=43, eps_d=0.006)[2:4],
+                 None, None, SMALL_N_TOL)):
+            n = len(mass)
+            if acc_ref is None:
+                acc_ref = oracle.accel_f64(pos, mass, eps2)
+                phi_ref = oracle.phi_f64(pos, mass, eps2)
+            P, M, E = _dev(torch, pos), _dev(torch, mass), _dev(torch, eps2)
+            A = torch.full((n, 3), 0.25, dtype=torch.float64, device="cuda")
+            F = torch.full((n,), 2.0, dtype=torch.float64, device="cuda")
+            torch.cuda.synchronize()
+            ctx.accel(A.data_ptr(), P.data_ptr(), P.data_ptr(), M.data_ptr(), E.data_ptr(), n, 0)
+            ctx.phi(F.data_ptr(), P.data_ptr(), P.data_ptr(), M.data_ptr(), E.data_ptr(), n, 0)
+            ctx.synchronize()
+            assert rel_rms(A.cpu().numpy() - 0.25, acc_ref) <= tol
+            assert rel_rms(F.cpu().numpy() - 2.0, phi_ref) <= tol
+            ctx.accel(A.data_ptr(), P.data_ptr(), P.data_ptr(), M.data_ptr(), E.data_ptr(), n, khrr.OVERWRITE)
+            ctx.synchronize()
+            assert rel_rms(A.cpu().numpy(), acc_ref) <= tol
+        pos, vel, mass, eps2 = galaxy(256, 512, seed=4)
+        pos_i = np.random.default_rng(9).uniform(-1, 1, pos.shape)
+        P, Pi, M, E = _dev(torch, pos), _dev(torch, pos_i), _dev(torch, mass), _dev(torch, eps2)
+        A = torch.zeros((len(mass), 3), dtype=torch.float64, device="cuda")
+        torch.cuda.synchronize()
+        ctx.accel(A.data_ptr(), Pi.data_ptr(), P.data_ptr(), M.data_ptr(), E.data_ptr(), len(mass), khrr.OVERWRITE)
+        ctx.synchronize()
+    finally:
+        ctx.set_tuning()
+    d = pos[None, :, :] - pos_i[:, None, :]
+    r2 = (d ** 2).sum(-1) + 0.5 * (eps2[:, None] + eps2[None, :])
+    ref = (d * (mass[None, :] / r2 ** 1.5)[:, :, None]).sum(1)
+    assert rel_rms(A.cpu().numpy(), ref) <= SMALL_N_TOL
