@@ -215,16 +215,14 @@ def test_kernel_level_entry_points_under_the_pair_tuning(ctx, golden, oracle):
     import torch
     import khrr
     g = golden("forces_n1536.npz")
+    rpos, _, rmass, reps2 = galaxy(2500, 4321, seed=43, eps_d=0.006)
+    cases = [(g["pos"], g["mass"], g["eps2"], g["acc_f64"], g["phi"], 1e-6),
+             (rpos, rmass, reps2, oracle.accel_f64(rpos, rmass, reps2), oracle.phi_f64(rpos, rmass, reps2),
+              SMALL_N_TOL)]
     ctx.set_tuning(*PAIR, 0, 2)
     try:
-        for pos, mass, eps2, acc_ref, phi_ref, tol in (
-                (g["pos"], g["mass"], g["eps2"], g["acc_f64"], g["phi"], 1e-6),
-                (*galaxy(2500, 4321, seed=43, eps_d=0.006)[0:1], *galaxy(2500, 4321, seed=43, eps_d=0.006)[2:4],
-                 None, None, SMALL_N_TOL)):
+        for pos, mass, eps2, acc_ref, phi_ref, tol in cases:
             n = len(mass)
-            if acc_ref is None:
-                acc_ref = oracle.accel_f64(pos, mass, eps2)
-                phi_ref = oracle.phi_f64(pos, mass, eps2)
             P, M, E = _dev(torch, pos), _dev(torch, mass), _dev(torch, eps2)
             A = torch.full((n, 3), 0.25, dtype=torch.float64, device="cuda")
             F = torch.full((n,), 2.0, dtype=torch.float64, device="cuda")
