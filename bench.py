@@ -599,11 +599,11 @@ def run_khrr(args):
         "roofline": {"bound": "fp32", "kernel": "pair_kernel" if pair_kernel else "force_kernel",
                      "achieved": achieved, "peak": peak_tflops,
                      "unit": "TFLOP/s", "frac": achieved / peak_tflops,
-                     # DRAM read+write of one force launch from the ncu captures on
-                     # 131,072 bodies, scaled to n: the one-sided kernel's 2.80 MB
-                     # (the shadow, once) by n; the pair kernel's 215 MB (its
-                     # FP32 partial slots, n x blocks / 2 of them) by n^2.
-                     "traffic": 215.0e6 * (n / 131072) ** 2 if pair_kernel else 2.80e6 * n / 131072,
+                     # DRAM read+write of one force launch from ncu captures: the
+                     # pair kernel's 6.09 GB at 786,432 bodies (its FP32 partial
+                     # slots, ~n x blocks / 2 of them) scaled by n^2; the one-sided
+                     # kernel's 2.80 MB at 131,072 (the shadow, once) by n.
+                     "traffic": 6.09e9 * (n / 786432) ** 2 if pair_kernel else 2.80e6 * n / 131072,
                      "flops_per_launch": force_flops(n, pair_kernel),
                      "pairs_per_launch": pairs_timed / max(launches, 1),
                      "avg_launch_ms": avg_launch_s * 1e3,
