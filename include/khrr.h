@@ -82,7 +82,13 @@ typedef struct khrr_lie {
 /* Force-kernel shape: threads per CTA, i bodies per thread, j-tile size,
  * j_split = number of j chunks per system (0 = chosen automatically), and
  * packed = 1 for the packed-FP32 (f32x2, two j bodies per instruction) inner
- * loop, 0 for the scalar one. */
+ * loop, 0 for the scalar one.  packed = 2 selects the symmetric pair kernel
+ * (shape {128, 8, 128}): each unordered pair of a system is evaluated once
+ * and applied to both bodies, the softening term (eps_i^2 + eps_j^2)/2 being
+ * symmetric; j_split is then its chunk of 1024-body blocks per work item
+ * (0 = chosen automatically).  It serves the state API and khrr_accel /
+ * khrr_phi calls with pos_i == pos_j; other calls run the packed 128 x 4
+ * one-sided kernel. */
 typedef struct khrr_tuning {
     int threads;
     int i_per_thread;
