@@ -643,13 +643,15 @@ khrr_status khrr_upload_state(khrr_ctx* c, int64_t n, const double* pos, const d
     if (off[0] != 0 || off[nsys] != n) return c->fail(KHRR_ERR_INVALID_ARG, "system offsets must span [0, n]");
     for (int k = 0; k < nsys; ++k)
         if (off[k + 1] <= off[k]) return c->fail(KHRR_ERR_INVALID_ARG, "system %d is empty", k);
-    for (int64_t i = 0; i < n; ++i)
-        if (!(eps2[i] > 0.0)) return c->fail(KHRR_ERR_INVALID_ARG, "eps2[%lld] must be > 0", (long long)i);
+    // One pass: every softening positive, and whether they are all equal.
+    bool uniform_new = true;
+    for (int64_t i = 0; i < n; ++i) {
+        const double e = eps2[i];
+        if (!(e > 0.0)) return c->fail(KHRR_ERR_INVALID_ARG, "eps2[%lld] must be > 0", (long long)i);
+        uniform_new = uniform_new && e == eps2[0];
+    }
     cudaSetDevice(c->device);
     // Same layout as the current state: plans and captured graphs stay valid.
-    bool uniform_new = true;
-    for (int64_t i = 1; i < n; ++i)
-        if (eps2[i] != eps2[0]) uniform_new = false;
     const bool same_layout = c->has_state && c->off == off && c->uniform == uniform_new &&
                              c->h_uniform == static_cast<float>(0.5 * eps2[0]);
     c->off.assign(off.begin(), off.end());
@@ -676,11 +678,13 @@ khrr_status khrr_upload_state(khrr_ctx* c, int64_t n, const double* pos, const d
     for (DevBuf<double>* b : {&c->pos, &c->vel, &c->acc, &c->post, &c->velt, &c->acct})
         cudaMemsetAsync(b->p, 0, 3 * np * sizeof(double), s);
     for (DevBuf<double>* b : {&c->mass, &c->phi}) cudaMemsetAsync(b->p, 0, np * sizeof(double), s);
-    // eps2 of ghosts = eps2 of their system's first body (positive).
-    std::vector<double> e2(np);
-    for (int k = 0; k < nsys; ++k) {
-        std::copy(eps2 + off[k], eps2 + off[k + 1], e2.begin() + c->poff[k]);
-        std::fill(e2.begin() + c->poff[k] + c->cnt[k], e2.begin() + c->poff[k + 1], eps2[off[k]]);
+    // eps2 of ghosts = eps2 of their system's first body (positive); the real
+    // bodies' values are copied straight from the caller's array below.
+    std::vector<double> ghost_eps2(np - static_cast<size_t>(n));
+    for (int k = 0, g = 0; k < nsys; ++k) {
+        const int64_t pad = c->poff[k + 1] - c->poff[k] - c->cnt[k];
+        std::fill(ghost_eps2.begin() + g, ghost_eps2.begin() + g + pad, eps2[off[k]]);
+        g += static_cast<int>(pad);
     }
     c->uniform = uniform_new;
     c->h_uniform = static_cast<float>(0.5 * eps2[0]);
@@ -713,11 +717,17 @@ khrr_status khrr_upload_state(khrr_ctx* c, int64_t n, const double* pos, const d
     if ((st = c->cuda(c->tile_mass.ensure(tm.size()), "alloc tile masses")) != KHRR_OK) return st;
     st = c->cuda(cudaMemcpyAsync(c->tile_mass.p, tm.data(), tm.size() * sizeof(float), cudaMemcpyHostToDevice, s),
                  "upload");
-    if (st == KHRR_OK)
-        st = c->cuda(cudaMemcpyAsync(c->eps2.p, e2.data(), np * sizeof(double), cudaMemcpyHostToDevice, s), "upload");
-    for (int k = 0; k < nsys && st == KHRR_OK; ++k) {
+    for (int k = 0, g = 0; k < nsys && st == KHRR_OK; ++k) {
         const size_t o = static_cast<size_t>(off[k]), q = static_cast<size_t>(c->poff[k]);
         const size_t m = static_cast<size_t>(c->cnt[k]);
+        const size_t pad = static_cast<size_t>(c->poff[k + 1]) - q - m;
+        st = c->cuda(cudaMemcpyAsync(c->eps2.p + q, eps2 + o, m * sizeof(double), cudaMemcpyHostToDevice, s), "upload");
+        if (st == KHRR_OK && pad)
+            st = c->cuda(cudaMemcpyAsync(c->eps2.p + q + m, ghost_eps2.data() + g, pad * sizeof(double),
+                                         cudaMemcpyHostToDevice, s),
+                         "upload");
+        g += static_cast<int>(pad);
+        if (st != KHRR_OK) break;
         st = c->cuda(cudaMemcpyAsync(c->pos.p + 3 * q, pos + 3 * o, 3 * m * sizeof(double), cudaMemcpyHostToDevice, s), "upload");
         if (st == KHRR_OK)
             st = c->cuda(cudaMemcpyAsync(c->vel.p + 3 * q, vel + 3 * o, 3 * m * sizeof(double), cudaMemcpyHostToDevice, s), "upload");
