@@ -21,14 +21,33 @@ namespace {
 int64_t round_up(int64_t v, int64_t m) { return (v + m - 1) / m * m; }
 
 // The pair kernel's plan, slot counts and partials for one system of n
-// bodies (the same set as i and j).
-khrr_status prepare_pair_pass(khrr_ctx* c, int64_t n, int64_t npad, bool acc, bool phi, const ForceVariant** vout) {
-    const ForceVariant* v = find_pair_variant(false, acc, phi, false);
+// bodies (the same set as i and j).  The caller's masses and softenings are
+// classified on the device first (one 8-byte read-back, which waits for the
+// stream's earlier work): whole 1024 blocks of one mass select the
+// block-mass form, equal softenings the uniform form.
+khrr_status prepare_pair_pass(khrr_ctx* c, const double* mass, const double* eps2, int64_t n, int64_t npad,
+                              bool acc, bool phi, const ForceVariant** vout) {
+    khrr_status st;
+    const size_t ntiles = static_cast<size_t>(npad / kPad);
+    if ((st = c->cuda(c->ktile_mass.ensure(ntiles), "alloc")) != KHRR_OK) return st;
+    if ((st = c->cuda(c->kflags.ensure(1), "alloc")) != KHRR_OK) return st;
+    cudaStream_t s = c->stream;
+    unsigned flags = 0;
+    double e0 = 0.0;
+    if ((st = c->cuda(cudaMemsetAsync(c->kflags.p, 0xff, sizeof(unsigned), s), "flags")) != KHRR_OK ||
+        (st = c->cuda(launch_classify(mass, eps2, n, c->ktile_mass.p, c->kflags.p, s), "classify")) != KHRR_OK ||
+        (st = c->cuda(cudaMemcpyAsync(&flags, c->kflags.p, sizeof flags, cudaMemcpyDeviceToHost, s), "flags")) !=
+            KHRR_OK ||
+        (st = c->cuda(cudaMemcpyAsync(&e0, eps2, sizeof e0, cudaMemcpyDeviceToHost, s), "flags")) != KHRR_OK ||
+        (st = c->cuda(cudaStreamSynchronize(s), "classify sync")) != KHRR_OK)
+        return st;
+    const bool unif = (flags & 2u) != 0, block_mass = (flags & 1u) != 0 && n % kPairBlock == 0;
+    c->kh_uniform = static_cast<float>(0.5 * e0);
+    const ForceVariant* v = find_pair_variant(unif, acc, phi, block_mass);
     const ForceVariant* vplan = find_pair_variant(false, true, false, false);
     if (!v || !vplan) return c->fail(KHRR_ERR_INVALID_ARG, "no pair kernel for this output set");
     ForcePlan& p = c->kplan;
     const int ctas = c->resident_ctas(vplan);
-    khrr_status st;
     if (!p.valid || !p.pair || c->kplan_n != n || p.split_req != c->tuning.j_split || p.ctas != ctas) {
         std::vector<int64_t> poff{0, npad}, cnt{n};
         std::vector<unsigned short> ns;
@@ -71,7 +90,7 @@ khrr_status prepare_kernel_pass(khrr_ctx* c, const double* pos_i, const double* 
     if (c->tuning.packed == 2 && pos_i == pos_j &&
         pair_slots_bound({0, npad}) * npad * 16 <= kPairPartBudget) {
         if ((st = c->cuda(c->kshadow.ensure(5 * static_cast<size_t>(npad)), "alloc")) != KHRR_OK) return st;
-        if ((st = prepare_pair_pass(c, n, npad, acc, phi, vout)) != KHRR_OK) return st;
+        if ((st = prepare_pair_pass(c, mass_j, eps2_j, n, npad, acc, phi, vout)) != KHRR_OK) return st;
         return c->cuda(launch_pack(pos_j, mass_j, eps2_j, n, npad, shadow_at(c->kshadow.p, npad), c->stream), "pack");
     }
     // The one-sided kernel (i and j may be different sets); the pair tuning
@@ -132,6 +151,8 @@ khrr_status run_kernel_pass(khrr_ctx* c, const ForceVariant* v, bool distinct_i)
         a.queue = c->queue.p;
         a.part = c->kpart4.p;
         a.npad = npad;
+        a.h_uniform = c->kh_uniform;
+        a.tile_mass = c->ktile_mass.p;
         a.err = c->errflag.p;
         cudaStream_t s = c->stream;
         cudaEvent_t e0 = nullptr, e1 = nullptr;

@@ -109,6 +109,11 @@ cudaError_t launch_pair(const ForceVariant* v, const PairArgs& a, int grid, cuda
 // phi[i] (-)= the potential sums.
 cudaError_t launch_reduce_pair_partials(const float4* part, long long npad, const unsigned short* nsplit, int64_t n,
                                        double* acc, double* phi, bool overwrite, cudaStream_t s);
+// Caller's arrays -> tile_mass (first mass of each 128 tile) and *flags &=
+// ~1 unless every 1024 block is real bodies of one mass, &= ~2 unless every
+// softening equals eps2[0] (set *flags to ~0 first).
+cudaError_t launch_classify(const double* mass, const double* eps2, int64_t n, float* tile_mass, unsigned* flags,
+                            cudaStream_t s);
 // The pair kernel's partials take 16 bytes per body and slot; layouts whose
 // largest system would need more than this use the one-sided kernel.
 constexpr int64_t kPairPartBudget = int64_t(32) << 30;

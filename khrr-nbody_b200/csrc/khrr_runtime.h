@@ -149,6 +149,9 @@ struct khrr_ctx {
     khrr::DevBuf<float> kshadow, kishadow;
     khrr::DevBuf<double4> kpart;
     khrr::DevBuf<float4> kpart4;  // the pair kernel's partials (pos_i == pos_j under the pair tuning)
+    khrr::DevBuf<float> ktile_mass;   // their per-tile masses (block-mass form)
+    khrr::DevBuf<unsigned> kflags;    // classification of the caller's arrays
+    float kh_uniform = 0.0f;          // 0.5 eps2[0] when the softenings are all equal
     khrr::ForcePlan kplan;
     int64_t kplan_n = -1;
 

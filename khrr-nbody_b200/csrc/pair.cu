@@ -418,6 +418,41 @@ __global__ void reduce_pair_partials_kernel(const float4* __restrict__ part, lon
     }
 }
 
+// Classification of a caller's body arrays for the kernel-level entry points,
+// one warp per 128-body tile: tile_mass[t] = the tile's first mass; bit 0 of
+// *flags is cleared unless every body of the tile is real and has the mass of
+// its 1024 block's first body (the block-mass form), bit 1 unless every
+// softening equals eps2[0] (the uniform form).
+__global__ void classify_kernel(const double* __restrict__ mass, const double* __restrict__ eps2, int64_t n,
+                                float* __restrict__ tile_mass, unsigned* __restrict__ flags) {
+    const int64_t warps = (static_cast<int64_t>(gridDim.x) * blockDim.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    const int64_t ntiles = (n + kPad - 1) / kPad;
+    const double e0 = eps2[0];
+    for (int64_t t = (blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x) >> 5; t < ntiles; t += warps) {
+        const double mt = mass[t * kPad], mb = mass[(t * kPad / kPairBlock) * kPairBlock];
+        bool same_mass = true, same_eps = true;
+#pragma unroll
+        for (int q = 0; q < kPad / 32; ++q) {
+            const int64_t i = t * kPad + q * 32 + lane;
+            if (i < n) {
+                const double m = mass[i];
+                same_mass = same_mass && m == mt && m == mb;
+                same_eps = same_eps && eps2[i] == e0;
+            } else {
+                same_mass = false;
+            }
+        }
+        same_mass = __all_sync(0xffffffffu, same_mass);
+        same_eps = __all_sync(0xffffffffu, same_eps);
+        if (lane == 0) {
+            tile_mass[t] = static_cast<float>(mt);
+            if (!same_mass) atomicAnd(flags, ~1u);
+            if (!same_eps) atomicAnd(flags, ~2u);
+        }
+    }
+}
+
 }  // namespace
 
 int pair_variant_count() { return pair_table().n; }
@@ -442,6 +477,16 @@ cudaError_t launch_reduce_pair_partials(const float4* part, long long npad, cons
     if (g < 1) g = 1;
     reduce_pair_partials_kernel<<<static_cast<unsigned>(g), 256, 0, s>>>(part, npad, nsplit, n, acc, phi,
                                                                          overwrite ? 1 : 0);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_classify(const double* mass, const double* eps2, int64_t n, float* tile_mass, unsigned* flags,
+                            cudaStream_t s) {
+    const int64_t ntiles = (n + kPad - 1) / kPad;
+    int64_t g = (ntiles * 32 + 255) / 256;
+    if (g > 148 * 16) g = 148 * 16;
+    if (g < 1) g = 1;
+    classify_kernel<<<static_cast<unsigned>(g), 256, 0, s>>>(mass, eps2, n, tile_mass, flags);
     return cudaGetLastError();
 }
 

@@ -209,16 +209,20 @@ def _dev(torch, a):
 
 def test_kernel_level_entry_points_under_the_pair_tuning(ctx, golden, oracle):
     """khrr_accel / khrr_phi (the reference's call sites) with pos_i == pos_j
-    take the pair kernel under the pair tuning: overwrite and accumulate modes,
-    the potential, a ragged multi-block size; a distinct target set still runs
-    the one-sided kernel."""
+    take the pair kernel under the pair tuning, in the form the caller's
+    arrays admit (classified on the device): overwrite and accumulate modes,
+    the potential, ragged and whole-block sizes, equal and per-component
+    softenings; a distinct target set still runs the one-sided kernel."""
     import torch
     import khrr
     g = golden("forces_n1536.npz")
-    rpos, _, rmass, reps2 = galaxy(2500, 4321, seed=43, eps_d=0.006)
-    cases = [(g["pos"], g["mass"], g["eps2"], g["acc_f64"], g["phi"], 1e-6),
-             (rpos, rmass, reps2, oracle.accel_f64(rpos, rmass, reps2), oracle.phi_f64(rpos, rmass, reps2),
-              SMALL_N_TOL)]
+    cases = [(g["pos"], g["mass"], g["eps2"], g["acc_f64"], g["phi"], 1e-6)]
+    # ragged (general form); whole 1024 blocks with equal softenings (the
+    # block-mass uniform form); whole blocks with two softenings
+    for ns, nd, eps_d, tol in ((2500, 4321, 0.006, SMALL_N_TOL), (2048, 4096, 0.004, 1e-6),
+                               (2048, 4096, 0.006, 1e-6)):
+        p_, _, m_, e_ = galaxy(ns, nd, seed=43, eps_d=eps_d)
+        cases.append((p_, m_, e_, oracle.accel_f64(p_, m_, e_), oracle.phi_f64(p_, m_, e_), tol))
     ctx.set_tuning(*PAIR, 0, 2)
     try:
         for pos, mass, eps2, acc_ref, phi_ref, tol in cases:
