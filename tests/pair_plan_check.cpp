@@ -1,0 +1,96 @@
+// Host-side check of the symmetric pair kernel's work plan (plan_pair_items
+// in libkhrr), run on the CPU by tests/test_pair_plan.py.  For a layout of
+// systems it replays every item as the kernel executes it:
+//   * evaluations, per ordered pair of 128-body tiles: the item's tiles of
+//     its own block ([j_begin, diag_end)) once, (i tile, j tile); every later
+//     tile twice, (i, j) and (j, i).  Every ordered pair of tiles of the same
+//     system must be evaluated exactly once, and none across systems.
+//   * partial slots: the i block's sums go to slot_i of its bodies, each
+//     symmetric tile's reactions to slot_j of the tile's bodies.  Every slot
+//     below a real body's count must be written exactly once, none above it,
+//     and no slot reaches nslots.
+// Prints "ok <items> <slots>" per layout, or the first violation.
+#include <cstdint>
+#include <cstdio>
+#include <cstdlib>
+#include <string>
+#include <vector>
+
+#include "khrr_runtime.h"
+
+using namespace khrr;
+
+namespace {
+
+int fail(const std::string& what, long long a, long long b) {
+    std::printf("FAIL %s (%lld, %lld)\n", what.c_str(), a, b);
+    return 1;
+}
+
+int check(const std::vector<int64_t>& cnt, int ctas, int chunk) {
+    std::vector<int64_t> poff(cnt.size() + 1, 0);
+    for (size_t k = 0; k < cnt.size(); ++k) poff[k + 1] = poff[k] + (cnt[k] + kPad - 1) / kPad * kPad;
+    const int64_t npad = poff.back(), ntiles = npad / kPad;
+    ForcePlan p;
+    std::vector<unsigned short> ns;
+    plan_pair_items(poff, cnt, ctas, chunk, p, ns);
+    if (static_cast<int64_t>(ns.size()) != npad) return fail("nsplit size", static_cast<long long>(ns.size()), npad);
+
+    std::vector<int> sys_of_tile(ntiles);
+    for (size_t k = 0; k < cnt.size(); ++k)
+        for (int64_t t = poff[k] / kPad; t < poff[k + 1] / kPad; ++t) sys_of_tile[t] = static_cast<int>(k);
+    std::vector<unsigned char> cover(static_cast<size_t>(ntiles * ntiles), 0);
+    std::vector<unsigned char> writes(static_cast<size_t>(p.nslots) * npad, 0);
+    auto hit = [&](int64_t a, int64_t b) { return ++cover[static_cast<size_t>(a * ntiles + b)] > 1; };
+    auto write = [&](int slot, int64_t i) {
+        if (slot < 0 || slot >= p.nslots) return true;
+        return ++writes[static_cast<size_t>(slot) * npad + i] > 1;
+    };
+
+    for (const PairItem& w : p.pair_items) {
+        if (w.i_begin % kPad || w.j_begin % kPad || w.j_end % kPad || w.i_end % kPad || w.diag_end % kPad)
+            return fail("unaligned item", w.i_begin, w.j_begin);
+        if (w.i_end - w.i_begin > kPairBlock || w.i_end <= w.i_begin || w.j_end <= w.j_begin)
+            return fail("bad item extent", w.i_begin, w.i_end);
+        if (w.diag_end != w.j_begin && !(w.j_begin == w.i_begin && w.diag_end == w.i_end))
+            return fail("own-block tiles must be the item's i block", w.j_begin, w.diag_end);
+        for (int64_t ti = w.i_begin / kPad; ti < w.i_end / kPad; ++ti)
+            for (int64_t tj = w.j_begin / kPad; tj < w.j_end / kPad; ++tj) {
+                if (sys_of_tile[ti] != sys_of_tile[tj]) return fail("pair across systems", ti, tj);
+                if (hit(ti, tj)) return fail("ordered tile pair evaluated twice", ti, tj);
+                if (tj * kPad >= w.diag_end && hit(tj, ti)) return fail("reverse tile pair evaluated twice", tj, ti);
+            }
+        for (int64_t i = w.i_begin; i < w.i_end; ++i)
+            if (write(w.slot_i, i)) return fail("i-side slot written twice or out of range", w.slot_i, i);
+        for (int64_t j = w.diag_end; j < w.j_end; ++j)
+            if (write(w.slot_j, j)) return fail("reaction slot written twice or out of range", w.slot_j, j);
+    }
+    for (int64_t a = 0; a < ntiles; ++a)
+        for (int64_t b = 0; b < ntiles; ++b) {
+            const bool same = sys_of_tile[a] == sys_of_tile[b];
+            if (cover[static_cast<size_t>(a * ntiles + b)] != (same ? 1 : 0)) return fail("tile pair not covered", a, b);
+        }
+    for (size_t k = 0; k < cnt.size(); ++k)
+        for (int64_t i = poff[k]; i < poff[k + 1]; ++i) {
+            const bool real = i < poff[k] + cnt[k];
+            if (!real && ns[i] != 0) return fail("ghost with slots", i, ns[i]);
+            for (int s = 0; s < ns[i]; ++s)
+                if (writes[static_cast<size_t>(s) * npad + i] != 1) return fail("slot of a real body not written", s, i);
+        }
+    std::printf("ok %zu %d\n", p.pair_items.size(), p.nslots);
+    return 0;
+}
+
+}  // namespace
+
+// Arguments: ctas chunk n_0 [n_1 ...]
+int main(int argc, char** argv) {
+    if (argc < 4) {
+        std::printf("usage: %s ctas chunk n0 [n1 ...]\n", argv[0]);
+        return 2;
+    }
+    const int ctas = std::atoi(argv[1]), chunk = std::atoi(argv[2]);
+    std::vector<int64_t> cnt;
+    for (int a = 3; a < argc; ++a) cnt.push_back(std::atoll(argv[a]));
+    return check(cnt, ctas, chunk);
+}
