@@ -78,7 +78,7 @@ int khrr_ctx::resident_ctas(const ForceVariant* v) {
 
 bool khrr_ctx::pair_mode() const {
     if (tuning.packed != 2 || !has_state) return false;
-    return pair_slots_bound(poff) * npad * 16 <= kPairPartBudget;
+    return pair_slots_bound(pair_blocks) * npad * 16 <= kPairPartBudget;
 }
 
 // The state's kernel: the symmetric pair kernel when the tuning asks for it
@@ -184,10 +184,33 @@ void plan_force_items(const std::vector<int64_t>& poff, const std::vector<int64_
     }
 }
 
-int64_t pair_slots_bound(const std::vector<int64_t>& poff) {
+PairBlocks pair_blocks_fixed(const std::vector<int64_t>& poff) {
+    PairBlocks out(poff.size() - 1);
+    for (size_t k = 0; k + 1 < poff.size(); ++k) {
+        for (int64_t b = poff[k]; b < poff[k + 1]; b += kPairBlock) out[k].push_back(b);
+        out[k].push_back(poff[k + 1]);
+    }
+    return out;
+}
+
+PairBlocks pair_blocks_by_mass(const std::vector<int64_t>& poff, const std::vector<float>& tile_mass) {
+    PairBlocks out(poff.size() - 1);
+    for (size_t k = 0; k + 1 < poff.size(); ++k) {
+        int64_t start = poff[k];
+        out[k].push_back(start);
+        for (int64_t t = poff[k] + kPad; t < poff[k + 1]; t += kPad)
+            if (t - start == kPairBlock || tile_mass[t / kPad] != tile_mass[start / kPad]) {
+                start = t;
+                out[k].push_back(start);
+            }
+        out[k].push_back(poff[k + 1]);
+    }
+    return out;
+}
+
+int64_t pair_slots_bound(const PairBlocks& blocks) {
     int64_t nb = 1;
-    for (size_t k = 0; k + 1 < poff.size(); ++k)
-        nb = std::max(nb, (poff[k + 1] - poff[k] + kPairBlock - 1) / kPairBlock);
+    for (const auto& bb : blocks) nb = std::max<int64_t>(nb, static_cast<int64_t>(bb.size()) - 1);
     return nb;
 }
 
@@ -196,32 +219,32 @@ int64_t pair_slots_bound(const std::vector<int64_t>& poff) {
 // partials: the reactions of blocks 0..b-1 (slots 0..b-1) and its own row's
 // chunk sums (slots b..).  C is the largest chunk (up to 32 blocks) that still
 // gives the persistent grid about 16 items per CTA; items run costliest first.
-void plan_pair_items(const std::vector<int64_t>& poff, const std::vector<int64_t>& cnt, int ctas, int chunk,
+void plan_pair_items(const PairBlocks& blocks, const std::vector<int64_t>& cnt, int ctas, int chunk,
                      ForcePlan& out, std::vector<unsigned short>& nsplit) {
     out.pair_items.clear();
     const size_t nsys = cnt.size();
-    nsplit.assign(static_cast<size_t>(poff[nsys]), 0);
+    nsplit.assign(static_cast<size_t>(blocks[nsys - 1].back()), 0);
     double block_pairs = 0.0;
-    for (size_t k = 0; k < nsys; ++k) {
-        const double nb = static_cast<double>((poff[k + 1] - poff[k] + kPairBlock - 1) / kPairBlock);
+    for (const auto& bb : blocks) {
+        const double nb = static_cast<double>(bb.size() - 1);
         block_pairs += nb * (nb + 1.0) / 2.0;
     }
     int C = chunk;
     if (C <= 0) C = static_cast<int>(std::clamp(block_pairs / (16.0 * std::max(ctas, 1)), 1.0, 32.0));
     out.nslots = 1;
     for (size_t k = 0; k < nsys; ++k) {
-        const int64_t P = poff[k], np = poff[k + 1] - poff[k], real_end = poff[k] + cnt[k];
-        const int64_t nb = (np + kPairBlock - 1) / kPairBlock;
+        const std::vector<int64_t>& bb = blocks[k];
+        const int64_t nb = static_cast<int64_t>(bb.size()) - 1, real_end = bb[0] + cnt[k];
         for (int64_t b = 0; b < nb; ++b) {
-            const int64_t ib = P + b * kPairBlock, ie = std::min(ib + kPairBlock, P + np);
+            const int64_t ib = bb[b], ie = bb[b + 1];
             const int64_t nch = (nb - b + C - 1) / C;
             for (int64_t u = 0; u < nch; ++u) {
                 const int64_t Jb = b + u * C, Je = std::min(Jb + C, nb);
                 PairItem it{};
                 it.i_begin = static_cast<int>(ib);
                 it.i_end = static_cast<int>(ie);
-                it.j_begin = static_cast<int>(P + Jb * kPairBlock);
-                it.j_end = static_cast<int>(std::min(P + Je * kPairBlock, P + np));
+                it.j_begin = static_cast<int>(bb[Jb]);
+                it.j_end = static_cast<int>(bb[Je]);
                 it.diag_end = u == 0 ? it.i_end : it.j_begin;
                 it.slot_i = static_cast<int>(b + u);
                 it.slot_j = static_cast<int>(b);
@@ -250,7 +273,7 @@ khrr_status khrr_ctx::ensure_plan(bool plain) {
     if (!plain && v->pair) {
         if (p.valid && p.pair && p.split_req == tuning.j_split && p.ctas == ctas) return KHRR_OK;
         std::vector<unsigned short> ns;
-        plan_pair_items(poff, cnt, ctas, tuning.j_split, p, ns);
+        plan_pair_items(pair_blocks, cnt, ctas, tuning.j_split, p, ns);
         p.pair = true;
         p.threads = v->threads;
         p.ipt = v->i_per_thread;
@@ -704,16 +727,16 @@ khrr_status khrr_upload_state(khrr_ctx* c, int64_t n, const double* pos, const d
     }
     if (tile_uniform != c->tile_uniform_mass) c->drop_graphs();
     c->tile_uniform_mass = tile_uniform;
-    // The pair kernel's block-mass form: whole 1024 blocks of one mass each.
-    bool block_uniform = tile_uniform;
-    for (int k = 0; k < nsys && block_uniform; ++k) {
-        if (c->cnt[k] % kPairBlock) block_uniform = false;
-        for (int64_t b = 0; b < c->cnt[k] && block_uniform; b += kPairBlock)
-            for (int64_t q = kPad; q < kPairBlock; q += kPad)
-                if (tm[(c->poff[k] + b + q) / kPad] != tm[(c->poff[k] + b) / kPad]) block_uniform = false;
+    // The pair kernel's blocks: with one mass per tile, runs of equal-mass
+    // tiles cut at 1024 bodies (one mass per block: the block-mass form);
+    // otherwise 1024-body blocks.
+    PairBlocks blocks = tile_uniform ? pair_blocks_by_mass(c->poff, tm) : pair_blocks_fixed(c->poff);
+    if (tile_uniform != c->block_uniform_mass || blocks != c->pair_blocks) {
+        c->plan_batched.valid = false;
+        c->drop_graphs();
     }
-    if (block_uniform != c->block_uniform_mass) c->drop_graphs();
-    c->block_uniform_mass = block_uniform;
+    c->block_uniform_mass = tile_uniform;
+    c->pair_blocks = std::move(blocks);
     if ((st = c->cuda(c->tile_mass.ensure(tm.size()), "alloc tile masses")) != KHRR_OK) return st;
     st = c->cuda(cudaMemcpyAsync(c->tile_mass.p, tm.data(), tm.size() * sizeof(float), cudaMemcpyHostToDevice, s),
                  "upload");

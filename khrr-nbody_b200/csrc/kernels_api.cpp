@@ -49,9 +49,9 @@ khrr_status prepare_pair_pass(khrr_ctx* c, const double* mass, const double* eps
     ForcePlan& p = c->kplan;
     const int ctas = c->resident_ctas(vplan);
     if (!p.valid || !p.pair || c->kplan_n != n || p.split_req != c->tuning.j_split || p.ctas != ctas) {
-        std::vector<int64_t> poff{0, npad}, cnt{n};
+        std::vector<int64_t> cnt{n};
         std::vector<unsigned short> ns;
-        plan_pair_items(poff, cnt, ctas, c->tuning.j_split, p, ns);
+        plan_pair_items(pair_blocks_fixed({0, npad}), cnt, ctas, c->tuning.j_split, p, ns);
         p.pair = true;
         p.threads = v->threads;
         p.ipt = v->i_per_thread;
@@ -88,7 +88,7 @@ khrr_status prepare_kernel_pass(khrr_ctx* c, const double* pos_i, const double* 
     const int64_t npad = round_up(n, kPad);
     khrr_status st;
     if (c->tuning.packed == 2 && pos_i == pos_j &&
-        pair_slots_bound({0, npad}) * npad * 16 <= kPairPartBudget) {
+        pair_slots_bound(pair_blocks_fixed({0, npad})) * npad * 16 <= kPairPartBudget) {
         if ((st = c->cuda(c->kshadow.ensure(5 * static_cast<size_t>(npad)), "alloc")) != KHRR_OK) return st;
         if ((st = prepare_pair_pass(c, mass_j, eps2_j, n, npad, acc, phi, vout)) != KHRR_OK) return st;
         return c->cuda(launch_pack(pos_j, mass_j, eps2_j, n, npad, shadow_at(c->kshadow.p, npad), c->stream), "pack");

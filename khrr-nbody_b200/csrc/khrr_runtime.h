@@ -75,14 +75,21 @@ struct ForcePlan {
 
 void plan_force_items(const std::vector<int64_t>& poff, const std::vector<int64_t>& cnt, int itile,
                       int jt, int ctas, int forced_split, bool plain, ForcePlan& out);
-// The symmetric pair kernel's items: block rows cut into chunks of
-// `chunk` blocks (0 = chosen from the CTA count); nsplit gets the slot count
-// of every padded body (0 for ghosts).
-void plan_pair_items(const std::vector<int64_t>& poff, const std::vector<int64_t>& cnt, int ctas, int chunk,
+// The symmetric pair kernel's blocks: per system the padded indices
+// P_k = b_0 < b_1 < ... < b_nb = P_{k+1}, each block at most kPairBlock
+// bodies starting at a multiple of kPad.
+using PairBlocks = std::vector<std::vector<int64_t>>;
+// 1024-body blocks over each system's padded range (the last may be shorter).
+PairBlocks pair_blocks_fixed(const std::vector<int64_t>& poff);
+// Runs of 128-body tiles of one mass (tile_mass[tile]), cut at 1024 bodies.
+PairBlocks pair_blocks_by_mass(const std::vector<int64_t>& poff, const std::vector<float>& tile_mass);
+// The pair kernel's items: block rows cut into chunks of `chunk` blocks (0 =
+// chosen from the CTA count); nsplit gets the slot count of every padded body
+// (0 for ghosts).
+void plan_pair_items(const PairBlocks& blocks, const std::vector<int64_t>& cnt, int ctas, int chunk,
                      ForcePlan& out, std::vector<unsigned short>& nsplit);
-// Upper bound of the pair kernel's slot count for a layout (the largest
-// system's block count).
-int64_t pair_slots_bound(const std::vector<int64_t>& poff);
+// The pair kernel's slot count for a layout (the largest system's block count).
+int64_t pair_slots_bound(const PairBlocks& blocks);
 
 struct StepGraph {
     cudaGraph_t graph = nullptr;
@@ -137,7 +144,8 @@ struct khrr_ctx {
     float h_uniform = 0.0f;
     bool tile_uniform_mass = false;     // every 128-body tile of the layout has one mass
     khrr::DevBuf<float> tile_mass;      // that mass per tile (FP32)
-    bool block_uniform_mass = false;    // every system a whole number of 1024 blocks, one mass each
+    bool block_uniform_mass = false;    // every pair block has one mass (the pair kernel's block-mass form)
+    khrr::PairBlocks pair_blocks;       // the pair kernel's blocks of the layout
     khrr::FieldConsts field{};
     khrr_tuning tuning{128, 4, 128, 0, 1};
     khrr::ForcePlan plan_batched, plan_plain;

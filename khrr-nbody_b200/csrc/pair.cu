@@ -4,8 +4,10 @@
 // (nbody-kernel.cuh:43-86); the reference's softening term
 // 0.5 (eps2_i + eps2_j) is symmetric in i and j, so one r^-3 serves both.
 //
-// Decomposition.  A system's padded bodies form blocks of kPairBlock = 1024
-// (the last block may be shorter).  Block row b is the block pairs (b, J),
+// Decomposition.  A system's padded bodies form blocks of at most
+// kPairBlock = 1024 (whole 128-body tiles; with one mass per tile, runs of
+// equal-mass tiles, so every block has one mass).  Block row b is the block
+// pairs (b, J),
 // J >= b, cut into chunks of C blocks, one PairItem each.  A CTA holds the
 // bodies of block b in registers (8 per thread, 128 threads) and streams the
 // chunk's j bodies through a 3-stage ring of 128-body shared-memory tiles
@@ -34,9 +36,9 @@
 // against one i body (its coordinates duplicated in both lanes once per
 // item): d (3 add), r^2 (3 fma), two MUFU.RSQ, r^-3 (2 mul), i side (3 fma),
 // j side (3 fma) = 14 FP32 operations per two pair evaluations, 7 per
-// interaction against 11 for the one-sided kernel.  When every 1024 block has
-// one mass (and no ghosts) the masses are factored out of both sums;
-// otherwise m_j and m_i enter per pair (2 more multiplies).
+// interaction against 11 for the one-sided kernel.  When every block has one
+// mass (and no ghosts) the masses are factored out of both sums; otherwise
+// m_j and m_i enter per pair (2 more multiplies).
 //
 // Accuracy: the i-side tile partials (two 64-term halves) fold into
 // compensated (hi + lo) running sums kept in shared memory; a reaction partial
@@ -89,7 +91,10 @@ constexpr int kSUnroll = KHRR_PAIR_UNROLL;
 constexpr unsigned kUnif = 1;   // every body has the same softening: no h array
 constexpr unsigned kAcc = 2;    // accumulate accelerations
 constexpr unsigned kPhi = 4;    // accumulate potentials
-constexpr unsigned kBMass = 8;  // one mass per 1024 block: masses factored out
+constexpr unsigned kBMass = 8;  // one mass per block: masses factored out
+// Lanes past a short block's end, in the block-mass form, sit this far away:
+// r^-3 underflows to exactly 0, so they add nothing to the reactions.
+constexpr float kFar = 1.0e18f;
 
 template <unsigned F>
 struct PairShape {
@@ -156,7 +161,7 @@ __device__ __forceinline__ void pair_tile(const float* __restrict__ tile, float*
                 }
                 if (PHI) {
                     ai[CP][k] = BMASS ? __fadd2_rn(ai[CP][k], inv) : __ffma2_rn(M2, inv, ai[CP][k]);
-                    if (SYM) rp = BMASS ? __fadd2_rn(rp, inv) : __ffma2_rn(mi[k], inv, rp);
+                    if (SYM) rp = __ffma2_rn(mi[k], inv, rp);  // mi: 1 or 0 in the block-mass form
                 }
             }
             if (SYM) {
@@ -241,16 +246,19 @@ __global__ void __launch_bounds__(NT, ((F & kPhi) ? 2 : 3)) pair_kernel(const Pa
         }
 
         // The thread's i bodies k (index i_begin + k NT + tid), each duplicated
-        // in both lanes: negated coordinates, the eps term and the mass (0 past
-        // the block's end, so those lanes add no reaction).
+        // in both lanes: negated coordinates, the eps term and the mass (1 in
+        // the block-mass form, whose mass is applied per partial).  Lanes past
+        // the block's end add no reaction: mass 0, and in the block-mass form
+        // (mass not in the pair term) a position kFar away.
         float2 nx[K], ny[K], nz[K], hi[K], mi[K];
 #pragma unroll
         for (int k = 0; k < K; ++k) {
             const int i = w.i_begin + k * NT + tid;
             const bool in = i < w.i_end;
-            const float x = in ? -a.sh.x[i] : 0.f, y = in ? -a.sh.y[i] : 0.f, z = in ? -a.sh.z[i] : 0.f;
+            const float far = BMASS ? -kFar : 0.f;
+            const float x = in ? -a.sh.x[i] : far, y = in ? -a.sh.y[i] : far, z = in ? -a.sh.z[i] : far;
             const float h = UNIF ? 0.f : (in ? a.sh.h[i] : 1.f);
-            const float m = BMASS ? 1.f : (in ? a.sh.m[i] : 0.f);
+            const float m = in ? (BMASS ? 1.f : a.sh.m[i]) : 0.f;
             nx[k] = f2(x, x);
             ny[k] = f2(y, y);
             nz[k] = f2(z, z);

@@ -1,6 +1,9 @@
 // Host-side check of the symmetric pair kernel's work plan (plan_pair_items
 // in libkhrr), run on the CPU by tests/test_pair_plan.py.  For a layout of
-// systems it replays every item as the kernel executes it:
+// systems, with 1024-body blocks or with the blocks the block-mass form uses
+// (runs of equal-mass 128-body tiles, here two components per system with the
+// first a third of the bodies rounded down to whole tiles), it replays every
+// item as the kernel executes it:
 //   * evaluations, per ordered pair of 128-body tiles: the item's tiles of
 //     its own block ([j_begin, diag_end)) once, (i tile, j tile); every later
 //     tile twice, (i, j) and (j, i).  Every ordered pair of tiles of the same
@@ -27,13 +30,30 @@ int fail(const std::string& what, long long a, long long b) {
     return 1;
 }
 
-int check(const std::vector<int64_t>& cnt, int ctas, int chunk) {
+int check(const std::vector<int64_t>& cnt, int ctas, int chunk, bool by_mass) {
     std::vector<int64_t> poff(cnt.size() + 1, 0);
     for (size_t k = 0; k < cnt.size(); ++k) poff[k + 1] = poff[k] + (cnt[k] + kPad - 1) / kPad * kPad;
     const int64_t npad = poff.back(), ntiles = npad / kPad;
+    PairBlocks blocks = pair_blocks_fixed(poff);
+    if (by_mass) {
+        std::vector<float> tm(static_cast<size_t>(ntiles));
+        for (size_t k = 0; k < cnt.size(); ++k) {
+            const int64_t first = cnt[k] / 3 / kPad * kPad;
+            for (int64_t t = poff[k] / kPad; t < poff[k + 1] / kPad; ++t)
+                tm[t] = (t * kPad - poff[k] < first) ? 1.0f : 0.25f;
+        }
+        blocks = pair_blocks_by_mass(poff, tm);
+        for (size_t k = 0; k < cnt.size(); ++k)
+            for (size_t b = 0; b + 1 < blocks[k].size(); ++b) {
+                const int64_t lo = blocks[k][b], hi = blocks[k][b + 1];
+                if (hi - lo > kPairBlock || lo % kPad) return fail("bad block", lo, hi);
+                for (int64_t t = lo / kPad; t < hi / kPad; ++t)
+                    if (tm[t] != tm[lo / kPad]) return fail("block with two masses", lo, t);
+            }
+    }
     ForcePlan p;
     std::vector<unsigned short> ns;
-    plan_pair_items(poff, cnt, ctas, chunk, p, ns);
+    plan_pair_items(blocks, cnt, ctas, chunk, p, ns);
     if (static_cast<int64_t>(ns.size()) != npad) return fail("nsplit size", static_cast<long long>(ns.size()), npad);
 
     std::vector<int> sys_of_tile(ntiles);
@@ -83,14 +103,15 @@ int check(const std::vector<int64_t>& cnt, int ctas, int chunk) {
 
 }  // namespace
 
-// Arguments: ctas chunk n_0 [n_1 ...]
+// Arguments: fixed|mass ctas chunk n_0 [n_1 ...]
 int main(int argc, char** argv) {
-    if (argc < 4) {
-        std::printf("usage: %s ctas chunk n0 [n1 ...]\n", argv[0]);
+    if (argc < 5) {
+        std::printf("usage: %s fixed|mass ctas chunk n0 [n1 ...]\n", argv[0]);
         return 2;
     }
-    const int ctas = std::atoi(argv[1]), chunk = std::atoi(argv[2]);
+    const bool by_mass = std::string(argv[1]) == "mass";
+    const int ctas = std::atoi(argv[2]), chunk = std::atoi(argv[3]);
     std::vector<int64_t> cnt;
-    for (int a = 3; a < argc; ++a) cnt.push_back(std::atoll(argv[a]));
-    return check(cnt, ctas, chunk);
+    for (int a = 4; a < argc; ++a) cnt.push_back(std::atoll(argv[a]));
+    return check(cnt, ctas, chunk, by_mass);
 }

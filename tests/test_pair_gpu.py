@@ -68,6 +68,25 @@ def test_block_mass_galaxy(ctx, oracle, split, eps_d):
     assert rel_rms(out["phi"], oracle.phi_f64(pos, mass, eps2)) <= 1e-6
 
 
+@pytest.mark.parametrize("sizes", [[(1536, 2560)], [(640, 1408)], [(1536, 2560), (512, 1024), (2048, 4096)]])
+def test_block_mass_with_short_blocks(ctx, oracle, sizes):
+    """Component counts that are whole 128-body tiles but not whole 1024
+    blocks: the blocks are runs of equal-mass tiles (some shorter than 1024),
+    so the factored-mass form still applies; single and several systems."""
+    import khrr
+    parts = [galaxy(ns, nd, seed=44 + k) for k, (ns, nd) in enumerate(sizes)]
+    pos = np.concatenate([p[0] for p in parts])
+    vel = np.concatenate([p[1] for p in parts])
+    mass = np.concatenate([p[2] for p in parts])
+    eps2 = np.concatenate([p[3] for p in parts])
+    off = np.cumsum([0] + [len(p[2]) for p in parts])
+    out = pair_forces(ctx, pos, vel, mass, eps2, khrr.ACC | khrr.PHI, offsets=off)
+    for k, (ps, vs, ms, es) in enumerate(parts):
+        s = slice(off[k], off[k + 1])
+        assert rel_rms(out["acc"][s], oracle.accel_f64(ps, ms, es)) <= 1e-6
+        assert rel_rms(out["phi"][s], oracle.phi_f64(ps, ms, es)) <= 1e-6
+
+
 @pytest.mark.parametrize("n_s,n_d", [(1000, 2000), (130, 0), (1, 0), (1023, 1025), (3000, 77)])
 def test_general_form_ragged_sizes(ctx, oracle, n_s, n_d):
     """Counts that are not multiples of 1024 (or 128): ghosts, a short last
