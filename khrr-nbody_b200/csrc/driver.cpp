@@ -4,7 +4,12 @@
 //
 //   khrr_nbody [--data DIR] [--device K] [--compat-accumulate] [--no-mesh]
 //              [--mesh-nx N] [--mesh-dx D] [--wave] [--wave-fp32] [--cic]
-//              [--wave-setup ITERS] [--quiet]
+//              [--wave-setup ITERS] [--kernel auto|pair|one-sided] [--quiet]
+//
+// --kernel picks the direct-sum force kernel: auto (default) times the
+// candidates on the initial state (khrr_autotune), pair is the symmetric
+// kernel (each unordered pair once for both bodies), one-sided the kernel
+// that evaluates every ordered pair.
 //
 // --wave selects the reference's Wave solver (NBodySolver::Wave, compiled in
 // the reference but switched off at nbody.cu:1132): forces and potentials
@@ -54,6 +59,7 @@ struct Options {
     bool wave_fp32 = false;
     bool cic = false;
     int wave_setup = 20000;  // _iterations_to_setup, nbody.cu:1143
+    std::string kernel = "auto";
     bool quiet = false;
 };
 
@@ -173,6 +179,11 @@ Options parse(int argc, char** argv) {
         else if (a == "--wave-fp32") o.wave_fp32 = true;
         else if (a == "--cic") o.cic = true;
         else if (a == "--wave-setup") o.wave_setup = std::stoi(next());
+        else if (a == "--kernel") {
+            o.kernel = next();
+            if (o.kernel != "auto" && o.kernel != "pair" && o.kernel != "one-sided")
+                die("--kernel takes auto, pair or one-sided");
+        }
         else if (a == "--quiet") o.quiet = true;
         else die("unknown argument " + a);
     }
@@ -288,6 +299,12 @@ int main(int argc, char** argv) {
     if (khrr_create(device, &ctx) != KHRR_OK) die(std::format("no usable sm_100 device {}", device));
     if (field.Mh != 0.0 || field.Mb != 0.0) check(khrr_set_external_field(ctx, &field), ctx, "external field");
     check(khrr_upload_state(ctx, nn, pos.data(), vel.data(), mass.data(), eps2.data(), 1, nullptr), ctx, "upload");
+    if (!opt.wave && opt.kernel == "auto") {
+        check(khrr_autotune(ctx, nullptr), ctx, "autotune");
+    } else if (opt.kernel == "pair") {
+        const khrr_tuning pair{128, 8, 128, 0, 2};
+        check(khrr_set_tuning(ctx, &pair), ctx, "tuning");
+    }
     // Mesh of the save-time binning and of the Wave solver (nbody.cu:1134-1143).
     const int NX = opt.mesh_nx;
     const double L = 0.5 * NX * opt.mesh_dx;

@@ -39,9 +39,11 @@ def write_inputs(d: pathlib.Path, i_cont: int, tmax: float):
     (ini / "__start_nbody.ini").write_text(f"{i_cont} \t--- i_cont\n{tmax} \t--- tmax\n0.010 \t--- dt_save\n")
 
 
-def run_driver(d):
-    r = subprocess.run([str(DRIVER), "--data", str(d), "--quiet", "--mesh-nx", "32", "--mesh-dx", "0.25"],
-                       capture_output=True, text=True, timeout=600)
+def run_driver(d, kernel="one-sided"):
+    # the API runs below use the library's default (one-sided) kernel, so the
+    # driver is pinned to it for the bit-for-bit comparisons
+    r = subprocess.run([str(DRIVER), "--data", str(d), "--quiet", "--mesh-nx", "32", "--mesh-dx", "0.25",
+                        "--kernel", kernel], capture_output=True, text=True, timeout=600)
     assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
     return r
 
@@ -129,6 +131,22 @@ def test_driver_run_outputs_and_restart(libkhrr, tmp_path):
     _, pd2, _ = read_snapshot(bins / "DM_   20.bin", n - ns)
     assert abs(t2 - 0.2) < 1e-12
     assert np.abs(np.concatenate([ps2, pd2]) - state2["pos"]).max() <= 1e-12
+
+
+@pytest.mark.parametrize("kernel", ["pair", "auto"])
+def test_driver_kernel_choice(libkhrr, tmp_path, kernel):
+    """--kernel pair (the symmetric kernel) and auto (the autotuner) follow
+    the one-sided trajectory to FP32-rounding level (same 50 steps)."""
+    torch = pytest.importorskip("torch")
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    d = tmp_path / "nbody"
+    write_inputs(d, 0, 0.1)
+    run_driver(d, kernel)
+    n, ns, state, _ = api_run(d, 50)
+    _, ps, _ = read_snapshot(d / "bin" / "S_   10.bin", ns)
+    _, pd, _ = read_snapshot(d / "bin" / "DM_   10.bin", n - ns)
+    assert np.abs(np.concatenate([ps, pd]) - state["pos"]).max() <= 1e-7
 
 
 def test_driver_wave_mode(libkhrr, tmp_path):
