@@ -136,7 +136,11 @@ def test_driver_run_outputs_and_restart(libkhrr, tmp_path):
 @pytest.mark.parametrize("kernel", ["pair", "auto"])
 def test_driver_kernel_choice(libkhrr, tmp_path, kernel):
     """--kernel pair (the symmetric kernel) and auto (the autotuner) follow
-    the one-sided trajectory to FP32-rounding level (same 50 steps)."""
+    the one-sided trajectory over the same 50 steps.  The kernels sum each
+    body's terms in different orders (both within 1e-6 of FP64 per force
+    evaluation), and close encounters amplify those differences along the
+    trajectory: max |dx| <= 1e-5 here (measured 1.2e-6), between the
+    suite's 1e-7 after 10 steps and 1e-4 after 100 steps."""
     torch = pytest.importorskip("torch")
     if not torch.cuda.is_available():
         pytest.skip("no CUDA device")
@@ -146,7 +150,7 @@ def test_driver_kernel_choice(libkhrr, tmp_path, kernel):
     n, ns, state, _ = api_run(d, 50)
     _, ps, _ = read_snapshot(d / "bin" / "S_   10.bin", ns)
     _, pd, _ = read_snapshot(d / "bin" / "DM_   10.bin", n - ns)
-    assert np.abs(np.concatenate([ps, pd]) - state["pos"]).max() <= 1e-7
+    assert np.abs(np.concatenate([ps, pd]) - state["pos"]).max() <= 1e-5
 
 
 def test_driver_wave_mode(libkhrr, tmp_path):
