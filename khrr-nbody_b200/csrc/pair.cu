@@ -93,7 +93,8 @@ constexpr unsigned kAcc = 2;    // accumulate accelerations
 constexpr unsigned kPhi = 4;    // accumulate potentials
 constexpr unsigned kBMass = 8;  // one mass per block: masses factored out
 // Lanes past a short block's end, in the block-mass form, sit this far away:
-// r^-3 underflows to exactly 0, so they add nothing to the reactions.
+// r^-3 underflows to exactly 0, so they add nothing to the accelerations'
+// reactions, and r^-1 (< 6e-19) adds nothing visible to the potentials'.
 constexpr float kFar = 1.0e18f;
 
 template <unsigned F>
@@ -161,7 +162,7 @@ __device__ __forceinline__ void pair_tile(const float* __restrict__ tile, float*
                 }
                 if (PHI) {
                     ai[CP][k] = BMASS ? __fadd2_rn(ai[CP][k], inv) : __ffma2_rn(M2, inv, ai[CP][k]);
-                    if (SYM) rp = __ffma2_rn(mi[k], inv, rp);  // mi: 1 or 0 in the block-mass form
+                    if (SYM) rp = BMASS ? __fadd2_rn(rp, inv) : __ffma2_rn(mi[k], inv, rp);
                 }
             }
             if (SYM) {
@@ -194,10 +195,17 @@ __device__ __forceinline__ void pair_tile(const float* __restrict__ tile, float*
 }
 
 // Resident CTAs per SM the register allocation aims at: three (168
-// registers) for accelerations; the potential variants carry one more
-// accumulator per i body and per reaction and run at two.
+// registers), the uniform block-mass force + potential variant included (171
+// ms per pass at 786k bodies against 178 ms at two); the other force +
+// potential variants carry per-body masses or softenings as well and run at
+// two rather than spill.
 template <unsigned F>
-__global__ void __launch_bounds__(NT, ((F & kPhi) ? 2 : 3)) pair_kernel(const PairArgs a) {
+constexpr int pair_min_blocks() {
+    return ((F & kAcc) && (F & kPhi) && !((F & kUnif) && (F & kBMass))) ? 2 : 3;
+}
+
+template <unsigned F>
+__global__ void __launch_bounds__(NT, (pair_min_blocks<F>())) pair_kernel(const PairArgs a) {
     using S = PairShape<F>;
     constexpr bool UNIF = S::UNIF, ACC = S::ACC, PHI = S::PHI, BMASS = S::BMASS;
     constexpr int NC = S::NC, NCOMP = S::NCOMP, CP = NC - 1;
