@@ -7,8 +7,8 @@
 // Decomposition.  A system's padded bodies form blocks of at most
 // kPairBlock = 1024 (whole 128-body tiles; with one mass per tile, runs of
 // equal-mass tiles, so every block has one mass).  Block row b is the block
-// pairs (b, J),
-// J >= b, cut into chunks of C blocks, one PairItem each.  A CTA holds the
+// pairs (b, J), J >= b, cut into chunks of C blocks, one PairItem each.  A CTA
+// holds the
 // bodies of block b in registers (8 per thread, 128 threads) and streams the
 // chunk's j bodies through a 3-stage ring of 128-body shared-memory tiles
 // filled by cp.async.bulk (no multicast) completing on mbarriers.  Tiles of
@@ -35,15 +35,16 @@
 // Inner loop: packed f32x2 instructions over the two j bodies of a step
 // against one i body (its coordinates duplicated in both lanes once per
 // item): d (3 add), r^2 (3 fma), two MUFU.RSQ, r^-3 (2 mul), i side (3 fma),
-// j side (3 fma) = 14 FP32 operations per two pair evaluations, 7 per
-// interaction against 11 for the one-sided kernel.  When every block has one
+// j side (3 fma) = 14 f32x2 instructions per two pair evaluations, that is 14
+// FP32 operations per evaluation of an unordered pair and 7 per interaction,
+// against 11 per interaction for the one-sided kernel.  When every block has one
 // mass (and no ghosts) the masses are factored out of both sums; otherwise
 // m_j and m_i enter per pair (2 more multiplies).
 //
 // Accuracy: the i-side partials (two halves of 64 terms per tile, over one or
 // two tiles) fold into compensated (hi + lo) running sums kept in shared
-// memory; a reaction partial
-// is a sum of 1024 terms in three levels (8 i bodies, 32 lanes, 4 warps).
+// memory; a reaction partial is a sum of 1024 terms in three levels (8 i
+// bodies, 32 lanes, 4 warps).
 #include <cstdint>
 
 #include "async_copy.cuh"
