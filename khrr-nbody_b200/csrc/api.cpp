@@ -78,7 +78,7 @@ int khrr_ctx::resident_ctas(const ForceVariant* v) {
 
 bool khrr_ctx::pair_mode() const {
     if (tuning.packed != 2 || !has_state) return false;
-    return pair_slots_bound(pair_blocks) * npad * 16 <= kPairPartBudget;
+    return pair_slots_bound(pair_blocks) * npad * 16 <= pair_budget;
 }
 
 // The state's kernel: the symmetric pair kernel when the tuning asks for it
@@ -571,6 +571,7 @@ khrr_status khrr_create(int device, khrr_ctx** out) {
     khrr_ctx* c = new khrr_ctx();
     c->device = device;
     c->sm_count = prop.multiProcessorCount;
+    c->pair_budget = std::max<int64_t>(kPairPartBudget, static_cast<int64_t>(prop.totalGlobalMem) / 5 * 2);
     if (cudaStreamCreateWithFlags(&c->own, cudaStreamNonBlocking) != cudaSuccess ||
         cudaEventCreate(&c->ph0) != cudaSuccess || cudaEventCreate(&c->ph1) != cudaSuccess ||
         c->queue.ensure(1) != cudaSuccess || c->errflag.ensure(1) != cudaSuccess ||

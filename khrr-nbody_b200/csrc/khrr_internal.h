@@ -115,7 +115,10 @@ cudaError_t launch_reduce_pair_partials(const float4* part, long long npad, cons
 cudaError_t launch_classify(const double* mass, const double* eps2, int64_t n, float* tile_mass, unsigned* flags,
                             cudaStream_t s);
 // The pair kernel's partials take 16 bytes per body and slot; layouts whose
-// largest system would need more than this use the one-sided kernel.
+// largest system would need more than the budget use the one-sided kernel.
+// The state API's budget is 40 % of the device's memory, at least this floor
+// (72 GB on a 180 GB B200: a 2.1 M-body system needs 68.7 GB); the
+// kernel-level entry points keep the floor.
 constexpr int64_t kPairPartBudget = int64_t(32) << 30;
 
 // Derived constants of the analytic halo/bulge field (dev_fex operands).

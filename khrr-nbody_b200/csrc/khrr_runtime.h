@@ -145,6 +145,7 @@ struct khrr_ctx {
     bool tile_uniform_mass = false;     // every 128-body tile of the layout has one mass
     khrr::DevBuf<float> tile_mass;      // that mass per tile (FP32)
     bool block_uniform_mass = false;    // every pair block has one mass (the pair kernel's block-mass form)
+    int64_t pair_budget = khrr::kPairPartBudget;  // bytes the pair kernel's partials may take
     khrr::PairBlocks pair_blocks;       // the pair kernel's blocks of the layout
     khrr::FieldConsts field{};
     khrr_tuning tuning{128, 4, 128, 0, 1};

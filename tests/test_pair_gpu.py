@@ -271,3 +271,30 @@ def test_kernel_level_entry_points_under_the_pair_tuning(ctx, golden, oracle):
     r2 = (d ** 2).sum(-1) + 0.5 * (eps2[:, None] + eps2[None, :])
     ref = (d * (mass[None, :] / r2 ** 1.5)[:, :, None]).sum(1)
     assert rel_rms(A.cpu().numpy(), ref) <= SMALL_N_TOL
+
+
+def test_two_million_bodies_within_the_device_sized_budget(ctx, oracle):
+    """The 2,097,152-body system of the large-mesh configuration (698,368
+    stars + 1,398,784 DM, eps 0.002): 2,048 blocks whose partial slots take
+    68.7 GB, above the kernel-level floor (32 GiB) and within the state API's
+    budget (40 % of the device).  The pair kernel runs (its slots show up in
+    the device's used memory) and sampled targets meet the FP64 oracle.
+    Last in this file: the context keeps the slots until the module ends."""
+    import torch
+    import khrr
+    pos, vel, mass, eps2 = galaxy(698368, 1398784, seed=45, eps_s=0.002, eps_d=0.002)
+    n = len(mass)
+    free0, total = torch.cuda.mem_get_info()
+    if total < 150e9:
+        pytest.skip("needs a device with 150 GB or more")
+    ctx.set_tuning(*PAIR, 0, 2)
+    try:
+        ctx.upload(pos, vel, mass, eps2)
+        ctx.forces(khrr.ACC)
+        free1, _ = torch.cuda.mem_get_info()
+        out = ctx.download(pos=False, vel=False, phi=False)
+    finally:
+        ctx.set_tuning()
+    assert free0 - free1 >= 60e9  # 2,048 slots x 2,097,152 bodies x 16 B
+    tgt = np.random.default_rng(45).choice(n, 256, replace=False)
+    assert rel_rms(out["acc"][tgt], oracle.accel_f64(pos, mass, eps2, targets=tgt)) <= 1e-6
