@@ -83,12 +83,14 @@ static_assert(NT * K == kPairBlock, "block = threads x bodies per thread");
 static_assert(JT == NT, "one thread per j body writes the reaction partials");
 static_assert(JT % 64 == 0 && JT == kPad, "tiles are whole sub-chunk pairs and padding units");
 
-// Unroll of the 32-step loop (2 measured best at 786k bodies: 151.2 ms per
-// pass against 152.2 ms for 1 and 153.4 ms for 4).
+// Unroll of the 32-step loop, measured at 786k bodies: 2 for accelerations
+// (149.6 ms per pass against 153.1 for 1 and 151.2 for 4), 1 with the
+// potential (168.9 ms against 171.1 for 2 and 175.4 for 4).
 #ifndef KHRR_PAIR_UNROLL
 #define KHRR_PAIR_UNROLL 2
 #endif
 constexpr int kSUnroll = KHRR_PAIR_UNROLL;
+constexpr int kSUnrollPhi = 1;
 
 constexpr unsigned kUnif = 1;   // every body has the same softening: no h array
 constexpr unsigned kAcc = 2;    // accumulate accelerations
@@ -130,10 +132,11 @@ __device__ __forceinline__ void pair_tile(const float* __restrict__ tile, float*
     const float* M = tile + S::kOffM * JT;
     const float* H = tile + S::kOffH * JT;
     const int src = (lane + 1) & 31;
+    constexpr int kU = PHI ? kSUnrollPhi : kSUnroll;
 #pragma unroll 1
     for (int c0 = 0; c0 < JT / 32; c0 += 2) {
         float2 rx = f2(0.f, 0.f), ry = rx, rz = rx, rp = rx;  // reactions held by this lane
-#pragma unroll kSUnroll
+#pragma unroll kU
         for (int s = 0; s < 32; ++s) {
             const int ja = c0 * 32 + ((lane + s) & 31), jb = ja + 32;
             const float2 X2 = f2(X[ja], X[jb]), Y2 = f2(Y[ja], Y[jb]), Z2 = f2(Z[ja], Z[jb]);
