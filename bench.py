@@ -67,6 +67,11 @@ def parse():
     ap.add_argument("--no-ensemble", action="store_true", help="skip the 64-galaxy batched-vs-plain leg")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-mesh", action="store_true", help="skip the p2mesh (binning, scan, wave) leg")
+    ap.add_argument("--no-configs", action="store_true",
+                    help="skip the legs of the other configurations (small galaxy on GPU and host, encounter on "
+                         "the mesh path, two-million-body system)")
+    ap.add_argument("--drift-steps", type=int, default=100,
+                    help="steps of the FP32-vs-FP64 precision run at the workload's size (0 = skip)")
     ap.add_argument("--mesh-max-iter", type=int, default=0, help="cap on wave iterations (0 = to tolerance)")
     ap.add_argument("--n-stars", type=int, default=N_STARS)
     ap.add_argument("--n-dm", type=int, default=N_DM)
@@ -159,24 +164,44 @@ class ClockSampler:
 # ---------------------------------------------------------------------------
 # reference arm: the reference's ACCEL_kernel compiled for the host
 # ---------------------------------------------------------------------------
-def cpu_reference_sample(pos, mass, eps2, seconds, rng):
+def cpu_reference_sample(pos, vel, mass, eps2, seconds, rng):
     """Times the host-compiled reference (or the oracle port when _ref is
-    absent) on a seeded target subset; returns (pairs/s, cores, kind, sample)."""
+    absent) for one predictor -> force -> corrector step: its ACCEL_kernel on
+    a seeded target subset (scaled to all n targets) and its
+    kernelNbody_integTime predictor and corrector on all n bodies.  Returns
+    (interactions/s of the whole step, cores, kind, sample, seconds timed)."""
     sys.path.insert(0, str(ROOT / "oracle"))
     import pyoracle
     n = len(mass)
+    p = np.ascontiguousarray(pos, np.float64).reshape(-1)
+    v = np.ascontiguousarray(vel, np.float64).reshape(-1)
+    acc, post, velt = np.zeros_like(p), np.zeros_like(p), np.zeros_like(p)
     try:
         ref = pyoracle.Reference()
+        ref.set_field(nn=n)
         run = ref.accel
         cores = ref.max_threads()
         kind = "reference"
-        what = "ACCEL_kernel (nbody-kernel.cuh:89-142) FP64, host build of the reference (oracle/_ref)"
+        what = ("ACCEL_kernel (nbody-kernel.cuh:89-142) FP64 + kernelNbody_integTime (nbody-kernel.cuh:144-193), "
+                "host build of the reference (oracle/_ref)")
+
+        def integ():
+            ref.integ(acc, post, velt, p, v, DT, 0, 0.0, acc)
+            ref.integ(acc, post.copy(), v.copy(), post, velt, DT, 1, 0.0, acc.copy())
     except FileNotFoundError:
         orc = pyoracle.Oracle()
         run = orc.accel_f64
         cores = orc.max_threads()
         kind = "port"
-        what = "FP64 direct sum, oracle restatement (oracle/oracle.c)"
+        what = "FP64 direct sum + predictor-corrector, oracle restatement (oracle/oracle.c)"
+
+        def integ():
+            orc.integ(None, acc, post, velt, p, v, DT, 0, acc)
+            orc.integ(None, acc, post.copy(), v.copy(), post, velt, DT, 1, acc.copy())
+    integ()
+    t0 = time.perf_counter()
+    integ()
+    t_int = time.perf_counter() - t0
     t_cal = max(2 * cores, 16)
     tg = rng.choice(n, t_cal, replace=False)
     t0 = time.perf_counter()
@@ -187,7 +212,10 @@ def cpu_reference_sample(pos, mass, eps2, seconds, rng):
     t0 = time.perf_counter()
     run(pos, mass, eps2, tg)
     dt = time.perf_counter() - t0
-    return nt * n / dt, cores, kind, f"{nt} seeded targets x {n} sources, {what}", dt
+    step_s = dt * n / nt + t_int
+    sample = (f"{nt} seeded targets x {n} sources (force, scaled to {n} targets) + predictor and corrector on "
+              f"all {n} bodies ({t_int * 1e3:.1f} ms), {what}")
+    return float(n) * n / step_s, cores, kind, sample, dt + t_int
 
 
 def run_reference(args):
@@ -198,11 +226,11 @@ def run_reference(args):
     rng = np.random.default_rng(7)
     rates, total_t, pairs = [], 0.0, 0.0
     for k in range(args.warmup + args.steps):
-        rate, cores, kind, sample, dt = cpu_reference_sample(pos, mass, eps2, 6.0, rng)
+        rate, cores, kind, sample, dt = cpu_reference_sample(pos, vel, mass, eps2, 6.0, rng)
         if k >= args.warmup:
             rates.append(rate)
-            total_t += dt
-            pairs += rate * dt
+            total_t += float(len(mass)) ** 2 / rate
+            pairs += float(len(mass)) ** 2
     value = pairs / total_t / 1e9
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup,
@@ -210,7 +238,8 @@ def run_reference(args):
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator)",
             "config": config(args),
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": kind,
-                             "sample": sample + "; ms_per_step extrapolates one full n^2 force pass"},
+                             "sample": sample + "; ms_per_step is one full step, the force pass scaled from the "
+                                                "sample"},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
@@ -219,9 +248,11 @@ def run_reference(args):
 # ---------------------------------------------------------------------------
 # our arm
 # ---------------------------------------------------------------------------
-def ensemble_leg(khrr, ctx_device, torch, steps=8):
-    """Configs' 64-galaxy uneven ensemble: one batched step launch vs one
-    force launch per system (the plain path), in galaxy-steps/s."""
+def ensemble_leg(khrr, ctx_device, torch, steps=200, plain_steps=40):
+    """BASELINE configuration 3, the 64-galaxy uneven ensemble: `steps` steps
+    with one batched (persistent) force launch per step vs `plain_steps` with
+    one force launch per system (the plain path), in galaxy-steps/s, and both
+    paths' acceleration error against the FP64 direct sum."""
     from khrr.galaxy import ensemble_sizes, make_galaxy
     sizes = ensemble_sizes(64, seed=77)
     parts = [make_galaxy(ns, nd, 2000 + k).arrays() for k, (ns, nd) in enumerate(sizes)]
@@ -237,7 +268,7 @@ def ensemble_leg(khrr, ctx_device, torch, steps=8):
         ctx.upload(pos, vel, mass, eps2, offsets=off)
         ctx.autotune(ROOT / "khrr-nbody_b200" / "build" / f"autotune_cache.{ctx_device}.json")
         out["tuning"] = ctx.get_tuning()
-        for label, flags in (("batched", 0), ("plain", khrr.PLAIN)):
+        for label, flags, nst in (("batched", 0, steps), ("plain", khrr.PLAIN, plain_steps)):
             ctx.upload(pos, vel, mass, eps2, offsets=off)
             ctx.forces(khrr.ACC | (flags & khrr.PLAIN))
             ctx.step(DT, 2, flags)
@@ -245,20 +276,22 @@ def ensemble_leg(khrr, ctx_device, torch, steps=8):
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             ctx.synchronize()
             e0.record(s)
-            ctx.step(DT, steps, flags)
+            ctx.step(DT, nst, flags)
             e1.record(s)
             e1.synchronize()
             ms = e0.elapsed_time(e1)
-            out[label + "_galaxy_steps_per_s"] = 64 * steps / (ms * 1e-3)
-            out[label + "_ms_per_step"] = ms / steps
-        # accuracy of the batched pass vs FP64 on sampled bodies of every galaxy
-        ctx.upload(pos, vel, mass, eps2, offsets=off)
-        ctx.forces(khrr.ACC)
-        acc = ctx.download(pos=False, vel=False, phi=False)["acc"]
+            out[label + "_steps"] = nst
+            out[label + "_galaxy_steps_per_s"] = 64 * nst / (ms * 1e-3)
+            out[label + "_ms_per_step"] = ms / nst
+        # accuracy of both passes vs FP64 on sampled bodies of every galaxy
         rng = np.random.default_rng(3)
         tg = np.sort(rng.choice(len(mass), 4096, replace=False))
+        ctx.upload(pos, vel, mass, eps2, offsets=off)
         ref, _ = ctx.accel_fp64_sample(tg)
-        out["acc_rel_rms_vs_fp64"] = float(np.sqrt(((acc[tg] - ref) ** 2).sum() / (ref ** 2).sum()))
+        for label, flags in (("", 0), ("plain_", khrr.PLAIN)):
+            ctx.forces(khrr.ACC | flags)
+            acc = ctx.download(pos=False, vel=False, phi=False)["acc"]
+            out[label + "acc_rel_rms_vs_fp64"] = float(np.sqrt(((acc[tg] - ref) ** 2).sum() / (ref ** 2).sum()))
     finally:
         ctx.close()
     out["batched_over_plain"] = out["batched_galaxy_steps_per_s"] / out["plain_galaxy_steps_per_s"]
@@ -419,6 +452,226 @@ def kick_drift_leg(khrr, ctx, torch, n, hbm_gbs):
     return out
 
 
+def _relative(log, key):
+    return [v[key] / log[0][key] - 1.0 if log[0][key] != 0 else None for v in log]
+
+
+def drift_vs_fp64_leg(khrr, ctx, torch, pos, vel, mass, eps2, steps, every=10, dt=DT, fp64_steps=None):
+    """The precision contract: `steps` predictor-corrector steps from the same
+    initial state with the FP32 force path (the context's tuned kernel) and
+    `fp64_steps` (default: as many) with the FP64 direct sum (KHRR_FP64), E
+    and L_z logged every `every` steps as the reference logs them at its saves
+    (nbody.cu:873-957).  ratio = |relative energy drift| of the FP32 run over
+    the FP64 run's after the same number of steps (target <= 1.1)."""
+    fp64_steps = steps if fp64_steps is None else fp64_steps
+    s = torch.cuda.ExternalStream(ctx.stream)
+    out = {"steps": steps, "fp64_steps": fp64_steps, "every": every, "dt": dt}
+    logs, final = {}, {}
+    for label, flags, nst in (("fp32", 0, steps), ("fp64", khrr.FP64, fp64_steps)):
+        ctx.upload(pos, vel, mass, eps2)
+        ctx.forces(khrr.ACC | khrr.PHI | flags)
+        log = [ctx.conservation()]
+        ms = 0.0
+        for _ in range(nst // every):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(s)
+            ctx.step(dt, every, flags | khrr.PHI)
+            e1.record(s)
+            e1.synchronize()
+            ms += e0.elapsed_time(e1)
+            log.append(ctx.conservation())
+        logs[label] = log
+        final[label] = ctx.download(vel=False, acc=False, phi=False)["pos"]
+        out[label + "_ms_per_step"] = ms / max(nst, 1)
+        out[label + "_interactions_per_s"] = float(len(mass)) ** 2 / (ms / max(nst, 1) * 1e-3)
+        out[label + "_energy_rel_log"] = _relative(log, "E")
+        out[label + "_lz_rel_log"] = _relative(log, "Lz")
+    k = min(steps, fp64_steps) // every
+    e32, e64 = out["fp32_energy_rel_log"][k], out["fp64_energy_rel_log"][k]
+    l32, l64 = out["fp32_lz_rel_log"][k], out["fp64_lz_rel_log"][k]
+    out.update({"compared_at_step": k * every, "energy_rel": abs(e32), "energy_rel_fp64": abs(e64),
+                "ratio": abs(e32) / abs(e64) if e64 else None,
+                "energy_rel_max": max(abs(x) for x in out["fp32_energy_rel_log"][:k + 1]),
+                "energy_rel_max_fp64": max(abs(x) for x in out["fp64_energy_rel_log"][:k + 1]),
+                "lz_rel": abs(l32) if l32 is not None else None,
+                "lz_rel_fp64": abs(l64) if l64 is not None else None,
+                "lz_ratio": abs(l32) / abs(l64) if l32 is not None and l64 else None})
+    if steps == fp64_steps:
+        out["max_dx_vs_fp64"] = float(np.abs(final["fp32"] - final["fp64"]).max())
+    return out
+
+
+def reference_cpu_steps(pos, vel, mass, eps2, n_stars, dt, nsteps):
+    """The reference's time loop (nbody.cu:1518-1582) on the host with its own
+    kernels (oracle/_ref, OpenMP): kernelNbody_integTime predictor,
+    ACCEL_kernel into a zeroed acct (the corrected loop), corrector.  Falls
+    back to the oracle's restatement when _ref is absent.  Returns (pos, vel,
+    seconds, cores, kind)."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import pyoracle
+    n = len(mass)
+    try:
+        ref = pyoracle.Reference()
+    except FileNotFoundError:
+        orc = pyoracle.Oracle()
+        t0 = time.perf_counter()
+        p, v, _, _ = orc.run_steps(pos, vel, mass, eps2, dt, nsteps)
+        return p, v, time.perf_counter() - t0, orc.max_threads(), "port"
+    ref.set_field(ns=n_stars, nn=n)
+    m = np.ascontiguousarray(mass, np.float64)
+    e = np.ascontiguousarray(eps2, np.float64)
+    p = np.ascontiguousarray(pos, np.float64).reshape(-1).copy()
+    v = np.ascontiguousarray(vel, np.float64).reshape(-1).copy()
+    post, velt = np.zeros_like(p), np.zeros_like(p)
+    t0 = time.perf_counter()
+    acc = ref.accel(p, m, e).reshape(-1).copy()
+    for _ in range(nsteps):
+        ref.integ(acc, post, velt, p, v, dt, 0, 0.0, acc)
+        acct = ref.accel(post, m, e).reshape(-1).copy()
+        ref.integ(acct, p, v, post, velt, dt, 1, 0.0, acc)
+    return p.reshape(-1, 3), v.reshape(-1, 3), time.perf_counter() - t0, ref.max_threads(), "reference"
+
+
+def config0_leg(khrr, device, torch, run_cpu=True):
+    """16,384 stars + 32,768 DM from the seeded
+    generator, dt 0.002, 100 predictor-corrector steps on the GPU (FP32 pair
+    kernel and FP64 direct sum) and on the reference's own kernels on the host
+    cores; trajectory differences and energy drifts of all three."""
+    from khrr.galaxy import make_galaxy
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import pyoracle
+    ns, nd, nsteps = 16384, 32768, 100
+    pos, vel, mass, eps = make_galaxy(ns, nd, SEED).arrays()
+    eps2 = eps * eps
+    n = len(mass)
+    ctx = khrr.Context(device)
+    try:
+        ctx.set_tuning(128, 8, 128, 0, 2)
+        d = drift_vs_fp64_leg(khrr, ctx, torch, pos, vel, mass, eps2, nsteps)
+        ctx.upload(pos, vel, mass, eps2)
+        ctx.forces(khrr.ACC)
+        ctx.step(DT, nsteps)
+        g32 = ctx.download(acc=False, phi=False)
+        ctx.upload(pos, vel, mass, eps2)
+        ctx.forces(khrr.ACC | khrr.FP64)
+        ctx.step(DT, nsteps, khrr.FP64)
+        g64 = ctx.download(acc=False, phi=False)
+    finally:
+        ctx.close()
+    out = {"bodies": n, "stars": ns, "dm": nd, "steps": nsteps, "dt": DT,
+           "gpu_fp32_ms_per_step": d["fp32_ms_per_step"], "gpu_fp64_ms_per_step": d["fp64_ms_per_step"],
+           "gpu_fp32_steps_per_s": 1e3 / d["fp32_ms_per_step"], "gpu_fp64_steps_per_s": 1e3 / d["fp64_ms_per_step"],
+           "gpu_fp32_interactions_per_s": d["fp32_interactions_per_s"],
+           "energy_rel_gpu_fp32": d["energy_rel"], "energy_rel_gpu_fp64": d["energy_rel_fp64"],
+           "energy_ratio_fp32_over_fp64": d["ratio"], "lz_rel_gpu_fp32": d["lz_rel"],
+           "max_dx_gpu_fp32_vs_gpu_fp64": d["max_dx_vs_fp64"]}
+    if run_cpu:
+        orc = pyoracle.Oracle()
+        p, v, sec, cores, kind = reference_cpu_steps(pos, vel, mass, eps2, ns, DT, nsteps)
+        c0 = orc.conservation(pos, vel, mass, orc.phi_f64(pos, mass, eps2))
+        c1 = orc.conservation(p, v, mass, orc.phi_f64(p, mass, eps2))
+        out.update({"cpu_kind": kind, "cpu_cores": cores, "cpu_seconds": sec,
+                    "cpu_steps_per_s": nsteps / sec,
+                    "cpu_interactions_per_s": float(n) ** 2 * (nsteps + 1) / sec,
+                    "cpu_what": "ACCEL_kernel + kernelNbody_integTime FP64 (oracle/_ref), OpenMP, "
+                                "acct zeroed each step",
+                    "energy_rel_cpu_reference": abs(c1["E"] / c0["E"] - 1.0),
+                    "max_dx_gpu_fp32_vs_cpu_reference": float(np.abs(g32["pos"] - p).max()),
+                    "max_dx_gpu_fp64_vs_cpu_reference": float(np.abs(g64["pos"] - p).max()),
+                    "max_dv_gpu_fp64_vs_cpu_reference": float(np.abs(g64["vel"] - v).max()),
+                    "gpu_fp64_steps_over_cpu": (1e3 / d["fp64_ms_per_step"]) / (nsteps / sec),
+                    "gpu_fp32_steps_over_cpu": (1e3 / d["fp32_ms_per_step"]) / (nsteps / sec)})
+    return out
+
+
+def config2_leg(khrr, device, torch, steps=500):
+    """the two-galaxy encounter (2 x (131,072 stars
+    + 262,144 DM), the second tilted 30 degrees) on the mesh path with the
+    analytic halo on (Mh 1, a 0.3333, Rh 1): CIC deposit on a 128^3 mesh over
+    [-4, 4]^3, (int)(dt / dt_wave) FP32 stencil iterations per step (the
+    reference's Wave mode), `steps` steps of dt 0.002 timed with CUDA events.
+    The mesh force is compared with the FP64 direct sum on 4096 targets at the
+    end (the mesh's resolution, not FP32 rounding, sets that difference)."""
+    from khrr.galaxy import two_galaxy_encounter
+    pos, vel, mass, eps2 = two_galaxy_encounter()
+    n, nx, L = len(mass), 128, 4.0
+    W = khrr.WaveParams.make(nx, 2 * L / nx)
+    ips = int(DT / W.dt)
+    ctx = khrr.Context(device)
+    try:
+        ctx.set_external_field(Mh=1.0, a=0.3333, Rh=1.0)
+        ctx.upload(pos, vel, mass, eps2)
+        ctx.set_mesh_solver(W, assign=khrr.ASSIGN_CIC, fp64=False, iters_per_step=ips, setup_iters=20000)
+        ctx.forces(khrr.ACC | khrr.PHI | khrr.MESH)
+        lie0 = ctx.conservation()
+        ctx.step(DT, 3, khrr.MESH)  # graphs of the ring rotations
+        s = torch.cuda.ExternalStream(ctx.stream)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(s)
+        ctx.step(DT, steps, khrr.MESH | khrr.PHI)
+        e1.record(s)
+        e1.synchronize()
+        ms = e0.elapsed_time(e1)
+        lie1 = ctx.conservation()
+        acc = ctx.download(pos=False, vel=False, phi=False)["acc"]
+        tg = np.sort(np.random.default_rng(17).choice(n, 4096, replace=False))
+        ref, _ = ctx.accel_fp64_sample(tg)
+        ctx.set_mesh_solver(None)
+    finally:
+        ctx.close()
+    cells = nx ** 3
+    return {"bodies": n, "mesh": f"{nx}^3 over [-{L:g}, {L:g}]^3", "steps": steps + 3, "timed_steps": steps,
+            "dt": DT, "halo": {"Mh": 1.0, "a": 0.3333, "Rh": 1.0}, "assign": "CIC", "stencil": "FP32",
+            "iterations_per_step": ips, "ms_per_step": ms / steps, "steps_per_s": steps / (ms * 1e-3),
+            "stencil_gbs": 16.0 * cells * ips / (ms / steps * 1e-3) / 1e9,
+            "stencil_gbs_note": "16 B per cell per iteration over the whole step time (deposit, gradient and "
+                                "gather included); the stencil alone is in mesh.encounter_128",
+            "energy_rel": abs(lie1["E"] / lie0["E"] - 1.0),
+            "energy_note": "E from the mesh potential of the N-body bodies (the reference's E excludes the "
+                           "external field, D11)",
+            "acc_rel_rms_vs_fp64_direct_sum": float(np.sqrt(((acc[tg] - ref) ** 2).sum() / (ref ** 2).sum()))}
+
+
+def config4_leg(khrr, device, torch, steps=20, targets=8192):
+    """2,097,152 bodies (698,368 stars + 1,398,784
+    DM, eps 0.002, total mass 7.699356), dt 0.001, `steps` steps with the
+    symmetric pair kernel; the acceleration error against the FP64 direct sum
+    on `targets` seeded bodies.  Its 256^3 mesh is mesh.large_256."""
+    from khrr.galaxy import assemble, make_galaxy
+    pos, vel, mass, eps2 = assemble([make_galaxy(698368, 1398784, 4000, eps_stars=0.002, eps_dm=0.002)],
+                                    [(0.0, (0, 0, 0), (0, 0, 0))])
+    n, dt = len(mass), 0.001
+    ctx = khrr.Context(device)
+    try:
+        ctx.set_tuning(128, 8, 128, 0, 2)
+        ctx.upload(pos, vel, mass, eps2)
+        ctx.forces(khrr.ACC)
+        acc = ctx.download(pos=False, vel=False, phi=False)["acc"]
+        tg = np.sort(np.random.default_rng(19).choice(n, targets, replace=False))
+        ref, _ = ctx.accel_fp64_sample(tg)
+        err = float(np.sqrt(((acc[tg] - ref) ** 2).sum() / (ref ** 2).sum()))
+        ctx.step(dt, 1)
+        s = torch.cuda.ExternalStream(ctx.stream)
+        ctx.synchronize()
+        ctx.enable_timing(True)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(s)
+        ctx.step(dt, steps)
+        e1.record(s)
+        e1.synchronize()
+        ms = e0.elapsed_time(e1)
+        fms, launches, pairs = ctx.force_timing()
+        ctx.enable_timing(False)
+    finally:
+        ctx.close()
+    per = fms / max(launches, 1)
+    return {"bodies": n, "steps": steps, "dt": dt, "ms_per_step": ms / steps, "steps_per_s": steps / (ms * 1e-3),
+            "interactions_per_s": float(n) ** 2 * steps / (ms * 1e-3), "force_ms_per_pass": per,
+            "force_tflops_20_per_pair": FLOPS_PER_PAIR * float(n) ** 2 / (per * 1e-3) / 1e12,
+            "acc_rel_rms_vs_fp64": err, "acc_err_targets": targets,
+            "force_memory_note": "pair kernel sums: 32 B per body (67 MB)"}
+
+
 def max_over_ranks(dist, values, device="cpu"):
     """Element-wise maximum of per-rank timings over all ranks (the identity
     without a process group).  Every rank calls it at the same point."""
@@ -568,6 +821,10 @@ def run_khrr(args):
     kick = None
     if rank == 0:
         kick = kick_drift_leg(khrr, ctx, torch, 4 * n, float(peaks.get("hbm_gbs", 6650.0)))
+    # the precision contract at this size: FP32 (tuned kernel) vs FP64 runs
+    drift64 = None
+    if rank == 0 and args.drift_steps > 0:
+        drift64 = drift_vs_fp64_leg(khrr, ctx, torch, pos, vel, mass, eps2, args.drift_steps)
     ens = None
     if not args.no_ensemble and rank == 0:
         ens = ensemble_leg(khrr, local, torch)
@@ -575,10 +832,17 @@ def run_khrr(args):
     if not args.no_mesh and rank == 0:
         mesh = mesh_leg(khrr, local, torch, float(peaks.get("hbm_gbs", 6650.0)), args.mesh_max_iter)
     ctx.close()
+    configs = None
+    if not args.no_configs and rank == 0:
+        configs = {"config0": config0_leg(khrr, local, torch, run_cpu=world == 1 and not args.no_cpu_baseline),
+                   "config1": "this line: value, roofline, acc_rel_rms_vs_fp64, drift_vs_fp64",
+                   "config2": config2_leg(khrr, local, torch),
+                   "config3": "ensemble",
+                   "config4": config4_leg(khrr, local, torch)}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        rate, cores, kind, sample, _ = cpu_reference_sample(pos, mass, eps2, 15.0, np.random.default_rng(5))
+        rate, cores, kind, sample, _ = cpu_reference_sample(pos, vel, mass, eps2, 15.0, np.random.default_rng(5))
         cpu = {"value": rate / 1e9, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample}
 
     if dist:
@@ -597,6 +861,7 @@ def run_khrr(args):
         "pct_fp32_peak_executed": 100.0 * executed / peak_tflops,
         "acc_rel_rms_vs_fp64": err, "acc_rel_max_vs_fp64": err_max, "acc_err_targets": int(len(tg)),
         "drift": drift,
+        "drift_vs_fp64": drift64,
         "plain": plain,
         "roofline": {"bound": "fp32", "kernel": "pair_kernel" if pair_kernel else "force_kernel",
                      "achieved": achieved, "peak": peak_tflops,
@@ -627,6 +892,7 @@ def run_khrr(args):
         "kick_drift": kick,
         "ensemble": ens,
         "mesh": mesh,
+        "configs": configs,
     }
     print(json.dumps(line), flush=True)
     return 0

@@ -59,9 +59,14 @@ enum {
                                    body per thread, shared-memory j tiles), one
                                    launch per system                              */
     KHRR_OVERWRITE = 16,        /* kernel-level calls: overwrite instead of +=    */
-    KHRR_MESH = 32              /* khrr_forces / khrr_step: forces from the mesh
+    KHRR_MESH = 32,             /* khrr_forces / khrr_step: forces from the mesh
                                    solver (khrr_set_mesh_solver), the reference's
                                    Wave mode, instead of the direct sum          */
+    KHRR_FP64 = 64              /* khrr_forces / khrr_step: the direct sum in FP64,
+                                   the reference's precision (ACCEL_kernel and
+                                   PHI_kernel with real = double), at about a
+                                   quarter of the FP32 pair kernel's rate: the
+                                   comparator for accuracy and energy drift      */
 };
 
 /* Analytic halo + bulge parameters (__gr_par.ini lines 1-6); the derived
@@ -334,14 +339,18 @@ khrr_status khrr_load_initial_conditions(const char* dir, const khrr_galaxy* g, 
  * KHRR_OVERWRITE), for 1 <= n <= KHRR_NOALLOC_MAX_BODIES; larger n returns
  * KHRR_ERR_TOO_LARGE before any device work.
  * Scratch: one file-scope device array of about 9.3 MiB (shadow positions,
- * work items, partial sums, a queue counter), which every GPU that loads the
- * library holds until the process exits.  The first call on a device looks up
- * that array's device address (with the device current) and sets the kernel's
- * attributes, so make the first call before any stream capture.  All calls
- * share the array and the counter is cleared on every call, so calls whose
- * GPU work overlaps (on different streams or host threads) race: serialize
- * them on one stream.  The call only enqueues work; it returns without
- * synchronizing. */
+ * work items, partial sums, a queue counter and an error flag), which every
+ * GPU that loads the library holds until the process exits.  The first call
+ * on a device looks up that array's device address (with the device current)
+ * and sets the kernel's attributes, so make the first call before any stream
+ * capture; if that set-up fails, the call returns the error and the next call
+ * tries it again.  All calls share the array and the counter and flag are
+ * cleared on every call, so calls whose GPU work overlaps (on different
+ * streams or host threads) race: serialize them on one stream.  The call only
+ * enqueues work; it returns without synchronizing, so a failure on the device
+ * cannot be its return value: if one of the kernel's bounded waits gives up
+ * (about 2 s without a copy completing), every entry of acc[0 .. 3n) is set
+ * to NaN instead of the sums, in either mode. */
 khrr_status khrr_accel_noalloc(double* acc, const double* pos_i, const double* pos_j,
                                const double* mass_j, const double* eps2_j, int64_t n,
                                int flags, void* stream);
@@ -368,12 +377,14 @@ khrr_status khrr_set_accelerations(khrr_ctx* ctx, const double* acc);
  * reference each run reports against.  acc: nt x 3, phi: nt (either NULL). */
 khrr_status khrr_accel_fp64_sample(khrr_ctx* ctx, const int64_t* targets, int64_t nt, double* acc,
                                    double* phi);
-/* Forces at the current positions (KHRR_ACC and/or KHRR_PHI; KHRR_PLAIN). */
+/* Forces at the current positions (KHRR_ACC and/or KHRR_PHI; KHRR_PLAIN or
+ * KHRR_FP64; KHRR_MESH). */
 khrr_status khrr_forces(khrr_ctx* ctx, int flags);
 /* nsteps predictor -> force -> corrector steps of size dt (nbody.cu:1525-1582),
  * replayed from a CUDA graph.  flags: KHRR_PHI evaluates the potential at the
  * new positions in the last step's force pass; KHRR_COMPAT_ACCUMULATE;
- * KHRR_PLAIN (per-system launches). */
+ * KHRR_PLAIN (per-system launches) or KHRR_FP64 (the FP64 direct sum);
+ * KHRR_MESH. */
 khrr_status khrr_step(khrr_ctx* ctx, double dt, int nsteps, int flags);
 /* L, Imp, Ek, Ep, E and maxima over all bodies (uses the last phi). */
 khrr_status khrr_conservation(khrr_ctx* ctx, khrr_lie* out);

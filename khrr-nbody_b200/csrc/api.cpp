@@ -7,8 +7,9 @@
 // reference's layout, so uploads and downloads are straight copies): pos,
 // vel, acc (a(t) without the external field), post/velt (predicted), acct
 // (force workspace of the literal reference loop), mass, eps2, phi.  The force
-// kernel reads the FP32 structure-of-arrays shadow (x, y, z, m, eps2 / 2) and
-// writes FP64 partials part[slot][body].
+// kernels read the FP32 structure-of-arrays shadow (x, y, z, m, eps2 / 2); the
+// one-sided kernel writes FP64 partials part[slot][body], the symmetric pair
+// kernel adds into 64-bit fixed-point sums fx[component][body].
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -76,10 +77,10 @@ int khrr_ctx::resident_ctas(const ForceVariant* v) {
     return occ * sm_count;
 }
 
-bool khrr_ctx::pair_mode() const {
-    if (tuning.packed != 2 || !has_state) return false;
-    return pair_slots_bound(pair_blocks) * npad * 16 <= pair_budget;
-}
+// The pair kernel's sums take 32 bytes per body whatever the layout, and the
+// state's softenings are positive (checked at upload), which the fixed-point
+// bounds need: the tuning alone decides.
+bool khrr_ctx::pair_mode() const { return tuning.packed == 2 && has_state; }
 
 // The state's kernel: the symmetric pair kernel when the tuning asks for it
 // (packed = 2) and the layout admits it; else the tile-mass form where the
@@ -208,22 +209,15 @@ PairBlocks pair_blocks_by_mass(const std::vector<int64_t>& poff, const std::vect
     return out;
 }
 
-int64_t pair_slots_bound(const PairBlocks& blocks) {
-    int64_t nb = 1;
-    for (const auto& bb : blocks) nb = std::max<int64_t>(nb, static_cast<int64_t>(bb.size()) - 1);
-    return nb;
-}
-
 // Block row b of a system with nb blocks holds the block pairs (b, J), J >= b,
-// cut into chunks of C blocks.  A body of block b receives nb_b = b + chunks(b)
-// partials: the reactions of blocks 0..b-1 (slots 0..b-1) and its own row's
-// chunk sums (slots b..).  C is the largest chunk (up to 32 blocks) that still
-// gives the persistent grid about 16 items per CTA; items run costliest first.
+// cut into chunks of C blocks.  A body of block b receives the reactions of
+// blocks 0..b-1 and its own row's chunk sums, all added into its fixed-point
+// accumulators.  C is the largest chunk (up to 32 blocks) that still gives
+// the persistent grid about 16 items per CTA; items run costliest first.
 void plan_pair_items(const PairBlocks& blocks, const std::vector<int64_t>& cnt, int ctas, int chunk,
-                     ForcePlan& out, std::vector<unsigned short>& nsplit) {
+                     ForcePlan& out) {
     out.pair_items.clear();
     const size_t nsys = cnt.size();
-    nsplit.assign(static_cast<size_t>(blocks[nsys - 1].back()), 0);
     double block_pairs = 0.0;
     for (const auto& bb : blocks) {
         const double nb = static_cast<double>(bb.size() - 1);
@@ -246,14 +240,10 @@ void plan_pair_items(const PairBlocks& blocks, const std::vector<int64_t>& cnt, 
                 it.j_begin = static_cast<int>(bb[Jb]);
                 it.j_end = static_cast<int>(bb[Je]);
                 it.diag_end = u == 0 ? it.i_end : it.j_begin;
-                it.slot_i = static_cast<int>(b + u);
-                it.slot_j = static_cast<int>(b);
+                it.real_end = static_cast<int>(real_end);
                 it.cost = static_cast<int>((ie - ib) * (it.j_end - it.j_begin) / kPairBlock);
                 out.pair_items.push_back(it);
             }
-            const int64_t ns = b + nch;
-            for (int64_t i = ib; i < std::min(ie, real_end); ++i) nsplit[i] = static_cast<unsigned short>(ns);
-            out.nslots = std::max<int>(out.nslots, static_cast<int>(ns));
         }
     }
     std::stable_sort(out.pair_items.begin(), out.pair_items.end(),
@@ -262,18 +252,48 @@ void plan_pair_items(const PairBlocks& blocks, const std::vector<int64_t>& cnt, 
 
 }  // namespace khrr
 
-khrr_status khrr_ctx::ensure_plan(bool plain) {
-    ForcePlan& p = plain ? plan_plain : plan_batched;
+khrr_status khrr_ctx::ensure_plan(int mode) {
+    ForcePlan& p = plan_for(mode);
+    const bool plain = mode == kModePlain;
+    khrr_status st;
+    if (mode == kModeF64) {
+        // The FP64 kernel's queue: 512-body i tiles, 128-body j tiles, the
+        // j split that fills the last wave of its resident CTAs.
+        const int ctas = fp64_force_ctas(sm_count);
+        if (p.valid && p.ctas == ctas) return KHRR_OK;
+        plan_force_items(poff, cnt, kF64ITile, kPad, ctas, 0, false, p);
+        p.pair = false;
+        p.threads = 128;
+        p.ipt = kF64ITile / 128;
+        p.jt = kPad;
+        p.split_req = 0;
+        p.ctas = ctas;
+        if ((st = cuda(p.d_items.ensure(p.items.size()), "alloc items")) != KHRR_OK) return st;
+        if ((st = cuda(cudaMemcpyAsync(p.d_items.p, p.items.data(), p.items.size() * sizeof(WorkItem),
+                                       cudaMemcpyHostToDevice, stream),
+                       "upload items")) != KHRR_OK)
+            return st;
+        std::vector<unsigned char> ns(static_cast<size_t>(npad), 0);
+        for (size_t k = 0; k < cnt.size(); ++k)
+            std::fill(ns.begin() + poff[k], ns.begin() + poff[k] + cnt[k], static_cast<unsigned char>(p.sys_split[k]));
+        if ((st = cuda(p.d_nsplit.ensure(ns.size()), "alloc nsplit")) != KHRR_OK) return st;
+        if ((st = cuda(cudaMemcpyAsync(p.d_nsplit.p, ns.data(), ns.size(), cudaMemcpyHostToDevice, stream),
+                       "upload nsplit")) != KHRR_OK)
+            return st;
+        if ((st = cuda(part.ensure(static_cast<size_t>(p.nslots) * npad), "alloc partials")) != KHRR_OK) return st;
+        if ((st = cuda(cudaStreamSynchronize(stream), "plan sync")) != KHRR_OK) return st;
+        p.valid = true;
+        drop_graphs();  // captured graphs may hold the old queue or partial buffer
+        return KHRR_OK;
+    }
     // The plan depends on the kernel shape only; acceleration and potential
     // passes of that shape share it (the grid follows each kernel's occupancy).
     const ForceVariant* v = variant(uniform, true, false);
     if (!v) return fail(KHRR_ERR_INVALID_ARG, "no force kernel for the current tuning");
     const int ctas = resident_ctas(v);
-    khrr_status st;
     if (!plain && v->pair) {
         if (p.valid && p.pair && p.split_req == tuning.j_split && p.ctas == ctas) return KHRR_OK;
-        std::vector<unsigned short> ns;
-        plan_pair_items(pair_blocks, cnt, ctas, tuning.j_split, p, ns);
+        plan_pair_items(pair_blocks, cnt, ctas, tuning.j_split, p);
         p.pair = true;
         p.threads = v->threads;
         p.ipt = v->i_per_thread;
@@ -285,12 +305,8 @@ khrr_status khrr_ctx::ensure_plan(bool plain) {
                                        cudaMemcpyHostToDevice, stream),
                        "upload items")) != KHRR_OK)
             return st;
-        if ((st = cuda(p.d_nsplit4.ensure(ns.size()), "alloc nsplit")) != KHRR_OK) return st;
-        if ((st = cuda(cudaMemcpyAsync(p.d_nsplit4.p, ns.data(), ns.size() * sizeof(unsigned short),
-                                       cudaMemcpyHostToDevice, stream),
-                       "upload nsplit")) != KHRR_OK)
+        if ((st = cuda(fx.ensure(static_cast<size_t>(kFxComps) * npad), "alloc fixed-point sums")) != KHRR_OK)
             return st;
-        if ((st = cuda(part4.ensure(static_cast<size_t>(p.nslots) * npad), "alloc partials")) != KHRR_OK) return st;
         if ((st = cuda(cudaStreamSynchronize(stream), "plan sync")) != KHRR_OK) return st;
         p.valid = true;
         drop_graphs();
@@ -360,18 +376,33 @@ ForceArgs khrr_ctx::force_args(const ForcePlan& p, int item_begin, int item_end)
     return a;
 }
 
-khrr_status khrr_ctx::enqueue_force(bool plain, bool acc, bool phi, bool events) {
+khrr_status khrr_ctx::enqueue_force(int mode, bool acc, bool phi, bool events, const double* x) {
+    const bool plain = mode == kModePlain;
     const ForceVariant* v = variant(uniform, acc, phi);
     if (!v) return fail(KHRR_ERR_INVALID_ARG, "no force kernel for the current tuning");
-    khrr_status st = ensure_plan(plain);
+    khrr_status st = ensure_plan(mode);
     if (st != KHRR_OK) return st;
-    ForcePlan& p = plain ? plan_plain : plan_batched;
-    const int ctas = resident_ctas(v);
+    ForcePlan& p = plan_for(mode);
+    const int ctas = mode == kModeF64 ? p.ctas : resident_ctas(v);
     // External records become event-record nodes when captured into a graph;
     // khrr_step points them at fresh timing events before each replay.
     if (events && (st = cuda(cudaEventRecordWithFlags(ph0, stream, cudaEventRecordExternal), "event")) != KHRR_OK)
         return st;
-    if (plain) {
+    if (mode == kModeF64) {
+        if ((st = cuda(cudaMemsetAsync(queue.p, 0, sizeof(unsigned), stream), "queue reset")) != KHRR_OK) return st;
+        F64Args a{};
+        a.pos = x;
+        a.mass = mass.p;
+        a.eps2 = eps2.p;
+        a.items = p.d_items.p;
+        a.n_items = static_cast<int>(p.items.size());
+        a.queue = queue.p;
+        a.part = part.p;
+        a.npad = npad;
+        if ((st = cuda(launch_fp64_force(a, acc, phi, std::min(a.n_items, ctas), stream), "FP64 force kernel")) !=
+            KHRR_OK)
+            return st;
+    } else if (plain) {
         // The conventional baseline: one launch per system, one i body per thread.
         for (size_t k = 0; k < cnt.size(); ++k) {
             Shadow sh = shadow();
@@ -389,13 +420,17 @@ khrr_status khrr_ctx::enqueue_force(bool plain, bool acc, bool phi, bool events)
     } else if (p.pair) {
         if (!v->pair) return fail(KHRR_ERR_INVALID_ARG, "no pair kernel for this output set");
         if ((st = cuda(cudaMemsetAsync(queue.p, 0, sizeof(unsigned), stream), "queue reset")) != KHRR_OK) return st;
+        if ((st = cuda(cudaMemsetAsync(fx.p, 0, sizeof(unsigned long long) * kFxComps * npad, stream),
+                       "sums reset")) != KHRR_OK)
+            return st;
         PairArgs a{};
         a.sh = shadow();
         a.items = p.d_pair_items.p;
         a.n_items = static_cast<int>(p.pair_items.size());
         a.queue = queue.p;
-        a.part = part4.p;
+        a.fx = fx.p;
         a.npad = npad;
+        a.scale = fx_scale.p;
         a.h_uniform = h_uniform;
         a.tile_mass = tile_mass.p;
         a.err = errflag.p;
@@ -426,18 +461,19 @@ StepArgs khrr_ctx::step_args(const ForcePlan& p, double dt) {
     a.part = part.p;
     a.npad = npad;
     a.nsplit = p.d_nsplit.p;
-    a.part4 = p.pair ? part4.p : nullptr;
-    a.nsplit4 = p.pair ? p.d_nsplit4.p : nullptr;
+    a.fx = p.pair ? fx.p : nullptr;
+    a.fx_scale = fx_scale.p;
     a.n = npad;
     a.dt = dt;
     a.field = field;
     return a;
 }
 
-khrr_status khrr_ctx::enqueue_step(double dt, bool plain, bool phi_now, bool compat) {
-    khrr_status st = enqueue_force(plain, true, phi_now, true);
+khrr_status khrr_ctx::enqueue_step(double dt, int mode, bool phi_now, bool compat) {
+    const bool plain = mode == kModePlain;
+    khrr_status st = enqueue_force(mode, true, phi_now, true, post.p);
     if (st != KHRR_OK) return st;
-    ForcePlan& p = plain ? plan_plain : plan_batched;
+    ForcePlan& p = plan_for(mode);
     StepArgs sa = step_args(p, dt);
     sa.compat_accumulate = compat ? 1 : 0;
     sa.want_phi = phi_now ? 1 : 0;
@@ -469,13 +505,13 @@ khrr_status khrr_ctx::enqueue_step(double dt, bool plain, bool phi_now, bool com
     return KHRR_OK;
 }
 
-khrr_status khrr_ctx::get_step_graph(double dt, bool plain, bool phi_now, bool compat, StepGraph** out) {
+khrr_status khrr_ctx::get_step_graph(double dt, int mode, bool phi_now, bool compat, StepGraph** out) {
     // Plans first: their uploads must not happen inside a capture.
-    khrr_status st = ensure_plan(plain);
+    khrr_status st = ensure_plan(mode);
     if (st != KHRR_OK) return st;
     uint64_t dt_bits;
     std::memcpy(&dt_bits, &dt, sizeof dt_bits);
-    const auto key = std::make_tuple(dt_bits, plain, phi_now, compat);
+    const auto key = std::make_tuple(dt_bits, mode, phi_now, compat);
     auto it = graphs.find(key);
     if (it != graphs.end()) {
         *out = &it->second;
@@ -484,7 +520,7 @@ khrr_status khrr_ctx::get_step_graph(double dt, bool plain, bool phi_now, bool c
     StepGraph g{};
     if ((st = cuda(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal), "begin capture")) != KHRR_OK)
         return st;
-    khrr_status est = enqueue_step(dt, plain, phi_now, compat);
+    khrr_status est = enqueue_step(dt, mode, phi_now, compat);
     cudaGraph_t graph = nullptr;
     cudaError_t ce = cudaStreamEndCapture(stream, &graph);
     if (est != KHRR_OK) {
@@ -526,6 +562,13 @@ khrr_status khrr_ctx::timing_pair(cudaEvent_t* e0, cudaEvent_t* e1) {
     *e0 = ev_pool[ev_used].first;
     *e1 = ev_pool[ev_used].second;
     ++ev_used;
+    return KHRR_OK;
+}
+
+khrr_status khrr_ctx::force_mode(int flags, int* mode) {
+    const bool plain = (flags & KHRR_PLAIN) != 0, f64 = (flags & KHRR_FP64) != 0;
+    if (plain && f64) return fail(KHRR_ERR_INVALID_ARG, "KHRR_PLAIN and KHRR_FP64 exclude each other");
+    *mode = plain ? kModePlain : (f64 ? kModeF64 : kModeBatched);
     return KHRR_OK;
 }
 
@@ -571,7 +614,6 @@ khrr_status khrr_create(int device, khrr_ctx** out) {
     khrr_ctx* c = new khrr_ctx();
     c->device = device;
     c->sm_count = prop.multiProcessorCount;
-    c->pair_budget = std::max<int64_t>(kPairPartBudget, static_cast<int64_t>(prop.totalGlobalMem) / 5 * 2);
     if (cudaStreamCreateWithFlags(&c->own, cudaStreamNonBlocking) != cudaSuccess ||
         cudaEventCreate(&c->ph0) != cudaSuccess || cudaEventCreate(&c->ph1) != cudaSuccess ||
         c->queue.ensure(1) != cudaSuccess || c->errflag.ensure(1) != cudaSuccess ||
@@ -739,6 +781,27 @@ khrr_status khrr_upload_state(khrr_ctx* c, int64_t n, const double* pos, const d
     c->block_uniform_mass = tile_uniform;
     c->pair_blocks = std::move(blocks);
     if ((st = c->cuda(c->tile_mass.ensure(tm.size()), "alloc tile masses")) != KHRR_OK) return st;
+    // Scales of the pair kernel's fixed-point sums per 128-body tile, from the
+    // tile's smallest h = eps2 / 2, its system's smallest h and total |mass|
+    // (real bodies; ghosts carry the system's first softening and no sums).
+    c->fx_scales.assign(tm.size(), FxScale{1.0, 1.0, 1.0, 1.0});
+    for (int k = 0; k < nsys; ++k) {
+        double msum = 0.0, hsys = 1e300;
+        for (int64_t i = off[k]; i < off[k + 1]; ++i) {
+            msum += std::fabs(mass[i]);
+            hsys = std::min(hsys, 0.5 * eps2[i]);
+        }
+        for (int64_t b = 0; b < c->cnt[k]; b += kPad) {
+            double ht = 1e300;
+            for (int64_t i = off[k] + b; i < std::min(off[k] + b + kPad, off[k + 1]); ++i) ht = std::min(ht, 0.5 * eps2[i]);
+            c->fx_scales[(c->poff[k] + b) / kPad] = fx_scale(ht, hsys, msum);
+        }
+    }
+    if ((st = c->cuda(c->fx_scale.ensure(tm.size()), "alloc tile scales")) != KHRR_OK) return st;
+    if ((st = c->cuda(cudaMemcpyAsync(c->fx_scale.p, c->fx_scales.data(), tm.size() * sizeof(FxScale),
+                                      cudaMemcpyHostToDevice, s),
+                      "upload")) != KHRR_OK)
+        return st;
     st = c->cuda(cudaMemcpyAsync(c->tile_mass.p, tm.data(), tm.size() * sizeof(float), cudaMemcpyHostToDevice, s),
                  "upload");
     for (int k = 0, g = 0; k < nsys && st == KHRR_OK; ++k) {
@@ -766,6 +829,7 @@ khrr_status khrr_upload_state(khrr_ctx* c, int64_t n, const double* pos, const d
     if (!same_layout) {
         c->plan_batched.valid = false;
         c->plan_plain.valid = false;
+        c->plan_fp64.valid = false;
         c->drop_graphs();
     }
     c->has_state = true;
@@ -851,7 +915,9 @@ khrr_status khrr_forces(khrr_ctx* c, int flags) {
     const bool want_acc = (flags & KHRR_ACC) != 0, want_phi = (flags & KHRR_PHI) != 0;
     if (!want_acc && !want_phi) return c->fail(KHRR_ERR_INVALID_ARG, "flags select nothing");
     if (flags & KHRR_MESH) return c->mesh_forces(flags);
-    const bool plain = (flags & KHRR_PLAIN) != 0;
+    int mode;
+    if (khrr_status st = c->force_mode(flags, &mode); st != KHRR_OK) return st;
+    const bool plain = mode == kModePlain;
     cudaStream_t s = c->stream;
     khrr_status st;
     // Shadow of the current positions (a previous step leaves the predicted ones).
@@ -861,13 +927,13 @@ khrr_status khrr_forces(khrr_ctx* c, int flags) {
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     if (c->timing && (st = c->timing_pair(&e0, &e1)) != KHRR_OK) return st;
     if (e0) cudaEventRecord(e0, s);
-    if ((st = c->enqueue_force(plain, want_acc, want_phi, false)) != KHRR_OK) return st;
+    if ((st = c->enqueue_force(mode, want_acc, want_phi, false, c->pos.p)) != KHRR_OK) return st;
     if (e1) cudaEventRecord(e1, s);
     if (c->timing) {
         c->timed_launches += plain ? static_cast<int64_t>(c->cnt.size()) : 1;
         c->timed_pairs += c->pairs_per_pass();
     }
-    ForcePlan& p = plain ? c->plan_plain : c->plan_batched;
+    ForcePlan& p = c->plan_for(mode);
     StepArgs sa = c->step_args(p, 0.0);
     sa.want_phi = want_phi ? 1 : 0;
     if ((st = c->cuda(launch_collect(sa, want_acc, (flags & KHRR_COMPAT_ACCUMULATE) != 0, s), "collect")) != KHRR_OK)
@@ -883,20 +949,21 @@ khrr_status khrr_step(khrr_ctx* c, double dt, int nsteps, int flags) {
     if (nsteps < 0 || !std::isfinite(dt)) return c->fail(KHRR_ERR_INVALID_ARG, "bad step arguments");
     if (nsteps == 0) return KHRR_OK;
     if (flags & KHRR_MESH) return c->mesh_step(dt, nsteps, flags);
-    const bool plain = (flags & KHRR_PLAIN) != 0;
+    int mode;
+    if (khrr_status st = c->force_mode(flags, &mode); st != KHRR_OK) return st;
+    const bool plain = mode == kModePlain;
     const bool compat = (flags & KHRR_COMPAT_ACCUMULATE) != 0;
     const bool phi_last = (flags & KHRR_PHI) != 0;
     khrr_status st;
     cudaStream_t s = c->stream;
     if (!c->predicted || c->pred_dt != dt) {
-        const ForcePlan& p = plain ? c->plan_plain : c->plan_batched;
-        StepArgs sa = c->step_args(p, dt);
+        StepArgs sa = c->step_args(c->plan_for(mode), dt);
         if ((st = c->cuda(launch_predictor(sa, s), "predictor")) != KHRR_OK) return st;
     }
     for (int k = 0; k < nsteps; ++k) {
         const bool phi_now = phi_last && k == nsteps - 1;
         StepGraph* g = nullptr;
-        if ((st = c->get_step_graph(dt, plain, phi_now, compat, &g)) != KHRR_OK) return st;
+        if ((st = c->get_step_graph(dt, mode, phi_now, compat, &g)) != KHRR_OK) return st;
         if (!g->ev0 || !g->ev1) return c->fail(KHRR_ERR_CUDA, "step graph lacks its timing event nodes");
         cudaEvent_t e0 = c->ph0, e1 = c->ph1;
         if (c->timing && (st = c->timing_pair(&e0, &e1)) != KHRR_OK) return st;

@@ -107,15 +107,13 @@ __global__ void predictor_kernel(const StepArgs a) {
 __device__ __forceinline__ void sum_partials(const StepArgs& a, int64_t i, d3& s, double& sp) {
     s = d3{0.0, 0.0, 0.0};
     sp = 0.0;
-    if (a.part4) {
-        const int ns = a.nsplit4[i];
-        for (int k = 0; k < ns; ++k) {
-            const float4 p = a.part4[k * a.npad + i];
-            s.x += static_cast<double>(p.x);
-            s.y += static_cast<double>(p.y);
-            s.z += static_cast<double>(p.z);
-            sp += static_cast<double>(p.w);
-        }
+    if (a.fx) {
+        // The pair kernel's fixed-point sums (zero for ghosts).
+        const FxScale sc = a.fx_scale[i / kPad];
+        s.x = static_cast<double>(static_cast<long long>(a.fx[i])) * sc.inv_acc;
+        s.y = static_cast<double>(static_cast<long long>(a.fx[a.npad + i])) * sc.inv_acc;
+        s.z = static_cast<double>(static_cast<long long>(a.fx[2 * a.npad + i])) * sc.inv_acc;
+        sp = static_cast<double>(static_cast<long long>(a.fx[3 * a.npad + i])) * sc.inv_phi;
         return;
     }
     const int ns = a.nsplit[i];

@@ -20,27 +20,37 @@ namespace {
 
 int64_t round_up(int64_t v, int64_t m) { return (v + m - 1) / m * m; }
 
-// The pair kernel's plan, slot counts and partials for one system of n
-// bodies (the same set as i and j).  The caller's masses and softenings are
-// classified on the device first (one 8-byte read-back, which waits for the
+// The pair kernel's plan, tile scales and fixed-point sums for one system of
+// n bodies (the same set as i and j).  The caller's masses and softenings are
+// classified on the device first (one 4-byte read-back, which waits for the
 // stream's earlier work): whole 1024 blocks of one mass select the
-// block-mass form, equal softenings the uniform form.
+// block-mass form, equal softenings the uniform form; a softening <= 0 leaves
+// the pass to the one-sided kernel (*vout = NULL), since the fixed-point
+// bounds need positive softenings.
 khrr_status prepare_pair_pass(khrr_ctx* c, const double* mass, const double* eps2, int64_t n, int64_t npad,
                               bool acc, bool phi, const ForceVariant** vout) {
+    *vout = nullptr;
     khrr_status st;
     const size_t ntiles = static_cast<size_t>(npad / kPad);
-    if ((st = c->cuda(c->ktile_mass.ensure(ntiles), "alloc")) != KHRR_OK) return st;
-    if ((st = c->cuda(c->kflags.ensure(1), "alloc")) != KHRR_OK) return st;
+    if ((st = c->cuda(c->ktile_mass.ensure(ntiles), "alloc")) != KHRR_OK ||
+        (st = c->cuda(c->ktile_hmin.ensure(ntiles), "alloc")) != KHRR_OK ||
+        (st = c->cuda(c->ktile_msum.ensure(ntiles), "alloc")) != KHRR_OK ||
+        (st = c->cuda(c->kscale.ensure(ntiles), "alloc")) != KHRR_OK ||
+        (st = c->cuda(c->kflags.ensure(1), "alloc")) != KHRR_OK)
+        return st;
     cudaStream_t s = c->stream;
     unsigned flags = 0;
     double e0 = 0.0;
     if ((st = c->cuda(cudaMemsetAsync(c->kflags.p, 0xff, sizeof(unsigned), s), "flags")) != KHRR_OK ||
-        (st = c->cuda(launch_classify(mass, eps2, n, c->ktile_mass.p, c->kflags.p, s), "classify")) != KHRR_OK ||
+        (st = c->cuda(launch_classify(mass, eps2, n, c->ktile_mass.p, c->ktile_hmin.p, c->ktile_msum.p, c->kscale.p,
+                                      c->kflags.p, s),
+                      "classify")) != KHRR_OK ||
         (st = c->cuda(cudaMemcpyAsync(&flags, c->kflags.p, sizeof flags, cudaMemcpyDeviceToHost, s), "flags")) !=
             KHRR_OK ||
         (st = c->cuda(cudaMemcpyAsync(&e0, eps2, sizeof e0, cudaMemcpyDeviceToHost, s), "flags")) != KHRR_OK ||
         (st = c->cuda(cudaStreamSynchronize(s), "classify sync")) != KHRR_OK)
         return st;
+    if (!(flags & 4u)) return KHRR_OK;  // a softening <= 0: one-sided kernel
     const bool unif = (flags & 2u) != 0, block_mass = (flags & 1u) != 0 && n % kPairBlock == 0;
     c->kh_uniform = static_cast<float>(0.5 * e0);
     const ForceVariant* v = find_pair_variant(unif, acc, phi, block_mass);
@@ -50,8 +60,7 @@ khrr_status prepare_pair_pass(khrr_ctx* c, const double* mass, const double* eps
     const int ctas = c->resident_ctas(vplan);
     if (!p.valid || !p.pair || c->kplan_n != n || p.split_req != c->tuning.j_split || p.ctas != ctas) {
         std::vector<int64_t> cnt{n};
-        std::vector<unsigned short> ns;
-        plan_pair_items(pair_blocks_fixed({0, npad}), cnt, ctas, c->tuning.j_split, p, ns);
+        plan_pair_items(pair_blocks_fixed({0, npad}), cnt, ctas, c->tuning.j_split, p);
         p.pair = true;
         p.threads = v->threads;
         p.ipt = v->i_per_thread;
@@ -63,15 +72,10 @@ khrr_status prepare_pair_pass(khrr_ctx* c, const double* mass, const double* eps
                                      cudaMemcpyHostToDevice),
                           "upload items")) != KHRR_OK)
             return st;
-        if ((st = c->cuda(p.d_nsplit4.ensure(ns.size()), "alloc")) != KHRR_OK) return st;
-        if ((st = c->cuda(cudaMemcpy(p.d_nsplit4.p, ns.data(), ns.size() * sizeof(unsigned short),
-                                     cudaMemcpyHostToDevice),
-                          "upload nsplit")) != KHRR_OK)
-            return st;
         p.valid = true;
         c->kplan_n = n;
     }
-    if ((st = c->cuda(c->kpart4.ensure(static_cast<size_t>(p.nslots) * npad), "alloc partials")) != KHRR_OK)
+    if ((st = c->cuda(c->kfx.ensure(static_cast<size_t>(kFxComps) * npad), "alloc fixed-point sums")) != KHRR_OK)
         return st;
     *vout = v;
     return KHRR_OK;
@@ -87,11 +91,12 @@ khrr_status prepare_kernel_pass(khrr_ctx* c, const double* pos_i, const double* 
     if (!pos_i || !pos_j || !mass_j || !eps2_j) return c->fail(KHRR_ERR_INVALID_ARG, "null device pointer");
     const int64_t npad = round_up(n, kPad);
     khrr_status st;
-    if (c->tuning.packed == 2 && pos_i == pos_j &&
-        pair_slots_bound(pair_blocks_fixed({0, npad})) * npad * 16 <= kPairPartBudget) {
+    if (c->tuning.packed == 2 && pos_i == pos_j) {
         if ((st = c->cuda(c->kshadow.ensure(5 * static_cast<size_t>(npad)), "alloc")) != KHRR_OK) return st;
         if ((st = prepare_pair_pass(c, mass_j, eps2_j, n, npad, acc, phi, vout)) != KHRR_OK) return st;
-        return c->cuda(launch_pack(pos_j, mass_j, eps2_j, n, npad, shadow_at(c->kshadow.p, npad), c->stream), "pack");
+        if (*vout)
+            return c->cuda(launch_pack(pos_j, mass_j, eps2_j, n, npad, shadow_at(c->kshadow.p, npad), c->stream),
+                           "pack");
     }
     // The one-sided kernel (i and j may be different sets); the pair tuning
     // maps to its packed 128 x 4 shape.
@@ -149,8 +154,9 @@ khrr_status run_kernel_pass(khrr_ctx* c, const ForceVariant* v, bool distinct_i)
         a.items = p.d_pair_items.p;
         a.n_items = static_cast<int>(p.pair_items.size());
         a.queue = c->queue.p;
-        a.part = c->kpart4.p;
+        a.fx = c->kfx.p;
         a.npad = npad;
+        a.scale = c->kscale.p;
         a.h_uniform = c->kh_uniform;
         a.tile_mass = c->ktile_mass.p;
         a.err = c->errflag.p;
@@ -159,6 +165,9 @@ khrr_status run_kernel_pass(khrr_ctx* c, const ForceVariant* v, bool distinct_i)
         khrr_status st;
         if (c->timing && (st = c->timing_pair(&e0, &e1)) != KHRR_OK) return st;
         if ((st = c->cuda(cudaMemsetAsync(c->queue.p, 0, sizeof(unsigned), s), "queue reset")) != KHRR_OK) return st;
+        if ((st = c->cuda(cudaMemsetAsync(c->kfx.p, 0, sizeof(unsigned long long) * kFxComps * npad, s),
+                          "sums reset")) != KHRR_OK)
+            return st;
         if (e0) cudaEventRecord(e0, s);
         if ((st = c->cuda(launch_pair(v, a, std::min(a.n_items, c->resident_ctas(v)), s), "pair force kernel")) !=
             KHRR_OK)
@@ -211,9 +220,9 @@ khrr_status khrr_accel(khrr_ctx* c, double* acc, const double* pos_i, const doub
     if (st != KHRR_OK) return st;
     if ((st = run_kernel_pass(c, v, pos_i != pos_j)) != KHRR_OK) return st;
     if (v->pair)
-        return c->cuda(launch_reduce_pair_partials(c->kpart4.p, round_up(n, kPad), c->kplan.d_nsplit4.p, n, acc,
-                                                   nullptr, (flags & KHRR_OVERWRITE) != 0, c->stream),
-                       "reduce partials");
+        return c->cuda(launch_reduce_pair_fx(c->kfx.p, round_up(n, kPad), c->kscale.p, n, acc, nullptr,
+                                             (flags & KHRR_OVERWRITE) != 0, c->stream),
+                       "reduce sums");
     return c->cuda(launch_reduce_partials(c->kpart.p, round_up(n, kPad), c->kplan.nslots, n, acc, nullptr,
                                           (flags & KHRR_OVERWRITE) != 0, c->stream),
                    "reduce partials");
@@ -230,9 +239,9 @@ khrr_status khrr_phi(khrr_ctx* c, double* phi, const double* pos_i, const double
     if (st != KHRR_OK) return st;
     if ((st = run_kernel_pass(c, v, pos_i != pos_j)) != KHRR_OK) return st;
     if (v->pair)
-        return c->cuda(launch_reduce_pair_partials(c->kpart4.p, round_up(n, kPad), c->kplan.d_nsplit4.p, n,
-                                                   nullptr, phi, (flags & KHRR_OVERWRITE) != 0, c->stream),
-                       "reduce partials");
+        return c->cuda(launch_reduce_pair_fx(c->kfx.p, round_up(n, kPad), c->kscale.p, n, nullptr, phi,
+                                             (flags & KHRR_OVERWRITE) != 0, c->stream),
+                       "reduce sums");
     return c->cuda(launch_reduce_partials(c->kpart.p, round_up(n, kPad), c->kplan.nslots, n, nullptr, phi,
                                           (flags & KHRR_OVERWRITE) != 0, c->stream),
                    "reduce partials");

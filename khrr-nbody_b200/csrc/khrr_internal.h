@@ -77,25 +77,46 @@ constexpr int kPairTile = 128;                             // j bodies per share
 // bodies [j_begin, j_end) of later blocks of the same system (the first
 // chunk of a row starts with the i block itself, [j_begin, diag_end), which
 // is evaluated one-sided).  Padded device indices; j bounds are multiples of
-// kPairTile.
+// kPairTile.  real_end ends the system's real bodies: sums of the ghosts
+// past it are not accumulated.
 struct PairItem {
     int i_begin;
     int i_end;
     int j_begin;
     int j_end;
     int diag_end;  // == j_begin when the chunk holds no tile of the i block
-    int slot_i;    // slot of the i block's sums over this chunk
-    int slot_j;    // slot of the reactions on the chunk's bodies (the i block's index)
+    int real_end;  // end of the system's real bodies
     int cost;      // planner's estimate (i bodies x j bodies / 1024)
+    int pad;
 };
+
+// The pair kernel's results are 64-bit fixed-point sums: every partial (an
+// FP32 sum) is scaled by a power of two and rounded to an integer, then added
+// with an integer atomic into its body's accumulator.  Integer addition is
+// associative, so the totals do not depend on the order the partials arrive
+// in (bitwise reproducible), and the accumulators take 32 bytes per body
+// (components ax, ay, az, sum m/r; [component][npad]).  The scale of a
+// 128-body tile keeps every possible sum of its bodies below 2^61
+// (fx_scale): for a body i, |a_i| <= sum_j m_j max_d d / (d^2 + H)^{3/2}
+// = 0.3849 M / H with H = h_i + h_j >= h_i + h_min, and
+// |sum m/r| <= M / sqrt(h_i + h_min).
+constexpr int kFxComps = 4;
+struct FxScale {
+    double acc, phi;          // 2^E: partial -> integer
+    double inv_acc, inv_phi;  // 2^-E: integer -> value
+};
+// Scale of one tile from its smallest h = eps^2 / 2, the system's smallest h
+// and the system's total |mass|.
+FxScale fx_scale(double h_tile_min, double h_sys_min, double mass_sys);
 
 struct PairArgs {
     Shadow sh;               // the bodies (i and j are the same set)
     const PairItem* items;
     int n_items;
     unsigned* queue;         // next-item counter (zeroed before each launch)
-    float4* part;            // partial sums [slot][npad]: ax, ay, az, sum m/r
-    long long npad;          // slot stride
+    unsigned long long* fx;  // fixed-point sums [kFxComps][npad] (zeroed before each launch)
+    long long npad;          // component stride
+    const FxScale* scale;    // per 128-body tile
     float h_uniform;         // 0.5 * eps2 when every body shares it
     const float* tile_mass;  // mass per 128-body tile (block-mass kernels)
     unsigned* err;           // device error flag word
@@ -105,21 +126,16 @@ int pair_variant_count();
 const ForceVariant* pair_variant(int idx);
 const ForceVariant* find_pair_variant(bool unif, bool acc, bool phi, bool block_mass);
 cudaError_t launch_pair(const ForceVariant* v, const PairArgs& a, int grid, cudaStream_t s);
-// Pair-kernel partials -> out[i] (+)= sum of the body's nsplit[i] slots (FP64);
-// phi[i] (-)= the potential sums.
-cudaError_t launch_reduce_pair_partials(const float4* part, long long npad, const unsigned short* nsplit, int64_t n,
-                                       double* acc, double* phi, bool overwrite, cudaStream_t s);
-// Caller's arrays -> tile_mass (first mass of each 128 tile) and *flags &=
-// ~1 unless every 1024 block is real bodies of one mass, &= ~2 unless every
-// softening equals eps2[0] (set *flags to ~0 first).
-cudaError_t launch_classify(const double* mass, const double* eps2, int64_t n, float* tile_mass, unsigned* flags,
-                            cudaStream_t s);
-// The pair kernel's partials take 16 bytes per body and slot; layouts whose
-// largest system would need more than the budget use the one-sided kernel.
-// The state API's budget is 40 % of the device's memory, at least this floor
-// (72 GB on a 180 GB B200: a 2.1 M-body system needs 68.7 GB); the
-// kernel-level entry points keep the floor.
-constexpr int64_t kPairPartBudget = int64_t(32) << 30;
+// Fixed-point sums -> acc[i] (+)= a_i and/or phi[i] (-)= sum m/r, i < n (FP64).
+cudaError_t launch_reduce_pair_fx(const unsigned long long* fx, long long npad, const FxScale* scale, int64_t n,
+                                  double* acc, double* phi, bool overwrite, cudaStream_t s);
+// Caller's arrays -> tile_mass (first mass of each 128 tile), the tile
+// scales of the fixed-point sums, and *flags &= ~1 unless every 1024 block is
+// real bodies of one mass, &= ~2 unless every softening equals eps2[0], &= ~4
+// unless every softening is positive (the pair kernel's condition; set *flags
+// to ~0 first).  tile_hmin, tile_msum: scratch of one double per tile.
+cudaError_t launch_classify(const double* mass, const double* eps2, int64_t n, float* tile_mass, double* tile_hmin,
+                            double* tile_msum, FxScale* scale, unsigned* flags, cudaStream_t s);
 
 // Derived constants of the analytic halo/bulge field (dev_fex operands).
 struct FieldConsts {
@@ -157,6 +173,21 @@ cudaError_t launch_fp64_sample(const double* pos, const double* mass, const doub
                                const int64_t* tgt, const int64_t* jb, const int64_t* je, int64_t nt,
                                double* out4, cudaStream_t s);
 
+// ---- force64.cu: the FP64 direct sum (KHRR_FP64) ------------------------------
+constexpr int kF64ITile = 512;  // i bodies per work item (128 threads x 4)
+struct F64Args {
+    const double* pos;      // positions the forces are wanted at, AoS double3 [npad]
+    const double* mass;     // [npad]
+    const double* eps2;     // [npad]
+    const WorkItem* items;  // work queue (plan_force_items with kF64ITile, j tiles of kPad)
+    int n_items;
+    unsigned* queue;        // next-item counter (zeroed before each launch)
+    double4* part;          // partial sums [slot][npad]: ax, ay, az, sum m/r
+    long long npad;
+};
+cudaError_t launch_fp64_force(const F64Args& a, bool acc, bool phi, int grid, cudaStream_t s);
+int fp64_force_ctas(int sm_count);  // resident CTAs of the FP64 kernel on the device
+
 // ---- integrate.cu -----------------------------------------------------------
 struct StepArgs {
     double* pos;          // x(t)           [npad] double3
@@ -171,8 +202,8 @@ struct StepArgs {
     const double4* part;  // force partials [slot][npad]
     long long npad;
     const unsigned char* nsplit;  // partial slots per body
-    const float4* part4;          // the pair kernel's FP32 partials [slot][npad] (replaces part when set)
-    const unsigned short* nsplit4;  // their slot count per body
+    const unsigned long long* fx;   // the pair kernel's fixed-point sums [kFxComps][npad] (replace part when set)
+    const FxScale* fx_scale;        // their scales per 128-body tile
     int64_t n;            // padded count
     double dt;
     FieldConsts field;

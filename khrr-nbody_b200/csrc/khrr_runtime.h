@@ -63,11 +63,10 @@ struct ForcePlan {
     int nslots = 1;
     DevBuf<WorkItem> d_items;
     DevBuf<unsigned char> d_nsplit;
-    // The symmetric pair kernel's queue (pair plans only) and slot counts.
+    // The symmetric pair kernel's queue (pair plans only).
     bool pair = false;
     std::vector<PairItem> pair_items;
     DevBuf<PairItem> d_pair_items;
-    DevBuf<unsigned short> d_nsplit4;
     ForcePlan() = default;
     ForcePlan(const ForcePlan&) = delete;
     ForcePlan& operator=(const ForcePlan&) = delete;
@@ -84,12 +83,14 @@ PairBlocks pair_blocks_fixed(const std::vector<int64_t>& poff);
 // Runs of 128-body tiles of one mass (tile_mass[tile]), cut at 1024 bodies.
 PairBlocks pair_blocks_by_mass(const std::vector<int64_t>& poff, const std::vector<float>& tile_mass);
 // The pair kernel's items: block rows cut into chunks of `chunk` blocks (0 =
-// chosen from the CTA count); nsplit gets the slot count of every padded body
-// (0 for ghosts).
+// chosen from the CTA count), costliest first.
 void plan_pair_items(const PairBlocks& blocks, const std::vector<int64_t>& cnt, int ctas, int chunk,
-                     ForcePlan& out, std::vector<unsigned short>& nsplit);
-// The pair kernel's slot count for a layout (the largest system's block count).
-int64_t pair_slots_bound(const PairBlocks& blocks);
+                     ForcePlan& out);
+
+// Force paths of the state API: the batched FP32 kernels (pair or one-sided,
+// per the tuning), the plain one-launch-per-system FP32 baseline (KHRR_PLAIN)
+// and the FP64 direct sum (KHRR_FP64).
+enum ForceMode { kModeBatched = 0, kModePlain = 1, kModeF64 = 2 };
 
 struct StepGraph {
     cudaGraph_t graph = nullptr;
@@ -137,7 +138,9 @@ struct khrr_ctx {
     khrr::DevBuf<double> pos, vel, acc, post, velt, acct, mass, eps2, phi;
     khrr::DevBuf<float> shadow_buf;  // SoA FP32 shadow, 5 x npad
     khrr::DevBuf<double4> part;
-    khrr::DevBuf<float4> part4;         // the pair kernel's FP32 partials
+    khrr::DevBuf<unsigned long long> fx;  // the pair kernel's fixed-point sums, kFxComps x npad
+    khrr::DevBuf<khrr::FxScale> fx_scale; // their scale per 128-body tile
+    std::vector<khrr::FxScale> fx_scales; // host copy (kept alive until the upload's copies complete)
     khrr::DevBuf<unsigned> queue, errflag;
     khrr::DevBuf<double> cons_blocks, scratch;
     bool uniform = false;
@@ -145,20 +148,21 @@ struct khrr_ctx {
     bool tile_uniform_mass = false;     // every 128-body tile of the layout has one mass
     khrr::DevBuf<float> tile_mass;      // that mass per tile (FP32)
     bool block_uniform_mass = false;    // every pair block has one mass (the pair kernel's block-mass form)
-    int64_t pair_budget = khrr::kPairPartBudget;  // bytes the pair kernel's partials may take
     khrr::PairBlocks pair_blocks;       // the pair kernel's blocks of the layout
     khrr::FieldConsts field{};
     khrr_tuning tuning{128, 4, 128, 0, 1};
-    khrr::ForcePlan plan_batched, plan_plain;
+    khrr::ForcePlan plan_batched, plan_plain, plan_fp64;
     bool predicted = false;
     double pred_dt = 0.0;
-    std::map<std::tuple<uint64_t, bool, bool, bool>, khrr::StepGraph> graphs;
+    std::map<std::tuple<uint64_t, int, bool, bool>, khrr::StepGraph> graphs;  // (dt, mode, phi, compat)
 
     // Kernel-level entry points: their own shadow, partials and plan.
     khrr::DevBuf<float> kshadow, kishadow;
     khrr::DevBuf<double4> kpart;
-    khrr::DevBuf<float4> kpart4;  // the pair kernel's partials (pos_i == pos_j under the pair tuning)
-    khrr::DevBuf<float> ktile_mass;   // their per-tile masses (block-mass form)
+    khrr::DevBuf<unsigned long long> kfx;  // the pair kernel's sums (pos_i == pos_j under the pair tuning)
+    khrr::DevBuf<khrr::FxScale> kscale;    // their tile scales
+    khrr::DevBuf<double> ktile_hmin, ktile_msum;  // classification scratch per tile
+    khrr::DevBuf<float> ktile_mass;   // per-tile masses (block-mass form)
     khrr::DevBuf<unsigned> kflags;    // classification of the caller's arrays
     float kh_uniform = 0.0f;          // 0.5 eps2[0] when the softenings are all equal
     khrr::ForcePlan kplan;
@@ -197,17 +201,23 @@ struct khrr_ctx {
     khrr_status check_device_flag();
     int resident_ctas(const khrr::ForceVariant* v);
     const khrr::ForceVariant* variant(bool unif, bool acc, bool phi) const;
-    bool pair_mode() const;  // the tuning asks for the pair kernel and the layout admits it
-    khrr_status ensure_plan(bool plain);
+    bool pair_mode() const;  // the tuning asks for the pair kernel (any layout of the state admits it)
+    khrr::ForcePlan& plan_for(int mode) {
+        return mode == khrr::kModePlain ? plan_plain : (mode == khrr::kModeF64 ? plan_fp64 : plan_batched);
+    }
+    khrr_status ensure_plan(int mode);
     void drop_graphs();
     khrr::ForceArgs force_args(const khrr::ForcePlan& p, int item_begin, int item_end);
-    khrr_status enqueue_force(bool plain, bool acc, bool phi, bool events);
+    // x: the FP64 positions the forces are wanted at (read by the FP64 kernel;
+    // the FP32 kernels read the shadow packed from them).
+    khrr_status enqueue_force(int mode, bool acc, bool phi, bool events, const double* x);
     khrr::StepArgs step_args(const khrr::ForcePlan& p, double dt);
     khrr::Shadow shadow() { return khrr::shadow_at(shadow_buf.p, npad); }
-    khrr_status enqueue_step(double dt, bool plain, bool phi_now, bool compat);
-    khrr_status get_step_graph(double dt, bool plain, bool phi_now, bool compat, khrr::StepGraph** out);
+    khrr_status enqueue_step(double dt, int mode, bool phi_now, bool compat);
+    khrr_status get_step_graph(double dt, int mode, bool phi_now, bool compat, khrr::StepGraph** out);
     khrr_status timing_pair(cudaEvent_t* e0, cudaEvent_t* e1);
     double pairs_per_pass() const;
+    khrr_status force_mode(int flags, int* mode);  // KHRR_PLAIN / KHRR_FP64 -> ForceMode
     // Mesh-force solver (mesh_api.cpp).
     khrr_status mesh_ensure_layout();
     khrr_status mesh_enqueue_force(const double* x, int iters, int rot0);

@@ -12,8 +12,15 @@
 //   items     the work queue, written on the device by noalloc_items_kernel
 //   part      per-chunk FP64 partial sums, reduced into acc at the end
 // Host code never uses the array's name as an address: the device address is
-// looked up once per device with cudaGetSymbolAddress (with that device
-// current) and passed to the kernels.
+// looked up per device with cudaGetSymbolAddress (with that device current)
+// and passed to the kernels.  A set-up that failed is tried again on the next
+// call; only a successful one is kept.
+//
+// Failure reporting: the call only enqueues work, so a bounded wait that gives
+// up inside the force kernel cannot become its return status.  The final
+// reduce reads the error flag the force kernel raises and then writes NaN to
+// every acc entry instead of the sums, so a caller never gets partial forces
+// that look valid.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -68,36 +75,68 @@ __global__ void noalloc_items_kernel(WorkItem* items, int n, int itile, int spli
 }
 
 struct DeviceSetup {
-    std::once_flag once;
-    cudaError_t err = cudaSuccess;
+    bool ok = false;
     unsigned char* base = nullptr;
     int ctas = 1;
 };
 
 constexpr int kMaxDevices = 64;
 DeviceSetup g_setup[kMaxDevices];
+std::mutex g_setup_mutex;
 
-// Once per device, with that device current: the scratch's device address,
-// the kernel's shared-memory attribute and its resident CTA count.
+// Per device, with that device current: the scratch's device address, the
+// kernel's shared-memory attribute and its resident CTA count.  Kept once it
+// succeeded; after a failure (for instance a first call made inside a stream
+// capture) the next call tries again.
 cudaError_t setup_device(int dev, const ForceVariant* v, DeviceSetup** out) {
     if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
+    std::lock_guard<std::mutex> lock(g_setup_mutex);
     DeviceSetup& s = g_setup[dev];
-    std::call_once(s.once, [&] {
-        void* p = nullptr;
-        s.err = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-        if (s.err != cudaSuccess) return;
-        s.base = static_cast<unsigned char*>(p);
-        s.err = cudaFuncSetAttribute(v->fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     static_cast<int>(v->smem));
-        if (s.err != cudaSuccess) return;
-        int occ = 0, sms = 0;
-        s.err = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, v->fn, v->threads, v->smem);
-        if (s.err != cudaSuccess) return;
-        s.err = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        s.ctas = std::max(1, occ) * std::max(1, sms);
-    });
     *out = &s;
-    return s.err;
+    if (s.ok) return cudaSuccess;
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(v->fn, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(v->smem));
+    if (e != cudaSuccess) return e;
+    int occ = 0, sms = 0;
+    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, v->fn, v->threads, v->smem)) != cudaSuccess) return e;
+    if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
+    s.base = static_cast<unsigned char*>(p);
+    s.ctas = std::max(1, occ) * std::max(1, sms);
+    s.ok = true;
+    return cudaSuccess;
+}
+
+// acc[i] (+)= sum of the body's split partials, in FP64; NaN for every body
+// when the force kernel raised its error flag (a bounded wait gave up, so
+// some partials were never written).
+__global__ void noalloc_reduce_kernel(const double4* __restrict__ part, long long npad, int nslots, int64_t n,
+                                      const unsigned* __restrict__ err, double* __restrict__ acc, int overwrite) {
+    const bool failed = *err != 0u;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        if (failed) {
+            acc[3 * i] = acc[3 * i + 1] = acc[3 * i + 2] = __longlong_as_double(0x7ff8000000000000LL);
+            continue;
+        }
+        double sx = 0.0, sy = 0.0, sz = 0.0;
+        for (int s = 0; s < nslots; ++s) {
+            const double4 p = part[s * npad + i];
+            sx += p.x;
+            sy += p.y;
+            sz += p.z;
+        }
+        if (overwrite) {
+            acc[3 * i] = sx;
+            acc[3 * i + 1] = sy;
+            acc[3 * i + 2] = sz;
+        } else {
+            acc[3 * i] += sx;
+            acc[3 * i + 1] += sy;
+            acc[3 * i + 2] += sz;
+        }
+    }
 }
 
 khrr_status as_status(cudaError_t e) { return e == cudaSuccess ? KHRR_OK : KHRR_ERR_CUDA; }
@@ -153,5 +192,8 @@ extern "C" khrr_status khrr_accel_noalloc(double* acc, const double* pos_i, cons
     a.h_uniform = 0.0f;
     a.err = counters + 1;
     if ((e = launch_force(v, a, std::min(nitems, s->ctas), st)) != cudaSuccess) return as_status(e);
-    return as_status(launch_reduce_partials(part, npad, split, n, acc, nullptr, (flags & KHRR_OVERWRITE) != 0, st));
+    const int rgrid = static_cast<int>(std::min<int64_t>((n + 255) / 256, 148 * 8));
+    noalloc_reduce_kernel<<<rgrid, 256, 0, st>>>(part, npad, split, n, counters + 1, acc,
+                                                 (flags & KHRR_OVERWRITE) != 0 ? 1 : 0);
+    return as_status(cudaGetLastError());
 }

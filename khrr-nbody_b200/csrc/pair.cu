@@ -15,13 +15,17 @@
 // block b itself are evaluated one-sided (every ordered pair once, i side
 // only).  Tiles of J > b are evaluated symmetrically: the i side accumulates
 // in registers, and the reaction on each j body, summed over the CTA's i
-// bodies, is written once as an FP32 partial.
+// bodies, is one FP32 partial added to the body's sums.
 //
-// Partial slots (float4 {ax, ay, az, sum m/r} per [slot][body]).  A body of
-// block B receives the reaction of every block I < B in slot I and one i-side
-// sum per chunk u of its own row in slot B + u; the corrector adds its
-// B + (chunks of row B) slots in FP64.  Every slot is written exactly once per
-// pass: no atomics, and the result is bitwise reproducible.
+// Results: 64-bit fixed-point sums, one accumulator per body and component
+// (ax, ay, az, sum m/r).  Each (i block, symmetric j tile) adds the reactions
+// on the tile's 128 bodies, summed over the CTA's 1024 i bodies, and each item
+// adds the i block's sums over its chunk; a partial is scaled by its tile's
+// power of two, rounded to an integer and added with an integer atomic
+// (red.global.add.u64).  Integer addition is associative, so the totals do
+// not depend on the order in which CTAs finish: the result is bitwise
+// reproducible, and the accumulators take 32 bytes per body, independent of
+// the number of blocks.  The corrector converts them back to FP64.
 //
 // The reaction sum across a warp.  The tile's 128 j bodies form four 32-body
 // sub-chunks, taken two at a time.  At step s (0..31) lane l evaluates body
@@ -30,7 +34,7 @@
 // hands the pair to lane l - 1 (shuffles); after 32 steps lane l holds the
 // reactions of the bodies r = l summed over the warp's 256 i bodies.  The four
 // warps' sums meet in shared memory (double-buffered by tile parity) and one
-// thread per j body adds them and writes the partial.
+// thread per j body adds them and accumulates the partial.
 //
 // Inner loop: packed f32x2 instructions over the two j bodies of a step
 // against one i body (its coordinates duplicated in both lanes once per
@@ -68,6 +72,18 @@ __device__ __forceinline__ void two_sum_into(float& hi, float& lo, float p) {
 }
 
 __device__ __forceinline__ float2 f2(float a, float b) { return make_float2(a, b); }
+
+// A partial (FP32) as a fixed-point integer: times the power of two s,
+// rounded to the nearest integer (exact for |v s| >= 2^24).
+__device__ __forceinline__ long long to_fx(float v, double s) {
+    return __double2ll_rn(static_cast<double>(v) * s);
+}
+
+// Integer atomic add without return (red.global.add.u64): two's complement
+// makes the unsigned add a signed one.
+__device__ __forceinline__ void fx_add(unsigned long long* p, long long v) {
+    atomicAdd(p, static_cast<unsigned long long>(v));
+}
 
 __device__ __forceinline__ float2 shfl2(float2 v, int src) {
     return f2(__shfl_sync(0xffffffffu, v.x, src), __shfl_sync(0xffffffffu, v.y, src));
@@ -348,31 +364,33 @@ __global__ void __launch_bounds__(NT, (pair_min_blocks<F>())) pair_kernel(const 
                     for (int v = 0; v < W; ++v) s += jw[(v * NC + c) * JT + tid];
                     r[c] = s;
                 }
-                float4 o = make_float4(0.f, 0.f, 0.f, 0.f);
-                if (ACC) {
-                    o.x = -mI * r[0];
-                    o.y = -mI * r[1];
-                    o.z = -mI * r[2];
+                const int j = jt0 + tid;
+                if (j < w.real_end) {
+                    const FxScale sc = a.scale[jt0 / JT];
+                    if (ACC) {
+                        fx_add(a.fx + j, to_fx(-mI * r[0], sc.acc));
+                        fx_add(a.fx + a.npad + j, to_fx(-mI * r[1], sc.acc));
+                        fx_add(a.fx + 2 * a.npad + j, to_fx(-mI * r[2], sc.acc));
+                    }
+                    if (PHI) fx_add(a.fx + 3 * a.npad + j, to_fx(mI * r[CP], sc.phi));
                 }
-                if (PHI) o.w = mI * r[CP];
-                a.part[static_cast<long long>(w.slot_j) * a.npad + jt0 + tid] = o;
             }
         }
         consumed += static_cast<unsigned>(ntiles);
 
-        float4* out = a.part + static_cast<long long>(w.slot_i) * a.npad;
+        // The i block's sums over the chunk: high and low parts rounded to
+        // the fixed point separately (the compensation survives).
 #pragma unroll
         for (int k = 0; k < K; ++k) {
             const int i = w.i_begin + k * NT + tid;
-            if (i < w.i_end) {
-                float4 o = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (i < w.real_end) {
+                const FxScale sc = a.scale[w.i_begin / JT + k];
                 if (ACC) {
-                    o.x = RH(0, k) + RL(0, k);
-                    o.y = RH(1, k) + RL(1, k);
-                    o.z = RH(2, k) + RL(2, k);
+#pragma unroll
+                    for (int c = 0; c < 3; ++c)
+                        fx_add(a.fx + c * a.npad + i, to_fx(RH(c, k), sc.acc) + to_fx(RL(c, k), sc.acc));
                 }
-                if (PHI) o.w = RH(CP, k) + RL(CP, k);
-                out[i] = o;
+                if (PHI) fx_add(a.fx + 3 * a.npad + i, to_fx(RH(CP, k), sc.phi) + to_fx(RL(CP, k), sc.phi));
             }
         }
     }
@@ -419,23 +437,38 @@ const PairTable& pair_table() {
     return t;
 }
 
-// Partials -> out[i] (+)= sum over the body's nsplit[i] slots, in FP64
-// (the kernel-level entry points; the state path sums them in the corrector).
-__global__ void reduce_pair_partials_kernel(const float4* __restrict__ part, long long npad,
-                                            const unsigned short* __restrict__ nsplit, int64_t n,
-                                            double* __restrict__ acc, double* __restrict__ phi, int overwrite) {
+// The fixed-point scale of one 128-body tile (FxScale): E = 61 - e with
+// bound < 2^e, for the acceleration bound 0.3849 M / (h_t + h_min) (0.385
+// used) and the potential bound M / sqrt(h_t + h_min).  A bound of zero (no
+// mass) or not finite takes E = 0.
+__host__ __device__ inline double fx_pow2(double bound, bool inverse) {
+    int e = 0;
+    if (bound > 0.0 && bound < 1e300) (void)frexp(bound, &e);
+    else e = 61;
+    int E = 61 - e;
+    E = E < -960 ? -960 : (E > 960 ? 960 : E);
+    return ldexp(1.0, inverse ? -E : E);
+}
+
+__host__ __device__ inline FxScale fx_scale_of(double h_tile_min, double h_sys_min, double mass_sys) {
+    const double H = h_tile_min + h_sys_min;
+    const double ba = 0.385 * mass_sys / H, bp = mass_sys / sqrt(H);
+    return FxScale{fx_pow2(ba, false), fx_pow2(bp, false), fx_pow2(ba, true), fx_pow2(bp, true)};
+}
+
+// Fixed-point sums -> out[i] (+)= sums times the tile's inverse scale, in
+// FP64 (the kernel-level entry points; the state path converts them in the
+// corrector).
+__global__ void reduce_pair_fx_kernel(const unsigned long long* __restrict__ fx, long long npad,
+                                      const FxScale* __restrict__ scale, int64_t n, double* __restrict__ acc,
+                                      double* __restrict__ phi, int overwrite) {
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
          i += (int64_t)gridDim.x * blockDim.x) {
-        double sx = 0.0, sy = 0.0, sz = 0.0, sp = 0.0;
-        const int ns = nsplit[i];
-        for (int s = 0; s < ns; ++s) {
-            const float4 p = part[s * npad + i];
-            sx += static_cast<double>(p.x);
-            sy += static_cast<double>(p.y);
-            sz += static_cast<double>(p.z);
-            sp += static_cast<double>(p.w);
-        }
+        const FxScale sc = scale[i / kPad];
         if (acc) {
+            const double sx = static_cast<double>(static_cast<long long>(fx[i])) * sc.inv_acc;
+            const double sy = static_cast<double>(static_cast<long long>(fx[npad + i])) * sc.inv_acc;
+            const double sz = static_cast<double>(static_cast<long long>(fx[2 * npad + i])) * sc.inv_acc;
             if (overwrite) {
                 acc[3 * i] = sx;
                 acc[3 * i + 1] = sy;
@@ -446,7 +479,10 @@ __global__ void reduce_pair_partials_kernel(const float4* __restrict__ part, lon
                 acc[3 * i + 2] += sz;
             }
         }
-        if (phi) phi[i] = overwrite ? -sp : phi[i] - sp;
+        if (phi) {
+            const double sp = static_cast<double>(static_cast<long long>(fx[3 * npad + i])) * sc.inv_phi;
+            phi[i] = overwrite ? -sp : phi[i] - sp;
+        }
     }
 }
 
@@ -454,38 +490,88 @@ __global__ void reduce_pair_partials_kernel(const float4* __restrict__ part, lon
 // one warp per 128-body tile: tile_mass[t] = the tile's first mass; bit 0 of
 // *flags is cleared unless every body of the tile is real and has the mass of
 // its 1024 block's first body (the block-mass form), bit 1 unless every
-// softening equals eps2[0] (the uniform form).
+// softening equals eps2[0] (the uniform form), bit 2 unless every softening
+// is positive (needed for the fixed-point bounds).  tile_hmin[t] and
+// tile_msum[t] receive the tile's smallest eps2 / 2 and its sum of |m|.
 __global__ void classify_kernel(const double* __restrict__ mass, const double* __restrict__ eps2, int64_t n,
-                                float* __restrict__ tile_mass, unsigned* __restrict__ flags) {
+                                float* __restrict__ tile_mass, double* __restrict__ tile_hmin,
+                                double* __restrict__ tile_msum, unsigned* __restrict__ flags) {
     const int64_t warps = (static_cast<int64_t>(gridDim.x) * blockDim.x) >> 5;
     const int lane = threadIdx.x & 31;
     const int64_t ntiles = (n + kPad - 1) / kPad;
     const double e0 = eps2[0];
     for (int64_t t = (blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x) >> 5; t < ntiles; t += warps) {
         const double mt = mass[t * kPad], mb = mass[(t * kPad / kPairBlock) * kPairBlock];
-        bool same_mass = true, same_eps = true;
+        bool same_mass = true, same_eps = true, pos_eps = true;
+        double hmin = 1e300, msum = 0.0;
 #pragma unroll
         for (int q = 0; q < kPad / 32; ++q) {
             const int64_t i = t * kPad + q * 32 + lane;
             if (i < n) {
-                const double m = mass[i];
+                const double m = mass[i], e = eps2[i];
                 same_mass = same_mass && m == mt && m == mb;
-                same_eps = same_eps && eps2[i] == e0;
+                same_eps = same_eps && e == e0;
+                pos_eps = pos_eps && e > 0.0;
+                hmin = fmin(hmin, 0.5 * e);
+                msum += fabs(m);
             } else {
                 same_mass = false;
             }
         }
         same_mass = __all_sync(0xffffffffu, same_mass);
         same_eps = __all_sync(0xffffffffu, same_eps);
+        pos_eps = __all_sync(0xffffffffu, pos_eps);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            hmin = fmin(hmin, __shfl_xor_sync(0xffffffffu, hmin, o));
+            msum += __shfl_xor_sync(0xffffffffu, msum, o);
+        }
         if (lane == 0) {
             tile_mass[t] = static_cast<float>(mt);
+            tile_hmin[t] = hmin;
+            tile_msum[t] = msum;
             if (!same_mass) atomicAnd(flags, ~1u);
             if (!same_eps) atomicAnd(flags, ~2u);
+            if (!pos_eps) atomicAnd(flags, ~4u);
         }
     }
 }
 
+// One CTA: the system's total |m| (tile sums added in tile order, so the
+// bound and hence the scales are the same on every call) and smallest h,
+// then every tile's scale.
+__global__ void fx_scales_kernel(const double* __restrict__ tile_hmin, const double* __restrict__ tile_msum,
+                                 int64_t ntiles, FxScale* __restrict__ scale) {
+    __shared__ double s_m[256], s_h[256];
+    double m = 0.0, h = 1e300;
+    const int64_t per = (ntiles + blockDim.x - 1) / blockDim.x;
+    const int64_t t0 = threadIdx.x * per, t1 = t0 + per < ntiles ? t0 + per : ntiles;
+    for (int64_t t = t0; t < t1; ++t) {
+        m += tile_msum[t];
+        h = fmin(h, tile_hmin[t]);
+    }
+    s_m[threadIdx.x] = m;
+    s_h[threadIdx.x] = h;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double M = 0.0, Hm = 1e300;
+        for (int k = 0; k < blockDim.x; ++k) {
+            M += s_m[k];
+            Hm = fmin(Hm, s_h[k]);
+        }
+        s_m[0] = M;
+        s_h[0] = Hm;
+    }
+    __syncthreads();
+    const double M = s_m[0], Hm = s_h[0];
+    for (int64_t t = threadIdx.x; t < ntiles; t += blockDim.x) scale[t] = fx_scale_of(tile_hmin[t], Hm, M);
+}
+
 }  // namespace
+
+FxScale fx_scale(double h_tile_min, double h_sys_min, double mass_sys) {
+    return fx_scale_of(h_tile_min, h_sys_min, mass_sys);
+}
 
 int pair_variant_count() { return pair_table().n; }
 
@@ -502,23 +588,25 @@ const ForceVariant* find_pair_variant(bool unif, bool acc, bool phi, bool block_
     return nullptr;
 }
 
-cudaError_t launch_reduce_pair_partials(const float4* part, long long npad, const unsigned short* nsplit, int64_t n,
-                                       double* acc, double* phi, bool overwrite, cudaStream_t s) {
+cudaError_t launch_reduce_pair_fx(const unsigned long long* fx, long long npad, const FxScale* scale, int64_t n,
+                                  double* acc, double* phi, bool overwrite, cudaStream_t s) {
     int64_t g = (n + 255) / 256;
     if (g > 148 * 32) g = 148 * 32;
     if (g < 1) g = 1;
-    reduce_pair_partials_kernel<<<static_cast<unsigned>(g), 256, 0, s>>>(part, npad, nsplit, n, acc, phi,
-                                                                         overwrite ? 1 : 0);
+    reduce_pair_fx_kernel<<<static_cast<unsigned>(g), 256, 0, s>>>(fx, npad, scale, n, acc, phi, overwrite ? 1 : 0);
     return cudaGetLastError();
 }
 
-cudaError_t launch_classify(const double* mass, const double* eps2, int64_t n, float* tile_mass, unsigned* flags,
-                            cudaStream_t s) {
+cudaError_t launch_classify(const double* mass, const double* eps2, int64_t n, float* tile_mass, double* tile_hmin,
+                            double* tile_msum, FxScale* scale, unsigned* flags, cudaStream_t s) {
     const int64_t ntiles = (n + kPad - 1) / kPad;
     int64_t g = (ntiles * 32 + 255) / 256;
     if (g > 148 * 16) g = 148 * 16;
     if (g < 1) g = 1;
-    classify_kernel<<<static_cast<unsigned>(g), 256, 0, s>>>(mass, eps2, n, tile_mass, flags);
+    classify_kernel<<<static_cast<unsigned>(g), 256, 0, s>>>(mass, eps2, n, tile_mass, tile_hmin, tile_msum, flags);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    fx_scales_kernel<<<1, 256, 0, s>>>(tile_hmin, tile_msum, ntiles, scale);
     return cudaGetLastError();
 }
 

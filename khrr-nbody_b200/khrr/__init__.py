@@ -22,6 +22,7 @@ COMPAT_ACCUMULATE = 4
 PLAIN = 8
 OVERWRITE = 16
 MESH = 32
+FP64 = 64
 ASSIGN_NGP = 0
 ASSIGN_CIC = 1
 

@@ -1,9 +1,9 @@
 """The symmetric pair kernel's work plan, checked on the CPU: every ordered
 pair of 128-body tiles of a system evaluated exactly once (none across
-systems), every partial slot below a real body's count written exactly once,
-none above it, and (equal-mass runs) every block of one mass, at most 1024
-bodies (tests/pair_plan_check.cpp replays the items against plan_pair_items
-in libkhrr.so; no device work)."""
+systems), sums accumulated for every real body and for no ghost, and
+(equal-mass runs) every block of one mass, at most 1024 bodies
+(tests/pair_plan_check.cpp replays the items against plan_pair_items in
+libkhrr.so; no device work)."""
 import os
 import subprocess
 
@@ -42,7 +42,7 @@ LAYOUTS = [
 
 
 @pytest.mark.parametrize("label,blocks,ctas,chunk,sizes", LAYOUTS, ids=[x[0] for x in LAYOUTS])
-def test_pair_plan_covers_every_pair_and_slot_once(checker, label, blocks, ctas, chunk, sizes):
+def test_pair_plan_covers_every_pair_once(checker, label, blocks, ctas, chunk, sizes):
     r = subprocess.run([str(checker), blocks, str(ctas), str(chunk)] + [str(n) for n in sizes],
                        capture_output=True, text=True, timeout=300)
     assert r.returncode == 0 and r.stdout.startswith("ok"), r.stdout + r.stderr
