@@ -257,9 +257,11 @@ int64_t scan_scratch_ints(int64_t ncells);
 // reference's start_id (total of earlier 512-cell blocks).  pair: count points
 // at {count, start_id} pairs and the starts go to the .start_id fields (16-byte
 // aligned); else counts and starts are plain int arrays (start 16-byte
-// aligned).  scratch: scan_scratch_ints(ncells) ints.
+// aligned).  scratch: scan_scratch_ints(ncells) ints (zeroed by the call).
+// The scan is one launch with bounded waits between its CTAs; a wait that
+// gives up raises kErrTimeout in *err.
 cudaError_t launch_scan(int* count, bool pair, int64_t ncells, int* maxpbc, int* start, bool ref_view, int* scratch,
-                        cudaStream_t s);
+                        unsigned* err, cudaStream_t s);
 cudaError_t launch_cell_phi(const double* phi, const int2* pci, const int* count, int cstride, int64_t n,
                             double* cell_phi, cudaStream_t s);
 cudaError_t launch_wave_f64(double* phi_new, const double* phi, const double* phi_old, const double* mass,

@@ -181,7 +181,7 @@ khrr_status khrr_compute_prefix_sums(khrr_ctx* c, int* cell_info, int* max_pbc, 
     khrr_status st = c->cuda(c->mtmp.ensure(static_cast<size_t>(scan_scratch_ints(ncells))), "alloc");
     if (st != KHRR_OK) return st;
     return c->cuda(launch_scan(cell_info, true, ncells, max_pbc, nullptr, mode == KHRR_SCAN_REFERENCE, c->mtmp.p,
-                               c->stream),
+                               c->errflag.p, c->stream),
                    "prefix sums");
 }
 
@@ -251,7 +251,8 @@ khrr_status khrr_bin(khrr_ctx* c, const khrr_mesh* mesh, int* cell_id, int* id_i
             return st;
     }
     if ((st = c->cuda(c->mscan.ensure(static_cast<size_t>(scan_scratch_ints(C))), "alloc")) != KHRR_OK) return st;
-    if ((st = c->cuda(launch_scan(c->mcount.p, false, C, c->maxpbc.p, c->mstart.p, false, c->mscan.p, s), "scan")) !=
+    if ((st = c->cuda(launch_scan(c->mcount.p, false, C, c->maxpbc.p, c->mstart.p, false, c->mscan.p, c->errflag.p, s),
+                      "scan")) !=
         KHRR_OK)
         return st;
     c->mesh = g;

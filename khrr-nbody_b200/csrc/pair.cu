@@ -220,8 +220,12 @@ __device__ __forceinline__ void pair_tile(const float* __restrict__ tile, float*
 // ms per pass at 786k bodies against 178 ms at two); the other force +
 // potential variants carry per-body masses or softenings as well and run at
 // two rather than spill.
+#ifndef KHRR_PAIR_ACC_CTAS
+#define KHRR_PAIR_ACC_CTAS 3
+#endif
 template <unsigned F>
 constexpr int pair_min_blocks() {
+    if ((F & kAcc) && !(F & kPhi)) return KHRR_PAIR_ACC_CTAS;
     return ((F & kAcc) && (F & kPhi) && !((F & kUnif) && (F & kBMass))) ? 2 : 3;
 }
 
