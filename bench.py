@@ -866,11 +866,11 @@ def run_khrr(args):
         "roofline": {"bound": "fp32", "kernel": "pair_kernel" if pair_kernel else "force_kernel",
                      "achieved": achieved, "peak": peak_tflops,
                      "unit": "TFLOP/s", "frac": achieved / peak_tflops,
-                     # DRAM read+write of one force launch from ncu captures: the
-                     # pair kernel's 6.09 GB at 786,432 bodies (its FP32 partial
-                     # slots, ~n x blocks / 2 of them) scaled by n^2; the one-sided
-                     # kernel's 2.80 MB at 131,072 (the shadow, once) by n.
-                     "traffic": 6.09e9 * (n / 786432) ** 2 if pair_kernel else 2.80e6 * n / 131072,
+                     # DRAM read+write of one force launch from ncu captures at
+                     # 131,072 bodies, scaled by n (both stream the shadow once
+                     # into L2; the pair kernel's fixed-point sums stay in L2):
+                     # pair kernel 5.09 MB, one-sided kernel 2.80 MB.
+                     "traffic": (5.09e6 if pair_kernel else 2.80e6) * n / 131072,
                      "flops_per_pair": FLOPS_PER_PAIR, "pairs_per_launch": pairs_timed / max(launches, 1),
                      "executed": {"tflops": executed, "frac": executed / peak_tflops,
                                   "flops_per_launch": force_flops(n, pair_kernel),
