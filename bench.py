@@ -70,8 +70,10 @@ def parse():
     ap.add_argument("--no-configs", action="store_true",
                     help="skip the legs of the other configurations (small galaxy on GPU and host, encounter on "
                          "the mesh path, two-million-body system)")
-    ap.add_argument("--drift-steps", type=int, default=100,
-                    help="steps of the FP32-vs-FP64 precision run at the workload's size (0 = skip)")
+    ap.add_argument("--drift-steps", type=int, default=1000,
+                    help="steps of the FP32 run of the precision leg at the workload's size (0 = skip the leg)")
+    ap.add_argument("--drift-fp64-steps", type=int, default=100,
+                    help="steps of its FP64 comparator run (the drifts are compared after these)")
     ap.add_argument("--mesh-max-iter", type=int, default=0, help="cap on wave iterations (0 = to tolerance)")
     ap.add_argument("--n-stars", type=int, default=N_STARS)
     ap.add_argument("--n-dm", type=int, default=N_DM)
@@ -472,7 +474,7 @@ def drift_vs_fp64_leg(khrr, ctx, torch, pos, vel, mass, eps2, steps, every=10, d
         ctx.forces(khrr.ACC | khrr.PHI | flags)
         log = [ctx.conservation()]
         ms = 0.0
-        for _ in range(nst // every):
+        for k in range(nst // every):
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record(s)
             ctx.step(dt, every, flags | khrr.PHI)
@@ -480,8 +482,9 @@ def drift_vs_fp64_leg(khrr, ctx, torch, pos, vel, mass, eps2, steps, every=10, d
             e1.synchronize()
             ms += e0.elapsed_time(e1)
             log.append(ctx.conservation())
+            if (k + 1) * every == min(steps, fp64_steps):
+                final[label] = ctx.download(vel=False, acc=False, phi=False)["pos"]
         logs[label] = log
-        final[label] = ctx.download(vel=False, acc=False, phi=False)["pos"]
         out[label + "_ms_per_step"] = ms / max(nst, 1)
         out[label + "_interactions_per_s"] = float(len(mass)) ** 2 / (ms / max(nst, 1) * 1e-3)
         out[label + "_energy_rel_log"] = _relative(log, "E")
@@ -496,8 +499,10 @@ def drift_vs_fp64_leg(khrr, ctx, torch, pos, vel, mass, eps2, steps, every=10, d
                 "lz_rel": abs(l32) if l32 is not None else None,
                 "lz_rel_fp64": abs(l64) if l64 is not None else None,
                 "lz_ratio": abs(l32) / abs(l64) if l32 is not None and l64 else None})
-    if steps == fp64_steps:
-        out["max_dx_vs_fp64"] = float(np.abs(final["fp32"] - final["fp64"]).max())
+    out["max_dx_vs_fp64"] = float(np.abs(final["fp32"] - final["fp64"]).max())
+    if steps != fp64_steps:
+        out["fp32_energy_rel_final"] = abs(out["fp32_energy_rel_log"][-1])
+        out["fp32_lz_rel_final"] = abs(out["fp32_lz_rel_log"][-1]) if out["fp32_lz_rel_log"][-1] is not None else None
     return out
 
 
@@ -824,7 +829,8 @@ def run_khrr(args):
     # the precision contract at this size: FP32 (tuned kernel) vs FP64 runs
     drift64 = None
     if rank == 0 and args.drift_steps > 0:
-        drift64 = drift_vs_fp64_leg(khrr, ctx, torch, pos, vel, mass, eps2, args.drift_steps)
+        drift64 = drift_vs_fp64_leg(khrr, ctx, torch, pos, vel, mass, eps2, args.drift_steps,
+                                    fp64_steps=min(args.drift_fp64_steps, args.drift_steps))
     ens = None
     if not args.no_ensemble and rank == 0:
         ens = ensemble_leg(khrr, local, torch)

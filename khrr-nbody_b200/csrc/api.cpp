@@ -709,12 +709,30 @@ khrr_status khrr_upload_state(khrr_ctx* c, int64_t n, const double* pos, const d
     if (off[0] != 0 || off[nsys] != n) return c->fail(KHRR_ERR_INVALID_ARG, "system offsets must span [0, n]");
     for (int k = 0; k < nsys; ++k)
         if (off[k + 1] <= off[k]) return c->fail(KHRR_ERR_INVALID_ARG, "system %d is empty", k);
-    // One pass: every softening positive, and whether they are all equal.
+    // One pass over the bodies: every softening positive, whether they are
+    // all equal, and per system its total |mass| and smallest h = eps2 / 2 and
+    // per 128-body tile of it the smallest h (the fixed-point scales below).
     bool uniform_new = true;
-    for (int64_t i = 0; i < n; ++i) {
-        const double e = eps2[i];
-        if (!(e > 0.0)) return c->fail(KHRR_ERR_INVALID_ARG, "eps2[%lld] must be > 0", (long long)i);
-        uniform_new = uniform_new && e == eps2[0];
+    std::vector<double> sys_msum(static_cast<size_t>(nsys), 0.0), sys_hmin(static_cast<size_t>(nsys), 1e300);
+    std::vector<double> tile_hmin;
+    tile_hmin.reserve(static_cast<size_t>(n / kPad + nsys));
+    for (int k = 0; k < nsys; ++k) {
+        double msum = 0.0, hsys = 1e300;
+        for (int64_t b = off[k]; b < off[k + 1]; b += kPad) {
+            const int64_t e_end = std::min(b + kPad, off[k + 1]);
+            double ht = 1e300;
+            for (int64_t i = b; i < e_end; ++i) {
+                const double e = eps2[i];
+                if (!(e > 0.0)) return c->fail(KHRR_ERR_INVALID_ARG, "eps2[%lld] must be > 0", (long long)i);
+                uniform_new = uniform_new && e == eps2[0];
+                ht = std::min(ht, 0.5 * e);
+                msum += std::fabs(mass[i]);
+            }
+            hsys = std::min(hsys, ht);
+            tile_hmin.push_back(ht);
+        }
+        sys_msum[k] = msum;
+        sys_hmin[k] = hsys;
     }
     cudaSetDevice(c->device);
     // Same layout as the current state: plans and captured graphs stay valid.
@@ -785,18 +803,9 @@ khrr_status khrr_upload_state(khrr_ctx* c, int64_t n, const double* pos, const d
     // tile's smallest h = eps2 / 2, its system's smallest h and total |mass|
     // (real bodies; ghosts carry the system's first softening and no sums).
     c->fx_scales.assign(tm.size(), FxScale{1.0, 1.0, 1.0, 1.0});
-    for (int k = 0; k < nsys; ++k) {
-        double msum = 0.0, hsys = 1e300;
-        for (int64_t i = off[k]; i < off[k + 1]; ++i) {
-            msum += std::fabs(mass[i]);
-            hsys = std::min(hsys, 0.5 * eps2[i]);
-        }
-        for (int64_t b = 0; b < c->cnt[k]; b += kPad) {
-            double ht = 1e300;
-            for (int64_t i = off[k] + b; i < std::min(off[k] + b + kPad, off[k + 1]); ++i) ht = std::min(ht, 0.5 * eps2[i]);
-            c->fx_scales[(c->poff[k] + b) / kPad] = fx_scale(ht, hsys, msum);
-        }
-    }
+    for (int k = 0, t = 0; k < nsys; ++k)
+        for (int64_t b = 0; b < c->cnt[k]; b += kPad, ++t)
+            c->fx_scales[(c->poff[k] + b) / kPad] = fx_scale(tile_hmin[t], sys_hmin[k], sys_msum[k]);
     if ((st = c->cuda(c->fx_scale.ensure(tm.size()), "alloc tile scales")) != KHRR_OK) return st;
     if ((st = c->cuda(cudaMemcpyAsync(c->fx_scale.p, c->fx_scales.data(), tm.size() * sizeof(FxScale),
                                       cudaMemcpyHostToDevice, s),
