@@ -244,7 +244,18 @@ struct WaveF32 {
     const float* sx;
     const float* sy;
     const float* sz;
+    // Optional occupancy of the FP32 mass (launch_to_float_flags): one byte
+    // per (z block of wave_zblock(nx) planes, y, x) column segment, nonzero
+    // when any of its cells has mass.  The stencil skips the mass loads of
+    // empty segments (their mass is +0.0f, so the bits do not change).
+    const unsigned char* mflag;
 };
+// z planes per thread of the FP32 stencil on an nx^3 mesh (the occupancy
+// flags' z block).
+inline int wave_zblock(int nx) { return nx >= 192 ? 8 : 4; }
+// cell_mass (FP64) -> mass (FP32) on an nx^3 mesh, with the occupancy flags
+// ((nx / wave_zblock(nx), rounded up) x nx x nx bytes).
+cudaError_t launch_to_float_flags(const double* src, float* dst, int nx, unsigned char* flags, cudaStream_t s);
 // Bins n bodies: slots from counter (stride counter_stride); count2 (may be
 // NULL) receives the same counts; cell_mass (may be NULL) the mass deposit.
 cudaError_t launch_assign(const double* pos, int64_t n, const MeshGeom& m, int2* pci, int* counter,

@@ -451,6 +451,8 @@ __global__ void __launch_bounds__(kWX * kWY) wave_f32_kernel(float* __restrict__
         const int64_t dym = iy > 0 ? sy : 0, dyp = iy < NX - 1 ? sy : 0;
         float c[kWZ + 2];  // phi at z = zb - 1 .. zb + kWZ (clamped into the mesh)
         float xm[kWZ], xp[kWZ], ym[kWZ], yp[kWZ], po[kWZ], ms[kWZ];
+        // Segments without mass hold +0.0f: their loads are skipped.
+        const bool massive = !W.mflag || W.mflag[static_cast<int64_t>(blockIdx.z) * sz + col] != 0;
 #pragma unroll
         for (int u = 0; u < kWZ + 2; ++u) {
             const int z = min(max(zb - 1 + u, 0), NX - 1);
@@ -464,7 +466,7 @@ __global__ void __launch_bounds__(kWX * kWY) wave_f32_kernel(float* __restrict__
             ym[u] = phi[at - dym];
             yp[u] = phi[at + dyp];
             po[u] = phi_old[at];
-            ms[u] = mass[at];
+            ms[u] = massive ? mass[at] : 0.0f;
         }
         const bool edge_xy = ix == 0 || ix == NX - 1 || iy == 0 || iy == NX - 1;
         const float sxy = (W.diss_base + W.sx[ix]) + W.sy[iy];
@@ -989,6 +991,26 @@ __global__ void acc_field_f32_kernel(double* __restrict__ cell_acc, const float*
     cell_acc[3 * at + 2] = d[2] * coef;
 }
 
+// One thread per (z block, y, x) segment of wz cells: FP32 copies and the
+// segment's occupancy byte.
+__global__ void to_float_flags_kernel(const double* __restrict__ src, float* __restrict__ dst, int nx, int wz,
+                                      unsigned char* __restrict__ flags) {
+    const int64_t plane = static_cast<int64_t>(nx) * nx;
+    const int64_t nseg = static_cast<int64_t>((nx + wz - 1) / wz) * plane;
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < nseg; t += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t zb = t / plane, col = t % plane;
+        bool any = false;
+        for (int u = 0; u < wz; ++u) {
+            const int64_t z = zb * wz + u;
+            if (z >= nx) break;
+            const float v = static_cast<float>(src[z * plane + col]);
+            dst[z * plane + col] = v;
+            any = any || v != 0.0f;
+        }
+        flags[t] = any ? 1 : 0;
+    }
+}
+
 __global__ void to_float_kernel(const double* __restrict__ src, float* __restrict__ dst, int64_t n) {
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
         dst[i] = static_cast<float>(src[i]);
@@ -1069,7 +1091,7 @@ cudaError_t launch_wave_f32(float* phi_new, const float* phi, const float* phi_o
     attr[0].val.programmaticStreamSerializationAllowed = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    if (w.nx >= 192) {
+    if (wave_zblock(w.nx) == 8) {
         cfg.gridDim = dim3((w.nx + kWX - 1) / kWX, (w.nx + kWY - 1) / kWY, (w.nx + 7) / 8);
         return cudaLaunchKernelEx(&cfg, wave_f32_kernel<8>, phi_new, phi, phi_old, mass, w, resid);
     }
@@ -1154,6 +1176,13 @@ cudaError_t launch_apply(double* pacc, double* pval, const double* cacc, const d
 cudaError_t launch_to_float(const double* src, float* dst, int64_t n, cudaStream_t s) {
     if (n < 1) return cudaSuccess;
     to_float_kernel<<<grid_for(n, 256), 256, 0, s>>>(src, dst, n);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_to_float_flags(const double* src, float* dst, int nx, unsigned char* flags, cudaStream_t s) {
+    const int wz = wave_zblock(nx);
+    const int64_t nseg = static_cast<int64_t>((nx + wz - 1) / wz) * nx * nx;
+    to_float_flags_kernel<<<grid_for(nseg, 256), 256, 0, s>>>(src, dst, nx, wz, flags);
     return cudaGetLastError();
 }
 
