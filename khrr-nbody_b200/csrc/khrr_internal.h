@@ -244,18 +244,7 @@ struct WaveF32 {
     const float* sx;
     const float* sy;
     const float* sz;
-    // Optional occupancy of the FP32 mass (launch_to_float_flags): one byte
-    // per (z block of wave_zblock(nx) planes, y, x) column segment, nonzero
-    // when any of its cells has mass.  The stencil skips the mass loads of
-    // empty segments (their mass is +0.0f, so the bits do not change).
-    const unsigned char* mflag;
 };
-// z planes per thread of the FP32 stencil on an nx^3 mesh (the occupancy
-// flags' z block).
-inline int wave_zblock(int nx) { return nx >= 192 ? 8 : 4; }
-// cell_mass (FP64) -> mass (FP32) on an nx^3 mesh, with the occupancy flags
-// ((nx / wave_zblock(nx), rounded up) x nx x nx bytes).
-cudaError_t launch_to_float_flags(const double* src, float* dst, int nx, unsigned char* flags, cudaStream_t s);
 // Bins n bodies: slots from counter (stride counter_stride); count2 (may be
 // NULL) receives the same counts; cell_mass (may be NULL) the mass deposit.
 cudaError_t launch_assign(const double* pos, int64_t n, const MeshGeom& m, int2* pci, int* counter,
@@ -268,11 +257,9 @@ int64_t scan_scratch_ints(int64_t ncells);
 // reference's start_id (total of earlier 512-cell blocks).  pair: count points
 // at {count, start_id} pairs and the starts go to the .start_id fields (16-byte
 // aligned); else counts and starts are plain int arrays (start 16-byte
-// aligned).  scratch: scan_scratch_ints(ncells) ints (zeroed by the call).
-// The scan is one launch with bounded waits between its CTAs; a wait that
-// gives up raises kErrTimeout in *err.
+// aligned).  scratch: scan_scratch_ints(ncells) ints.
 cudaError_t launch_scan(int* count, bool pair, int64_t ncells, int* maxpbc, int* start, bool ref_view, int* scratch,
-                        unsigned* err, cudaStream_t s);
+                        cudaStream_t s);
 cudaError_t launch_cell_phi(const double* phi, const int2* pci, const int* count, int cstride, int64_t n,
                             double* cell_phi, cudaStream_t s);
 cudaError_t launch_wave_f64(double* phi_new, const double* phi, const double* phi_old, const double* mass,

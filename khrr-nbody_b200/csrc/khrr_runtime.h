@@ -107,7 +107,6 @@ struct MeshSolver {
     int64_t cells = 0;
     DevBuf<double> cell_mass, phi64, cell_acc;  // C, 4 C (field ring), 3 C
     DevBuf<float> mass32, phi32, tab;           // C, 4 C (field ring), 3 nx
-    DevBuf<unsigned char> mflag;                // occupancy of mass32 per z-block segment (<= C)
     DevBuf<int2> pci;                           // npad
     DevBuf<double4> part;                       // npad: {acc, -phi} per body
     WaveMaps maps;                              // tensor maps of phi32 / mass32
@@ -179,7 +178,6 @@ struct khrr_ctx {
     khrr::DevBuf<double> cell_mass, cell_phi, wave_resid;
     int64_t cell_phi_cells = 0;                          // mesh size the cell_phi sums belong to
     khrr::DevBuf<float> wave_phi, wave_mass, wave_tab;   // 4 C (field ring), C, 3 nx
-    khrr::DevBuf<unsigned char> wave_mflag;              // occupancy of wave_mass per z-block segment (<= C)
     int wave_nx = 0;
     int wave_rot = khrr::kRingStart;                     // ring state: 4 * (phi^{n-1} buffer) + phi^n buffer
     khrr::WaveMaps wave_maps;                            // tensor maps of wave_phi / wave_mass

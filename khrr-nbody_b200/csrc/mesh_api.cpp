@@ -181,7 +181,7 @@ khrr_status khrr_compute_prefix_sums(khrr_ctx* c, int* cell_info, int* max_pbc, 
     khrr_status st = c->cuda(c->mtmp.ensure(static_cast<size_t>(scan_scratch_ints(ncells))), "alloc");
     if (st != KHRR_OK) return st;
     return c->cuda(launch_scan(cell_info, true, ncells, max_pbc, nullptr, mode == KHRR_SCAN_REFERENCE, c->mtmp.p,
-                               c->errflag.p, c->stream),
+                               c->stream),
                    "prefix sums");
 }
 
@@ -251,8 +251,7 @@ khrr_status khrr_bin(khrr_ctx* c, const khrr_mesh* mesh, int* cell_id, int* id_i
             return st;
     }
     if ((st = c->cuda(c->mscan.ensure(static_cast<size_t>(scan_scratch_ints(C))), "alloc")) != KHRR_OK) return st;
-    if ((st = c->cuda(launch_scan(c->mcount.p, false, C, c->maxpbc.p, c->mstart.p, false, c->mscan.p, c->errflag.p, s),
-                      "scan")) !=
+    if ((st = c->cuda(launch_scan(c->mcount.p, false, C, c->maxpbc.p, c->mstart.p, false, c->mscan.p, s), "scan")) !=
         KHRR_OK)
         return st;
     c->mesh = g;
@@ -341,7 +340,6 @@ khrr_status khrr_wave_solve(khrr_ctx* c, const khrr_wave_params* p, double tol, 
         c->wave_graphs.clear();
         if ((st = c->cuda(c->wave_phi.ensure(4 * cz), "alloc")) != KHRR_OK) return st;
         if ((st = c->cuda(c->wave_mass.ensure(cz), "alloc")) != KHRR_OK) return st;
-        if ((st = c->cuda(c->wave_mflag.ensure(cz), "alloc")) != KHRR_OK) return st;
         if ((st = c->cuda(c->wave_tab.ensure(3 * static_cast<size_t>(nx)), "alloc")) != KHRR_OK) return st;
         if ((st = c->cuda(c->wave_resid.ensure(2), "alloc")) != KHRR_OK) return st;
         c->wave_nx = p->nx;
@@ -352,15 +350,12 @@ khrr_status khrr_wave_solve(khrr_ctx* c, const khrr_wave_params* p, double tol, 
     if ((st = c->cuda(cudaMemcpyAsync(c->wave_tab.p, tab.data(), tab.size() * sizeof(float), cudaMemcpyHostToDevice, s),
                       "upload")) != KHRR_OK)
         return st;
-    if ((st = c->cuda(launch_to_float_flags(c->cell_mass.p, c->wave_mass.p, nx, c->wave_mflag.p, s),
-                      "mass to float")) != KHRR_OK)
-        return st;
+    if ((st = c->cuda(launch_to_float(c->cell_mass.p, c->wave_mass.p, C, s), "mass to float")) != KHRR_OK) return st;
     if (cold || !c->wave_warm) {
         cudaMemsetAsync(c->wave_phi.p, 0, 4 * cz * sizeof(float), s);
         c->wave_rot = kRingStart;
     }
-    WaveF32 w = wave_f32(p, c->wave_tab.p);
-    w.mflag = c->wave_mflag.p;
+    const WaveF32 w = wave_f32(p, c->wave_tab.p);
     make_wave_maps(&c->wave_maps, c->wave_phi.p, c->wave_mass.p, p->nx);
     // Graph of one chunk of `check_every` iterations starting at a ring state;
     // the last iteration of the chunk reduces the residual.
@@ -515,7 +510,6 @@ khrr_status khrr_set_mesh_solver(khrr_ctx* c, const khrr_mesh_solver* p) {
     } else {
         if ((st = c->cuda(M.phi32.ensure(4 * cz), "alloc")) != KHRR_OK) return st;
         if ((st = c->cuda(M.mass32.ensure(cz), "alloc")) != KHRR_OK) return st;
-        if ((st = c->cuda(M.mflag.ensure(cz), "alloc")) != KHRR_OK) return st;
         if ((st = c->cuda(M.tab.ensure(3 * static_cast<size_t>(nx)), "alloc")) != KHRR_OK) return st;
         std::vector<float> tab;
         sponge_tables(&p->wave, tab);
@@ -623,10 +617,8 @@ khrr_status khrr_ctx::mesh_enqueue_force(const double* x, int iters, int rot0) {
         }
         return KHRR_OK;
     }
-    if ((st = cuda(launch_to_float_flags(M.cell_mass.p, M.mass32.p, nx, M.mflag.p, s), "mass to float")) != KHRR_OK)
-        return st;
-    WaveF32 w = wave_f32(&P.wave, M.tab.p);
-    w.mflag = M.mflag.p;
+    if ((st = cuda(launch_to_float(M.cell_mass.p, M.mass32.p, M.cells, s), "mass to float")) != KHRR_OK) return st;
+    const WaveF32 w = wave_f32(&P.wave, M.tab.p);
     if ((st = cuda(enqueue_wave_f32(M.phi32.p, M.cells, M.mass32.p, w, iters, r, nullptr, s, &M.maps, errflag.p),
                    "wave")) != KHRR_OK)
         return st;
