@@ -27,25 +27,6 @@
 namespace khrr {
 namespace {
 
-// r^-1 of the pair: CUDA's rsqrt (0), or the rsqrt.approx.f64 seed refined
-// by one third-order (Halley) step and one Newton step (1).
-#ifndef KHRR_F64_RSQRT
-#define KHRR_F64_RSQRT 0
-#endif
-
-__device__ __forceinline__ double inv_sqrt(double x) {
-#if KHRR_F64_RSQRT
-    double y;
-    asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
-    double e = fma(-x * y, y, 1.0);
-    y = fma(y * e, fma(0.375, e, 0.5), y);
-    e = fma(-x * y, y, 1.0);
-    return fma(0.5 * y, e, y);
-#else
-    return rsqrt(x);
-#endif
-}
-
 constexpr int NT = 128;  // threads per CTA
 constexpr int K = 4;     // i bodies per thread
 constexpr int JT = 128;  // j bodies per shared-memory tile
@@ -106,7 +87,7 @@ __global__ void __launch_bounds__(NT, 4) fp64_force_kernel(const F64Args a) {
                     r2 = fma(dx, dx, r2);
                     r2 = fma(dy, dy, r2);
                     r2 = fma(dz, dz, r2);
-                    const double inv = inv_sqrt(r2);
+                    const double inv = rsqrt(r2);
                     if (ACC) {
                         const double k3 = mj * (inv * inv * inv);
                         ax[k] = fma(dx, k3, ax[k]);
