@@ -12,9 +12,9 @@
 // the id iz*gx*gy + iy*gz + ix).  Slots and the mass deposit come from one
 // atomic each per body (fused in one pass over the bodies).
 //
-// Scan: 4096-cell tiles in three launches (block and tile totals with 16-byte
-// loads, one CTA scanning the tile totals, per-tile downsweep with 16-byte
-// stores).  The inclusive block-total scan is exactly the reference's maxPBC
+// Scan: 4096-cell tiles in three launches (tile totals with 16-byte loads,
+// one CTA scanning the tile totals, per-tile downsweep with 16-byte stores
+// that also yields the 512-cell block totals).  The inclusive block-total scan is exactly the reference's maxPBC
 // array, and the reference's start_id (the total of earlier 512-cell blocks,
 // its in-block scan being discarded) is read off it; the true exclusive scan
 // is the other mode.  (A one-launch scan with decoupled look-back measured
@@ -166,10 +166,10 @@ __device__ __forceinline__ void load8(const int* __restrict__ count, int64_t c0,
     }
 }
 
-// K1: per tile, the totals of its 512-cell blocks and of the tile.
+// K1: per tile, the total of its counts.
 template <bool PAIR>
 __global__ void __launch_bounds__(kScanThreads) scan_totals_kernel(const int* __restrict__ count, int64_t ncells,
-                                                                   int* __restrict__ block_tot, int* __restrict__ tile_tot) {
+                                                                   int* __restrict__ tile_tot) {
     const int64_t t = blockIdx.x;
     const int tid = threadIdx.x;
     int v[kScanPer];
@@ -181,10 +181,6 @@ __global__ void __launch_bounds__(kScanThreads) scan_totals_kernel(const int* __
     __shared__ int ws[kScanThreads / 32];
     if ((tid & 31) == 0) ws[tid >> 5] = s;
     __syncthreads();
-    if (tid < kBlocksPerTile) {
-        const int64_t b = t * kBlocksPerTile + tid;
-        if (b * kRefBlock < ncells) block_tot[b] = ws[2 * tid] + ws[2 * tid + 1];
-    }
     if (tid == 0) {
         int tot = 0;
 #pragma unroll
@@ -220,16 +216,17 @@ __global__ void __launch_bounds__(1024) scan_tiles_kernel(int* __restrict__ tile
 }
 
 // K3: per tile, maxPBC for its blocks (inclusive block-total scan), the true
-// exclusive start of every cell and/or the reference's start_id view.
+// exclusive start of every cell and/or the reference's start_id view, all
+// from the tile's own scan and its offset (no other global reads).
 template <bool PAIR>
 __global__ void __launch_bounds__(kScanThreads) scan_downsweep_kernel(int* __restrict__ count, int64_t ncells,
-                                                                      const int* __restrict__ block_tot,
                                                                       const int* __restrict__ tile_off,
                                                                       int* __restrict__ maxpbc, int* __restrict__ start,
                                                                       bool ref_view) {
     const int64_t t = blockIdx.x;
     const int tid = threadIdx.x;
     const int64_t c0 = t * kScanTile + static_cast<int64_t>(tid) * kScanPer;
+    const int toff = tile_off[t];  // in flight while the tile is scanned
     int v[kScanPer];
     load8<PAIR>(count, c0, ncells, v);
     int s = 0;
@@ -244,7 +241,6 @@ __global__ void __launch_bounds__(kScanThreads) scan_downsweep_kernel(int* __res
         if (lane >= o) incl += y;
     }
     __shared__ int wsum[kScanThreads / 32];
-    __shared__ int bsum[kBlocksPerTile];
     if (lane == 31) wsum[w] = incl;
     __syncthreads();
     if (w == 0) {
@@ -256,21 +252,18 @@ __global__ void __launch_bounds__(kScanThreads) scan_downsweep_kernel(int* __res
         }
         if (lane < kScanThreads / 32) wsum[lane] = x;
     }
-    const int toff = tile_off[t];
-    if (tid < kBlocksPerTile) {
-        // maxPBC of this tile's blocks: tile offset + inclusive scan of its block totals.
-        const int64_t b0 = t * kBlocksPerTile;
-        int run = toff;
-        for (int q = 0; q <= tid; ++q)
-            if ((b0 + q) * kRefBlock < ncells) run += block_tot[b0 + q];
-        if ((b0 + tid) * kRefBlock < ncells) maxpbc[b0 + tid] = run;
-        bsum[tid] = run - ((b0 + tid) * kRefBlock < ncells ? block_tot[b0 + tid] : 0);  // exclusive: start of block
-    }
     __syncthreads();
+    // A 512-cell block is two warps (256 cells each): the inclusive prefix
+    // through block b ends at warp 2b + 1.
+    if (tid < kBlocksPerTile) {
+        const int64_t b = t * kBlocksPerTile + tid;
+        if (b * kRefBlock < ncells) maxpbc[b] = toff + wsum[2 * tid + 1];
+    }
     int out[kScanPer];
     if (ref_view) {
         // The reference's start_id: the total of all earlier 512-cell blocks.
-        const int r = bsum[tid / kThreadsPerBlock];
+        const int blk = tid / kThreadsPerBlock;
+        const int r = toff + (blk > 0 ? wsum[2 * blk - 1] : 0);
 #pragma unroll
         for (int k = 0; k < kScanPer; ++k) out[k] = r;
     } else {
@@ -1049,25 +1042,19 @@ cudaError_t launch_assign(const double* pos, int64_t n, const MeshGeom& m, int2*
 
 int64_t scan_block_count(int64_t ncells) { return (ncells + kRefBlock - 1) / kRefBlock; }
 
-int64_t scan_scratch_ints(int64_t ncells) {
-    return scan_block_count(ncells) + (ncells + kScanTile - 1) / kScanTile;
-}
+int64_t scan_scratch_ints(int64_t ncells) { return (ncells + kScanTile - 1) / kScanTile; }
 
 cudaError_t launch_scan(int* count, bool pair, int64_t ncells, int* maxpbc, int* start, bool ref_view, int* scratch,
                         cudaStream_t s) {
     if (ncells < 1) return cudaSuccess;
     const int64_t tiles = (ncells + kScanTile - 1) / kScanTile;
-    int* block_tot = scratch;
-    int* tile_tot = scratch + scan_block_count(ncells);
+    int* tile_tot = scratch;
     const unsigned g = static_cast<unsigned>(tiles);
-    if (pair) scan_totals_kernel<true><<<g, kScanThreads, 0, s>>>(count, ncells, block_tot, tile_tot);
-    else scan_totals_kernel<false><<<g, kScanThreads, 0, s>>>(count, ncells, block_tot, tile_tot);
+    if (pair) scan_totals_kernel<true><<<g, kScanThreads, 0, s>>>(count, ncells, tile_tot);
+    else scan_totals_kernel<false><<<g, kScanThreads, 0, s>>>(count, ncells, tile_tot);
     scan_tiles_kernel<<<1, 1024, 0, s>>>(tile_tot, tiles);
-    if (pair)
-        scan_downsweep_kernel<true><<<g, kScanThreads, 0, s>>>(count, ncells, block_tot, tile_tot, maxpbc, start, ref_view);
-    else
-        scan_downsweep_kernel<false><<<g, kScanThreads, 0, s>>>(count, ncells, block_tot, tile_tot, maxpbc, start,
-                                                                ref_view);
+    if (pair) scan_downsweep_kernel<true><<<g, kScanThreads, 0, s>>>(count, ncells, tile_tot, maxpbc, start, ref_view);
+    else scan_downsweep_kernel<false><<<g, kScanThreads, 0, s>>>(count, ncells, tile_tot, maxpbc, start, ref_view);
     return cudaGetLastError();
 }
 
