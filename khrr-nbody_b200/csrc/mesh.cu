@@ -420,30 +420,6 @@ __global__ void __launch_bounds__(256) wave_f64_kernel(double* __restrict__ phi_
 #endif
 constexpr int kWX = KHRR_WAVE_WX, kWY = KHRR_WAVE_WY;
 
-// L2 eviction priority of the stencil's mass and phi^{n-1} loads: 0 = the
-// default; 1 = the mass (read unchanged by every iteration of a solve) with
-// evict_last, so it tends to stay in L2 across iterations; 2 = also
-// phi^{n-1} (read once per iteration) with evict_first.
-#ifndef KHRR_WAVE_L2HINT
-#define KHRR_WAVE_L2HINT 0
-#endif
-#if KHRR_WAVE_L2HINT
-__device__ __forceinline__ uint64_t policy_evict_last() {
-    uint64_t pol;
-    asm("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(pol));
-    return pol;
-}
-__device__ __forceinline__ uint64_t policy_evict_first() {
-    uint64_t pol;
-    asm("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(pol));
-    return pol;
-}
-__device__ __forceinline__ float ld_hint(const float* p, uint64_t pol) {
-    float v;
-    asm("ld.global.nc.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(v) : "l"(p), "l"(pol));
-    return v;
-}
-#endif
 static_assert(kWX % 32 == 0 && kWX * kWY <= 1024, "whole warps along x");
 
 template <int kWZ>
@@ -482,16 +458,8 @@ __global__ void __launch_bounds__(kWX * kWY) wave_f32_kernel(float* __restrict__
             xp[u] = phi[at + dxp];
             ym[u] = phi[at - dym];
             yp[u] = phi[at + dyp];
-#if KHRR_WAVE_L2HINT >= 2
-            po[u] = ld_hint(phi_old + at, policy_evict_first());
-#else
             po[u] = phi_old[at];
-#endif
-#if KHRR_WAVE_L2HINT >= 1
-            ms[u] = ld_hint(mass + at, policy_evict_last());
-#else
             ms[u] = mass[at];
-#endif
         }
         const bool edge_xy = ix == 0 || ix == NX - 1 || iy == 0 || iy == NX - 1;
         const float sxy = (W.diss_base + W.sx[ix]) + W.sy[iy];
