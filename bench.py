@@ -828,21 +828,25 @@ def run_khrr(args):
     kick = None
     if rank == 0:
         kick = kick_drift_leg(khrr, ctx, torch, 4 * n, float(peaks.get("hbm_gbs", 6650.0)))
+    # The legs below describe single-GPU configurations and run in a
+    # single-GPU run only: under torchrun the other ranks would wait for them
+    # at the closing barrier, past the process group's timeout.
+    single = rank == 0 and world == 1
     # the precision contract at this size: FP32 (tuned kernel) vs FP64 runs
     drift64 = None
-    if rank == 0 and args.drift_steps > 0:
+    if single and args.drift_steps > 0:
         drift64 = drift_vs_fp64_leg(khrr, ctx, torch, pos, vel, mass, eps2, args.drift_steps,
                                     fp64_steps=min(args.drift_fp64_steps, args.drift_steps))
     ens = None
-    if not args.no_ensemble and rank == 0:
+    if not args.no_ensemble and single:
         ens = ensemble_leg(khrr, local, torch)
     mesh = None
-    if not args.no_mesh and rank == 0:
+    if not args.no_mesh and single:
         mesh = mesh_leg(khrr, local, torch, float(peaks.get("hbm_gbs", 6650.0)), args.mesh_max_iter)
     ctx.close()
     configs = None
-    if not args.no_configs and rank == 0:
-        configs = {"config0": config0_leg(khrr, local, torch, run_cpu=world == 1 and not args.no_cpu_baseline),
+    if not args.no_configs and single:
+        configs = {"config0": config0_leg(khrr, local, torch, run_cpu=not args.no_cpu_baseline),
                    "config1": "this line: value, roofline, acc_rel_rms_vs_fp64, drift_vs_fp64",
                    "config2": config2_leg(khrr, local, torch),
                    "config3": "ensemble",
