@@ -189,29 +189,55 @@ __global__ void __launch_bounds__(kScanThreads) scan_totals_kernel(const int* __
     }
 }
 
-// K2 (one CTA): tile totals -> exclusive tile offsets, in place.
+// K2 (one CTA): tile totals -> exclusive tile offsets, in place.  Chunks of
+// 1024 x kTilesPer tiles: each thread sums its kTilesPer consecutive totals,
+// the 1024 thread sums are scanned with warp shuffles and one pass over the
+// 32 warp sums (two barriers per chunk), and the chunks follow with a
+// running carry (one chunk covers 4096 tiles = 16.8 M cells, a 256^3 mesh).
+constexpr int kTilesPer = 4;
 __global__ void __launch_bounds__(1024) scan_tiles_kernel(int* __restrict__ tile, int64_t ntiles) {
     constexpr int T = 1024;
-    __shared__ int part[T];
-    const int tid = threadIdx.x;
-    const int64_t per = (ntiles + T - 1) / T;
-    // Chunks of T tiles (coalesced), scanned in order with a running carry.
+    __shared__ int wsum[T / 32];
+    __shared__ int s_total;
+    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+    const int64_t chunk = static_cast<int64_t>(T) * kTilesPer;
     int carry = 0;
-    for (int64_t r = 0; r < per; ++r) {
-        const int64_t e = r * T + tid;
-        const int x = e < ntiles ? tile[e] : 0;
-        part[tid] = x;
-        __syncthreads();
-        for (int o = 1; o < T; o <<= 1) {
-            const int y = tid >= o ? part[tid - o] : 0;
-            __syncthreads();
-            part[tid] += y;
-            __syncthreads();
+    for (int64_t c0 = 0; c0 < ntiles; c0 += chunk) {
+        const int64_t e0 = c0 + static_cast<int64_t>(tid) * kTilesPer;
+        int v[kTilesPer];
+        int sum = 0;
+#pragma unroll
+        for (int k = 0; k < kTilesPer; ++k) {
+            v[k] = e0 + k < ntiles ? tile[e0 + k] : 0;
+            sum += v[k];
         }
-        if (e < ntiles) tile[e] = carry + part[tid] - x;
-        const int total = part[T - 1];
+        int incl = sum;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += y;
+        }
+        if (lane == 31) wsum[w] = incl;
         __syncthreads();
-        carry += total;
+        if (w == 0) {
+            int x = wsum[lane];
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int y = __shfl_up_sync(0xffffffffu, x, o);
+                if (lane >= o) x += y;
+            }
+            wsum[lane] = x;
+            if (lane == 31) s_total = x;
+        }
+        __syncthreads();
+        int run = carry + (w > 0 ? wsum[w - 1] : 0) + (incl - sum);
+#pragma unroll
+        for (int k = 0; k < kTilesPer; ++k) {
+            if (e0 + k < ntiles) tile[e0 + k] = run;
+            run += v[k];
+        }
+        carry += s_total;
+        __syncthreads();  // wsum and s_total are rewritten by the next chunk
     }
 }
 
@@ -419,6 +445,10 @@ __global__ void __launch_bounds__(256) wave_f64_kernel(double* __restrict__ phi_
 #define KHRR_WAVE_WY 8
 #endif
 constexpr int kWX = KHRR_WAVE_WX, kWY = KHRR_WAVE_WY;
+// z planes per thread of the four-cells-per-thread form (0 = not used).
+#ifndef KHRR_WAVE_X4
+#define KHRR_WAVE_X4 0
+#endif
 
 static_assert(kWX % 32 == 0 && kWX * kWY <= 1024, "whole warps along x");
 
@@ -491,6 +521,107 @@ __global__ void __launch_bounds__(kWX * kWY) wave_f32_kernel(float* __restrict__
             n2 += __shfl_xor_sync(0xffffffffu, n2, o);
         }
         if ((threadIdx.x & 31) == 0) {
+            atomicAdd(&resid[0], d2);
+            atomicAdd(&resid[1], n2);
+        }
+    }
+}
+
+// The same step with four consecutive x cells per thread (nx % 4 == 0):
+// every row access is one 16-byte load or store, so a warp moves 512
+// contiguous bytes per access and issues a quarter of the load instructions.
+// The x neighbours come from the float4 itself and, across threads, by warp
+// shuffles (a warp covers 128 consecutive x cells); lanes 0 and 31 load the
+// one cell beyond their warp's span.  Threads past the mesh in x read
+// clamped addresses (for the shuffles) and store nothing.  Per cell the
+// arithmetic is wave_f32_kernel's, so the bits are the same.
+constexpr int kW4X = 32, kW4Y = 8;  // threads: 128 x cells x 8 rows
+
+__device__ __forceinline__ float f4c(const float4& v, int k) { return k == 0 ? v.x : k == 1 ? v.y : k == 2 ? v.z : v.w; }
+
+template <int kWZ>
+__global__ void __launch_bounds__(kW4X * kW4Y) wave_f32x4_kernel(float* __restrict__ phi_new, const float* __restrict__ phi,
+                                                                 const float* __restrict__ phi_old,
+                                                                 const float* __restrict__ mass, const WaveF32 W,
+                                                                 double* __restrict__ resid) {
+    const int NX = W.nx;
+    const int ix0 = (blockIdx.x * kW4X + threadIdx.x) * 4, iy = blockIdx.y * kW4Y + threadIdx.y;
+    const int zb = blockIdx.z * kWZ;
+    const int lane = threadIdx.x;  // kW4X == 32: one warp per x row segment
+    const int64_t sy = NX, sz = static_cast<int64_t>(NX) * NX;
+    double d2 = 0.0, n2 = 0.0;
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    if (iy < NX) {  // whole warps share iy: the shuffles below see every lane
+        const bool xin = ix0 < NX;
+        const int xc = xin ? ix0 : NX - 4;  // clamped for the loads
+        const int64_t col = static_cast<int64_t>(iy) * NX + xc;
+        const int64_t dym = iy > 0 ? sy : 0, dyp = iy < NX - 1 ? sy : 0;
+        const int64_t dxm = xc > 0 ? 1 : 0, dxp = xc + 4 < NX ? 4 : 3;  // the cells beyond the float4
+        float4 c[kWZ + 2];  // phi at z = zb - 1 .. zb + kWZ (clamped)
+        float4 ym[kWZ], yp[kWZ], po[kWZ], ms[kWZ];
+        float xl[kWZ], xr[kWZ];  // lanes 0 / 31: phi at xc - 1 / xc + 4
+#pragma unroll
+        for (int u = 0; u < kWZ + 2; ++u) {
+            const int z = min(max(zb - 1 + u, 0), NX - 1);
+            c[u] = *reinterpret_cast<const float4*>(phi + z * sz + col);
+        }
+#pragma unroll
+        for (int u = 0; u < kWZ; ++u) {
+            const int64_t at = min(zb + u, NX - 1) * sz + col;
+            ym[u] = *reinterpret_cast<const float4*>(phi + at - dym);
+            yp[u] = *reinterpret_cast<const float4*>(phi + at + dyp);
+            po[u] = *reinterpret_cast<const float4*>(phi_old + at);
+            ms[u] = *reinterpret_cast<const float4*>(mass + at);
+            xl[u] = lane == 0 ? phi[at - dxm] : 0.0f;
+            xr[u] = lane == 31 ? phi[at + dxp] : 0.0f;
+        }
+        const float4 sx4 = *reinterpret_cast<const float4*>(W.sx + xc);
+        const float sy1 = W.sy[iy];
+        const bool edge_y = iy == 0 || iy == NX - 1;
+#pragma unroll
+        for (int u = 0; u < kWZ; ++u) {
+            const int z = zb + u;
+            const float4 cc = c[u + 1];
+            // x neighbours of the end cells from the adjacent lanes
+            float left = __shfl_up_sync(0xffffffffu, cc.w, 1);
+            float right = __shfl_down_sync(0xffffffffu, cc.x, 1);
+            if (lane == 0) left = xl[u];
+            if (lane == 31) right = xr[u];
+            if (z >= NX || !xin) continue;
+            const int64_t at = z * sz + col;
+            float out[4];
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                const int ix = xc + k;
+                float o = 0.0f;
+                if (!(edge_y || ix == 0 || ix == NX - 1 || z == 0 || z == NX - 1)) {
+                    const float xm = k == 0 ? left : f4c(cc, k - 1);
+                    const float xp = k == 3 ? right : f4c(cc, k + 1);
+                    const float nb = ((xm + xp) + (f4c(ym[u], k) + f4c(yp[u], k))) + (f4c(c[u], k) + f4c(c[u + 2], k));
+                    const float diss = ((W.diss_base + f4c(sx4, k)) + sy1) + W.sz[z];
+                    const float Q = diss * W.cdt_half;
+                    const float w = __frcp_rn(1.0f + Q);  // correctly rounded: the bits of 1.0f / (1.0f + Q)
+                    o = fmaf(nb, W.K * w,
+                             fmaf(f4c(cc, k), W.A * w, fmaf(f4c(po[u], k), (Q - 1.0f) * w, f4c(ms[u], k) * (W.S * w))));
+                }
+                out[k] = o;
+                if (resid) {
+                    const double dd = static_cast<double>(o) - static_cast<double>(f4c(cc, k));
+                    d2 += dd * dd;
+                    n2 += static_cast<double>(o) * static_cast<double>(o);
+                }
+            }
+            *reinterpret_cast<float4*>(phi_new + at) = make_float4(out[0], out[1], out[2], out[3]);
+        }
+    }
+    if (resid) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            d2 += __shfl_xor_sync(0xffffffffu, d2, o);
+            n2 += __shfl_xor_sync(0xffffffffu, n2, o);
+        }
+        if (lane == 0) {
             atomicAdd(&resid[0], d2);
             atomicAdd(&resid[1], n2);
         }
@@ -1056,6 +1187,14 @@ cudaError_t launch_wave_f32(float* phi_new, const float* phi, const float* phi_o
     attr[0].val.programmaticStreamSerializationAllowed = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
+#if KHRR_WAVE_X4
+    if (w.nx % 4 == 0 && w.nx >= 8) {
+        cfg.blockDim = dim3(kW4X, kW4Y);
+        cfg.gridDim = dim3((w.nx + 4 * kW4X - 1) / (4 * kW4X), (w.nx + kW4Y - 1) / kW4Y,
+                           (w.nx + KHRR_WAVE_X4 - 1) / KHRR_WAVE_X4);
+        return cudaLaunchKernelEx(&cfg, wave_f32x4_kernel<KHRR_WAVE_X4>, phi_new, phi, phi_old, mass, w, resid);
+    }
+#endif
     if (w.nx >= 192) {
         cfg.gridDim = dim3((w.nx + kWX - 1) / kWX, (w.nx + kWY - 1) / kWY, (w.nx + 7) / 8);
         return cudaLaunchKernelEx(&cfg, wave_f32_kernel<8>, phi_new, phi, phi_old, mass, w, resid);
