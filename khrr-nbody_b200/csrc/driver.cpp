@@ -4,12 +4,14 @@
 //
 //   khrr_nbody [--data DIR] [--device K] [--compat-accumulate] [--no-mesh]
 //              [--mesh-nx N] [--mesh-dx D] [--wave] [--wave-fp32] [--cic]
-//              [--wave-setup ITERS] [--kernel auto|pair|one-sided] [--quiet]
+//              [--wave-setup ITERS] [--kernel auto|pair|one-sided|fp64] [--quiet]
 //
 // --kernel picks the direct-sum force kernel: auto (default) times the
 // candidates on the initial state (khrr_autotune), pair is the symmetric
 // kernel (each unordered pair once for both bodies), one-sided the kernel
-// that evaluates every ordered pair.
+// that evaluates every ordered pair, fp64 the direct sum in FP64 (the
+// reference's own precision, KHRR_FP64; about a fifth of the pair kernel's
+// rate).
 //
 // --wave selects the reference's Wave solver (NBodySolver::Wave, compiled in
 // the reference but switched off at nbody.cu:1132): forces and potentials
@@ -181,8 +183,8 @@ Options parse(int argc, char** argv) {
         else if (a == "--wave-setup") o.wave_setup = std::stoi(next());
         else if (a == "--kernel") {
             o.kernel = next();
-            if (o.kernel != "auto" && o.kernel != "pair" && o.kernel != "one-sided")
-                die("--kernel takes auto, pair or one-sided");
+            if (o.kernel != "auto" && o.kernel != "pair" && o.kernel != "one-sided" && o.kernel != "fp64")
+                die("--kernel takes auto, pair, one-sided or fp64");
         }
         else if (a == "--quiet") o.quiet = true;
         else die("unknown argument " + a);
@@ -334,6 +336,8 @@ int main(int argc, char** argv) {
         std::printf("Wave eq iterations: %d\n", ms.iters_per_step);
         check(khrr_set_mesh_solver(ctx, &ms), ctx, "mesh solver");
         solver_flag = KHRR_MESH;
+    } else if (opt.kernel == "fp64") {
+        solver_flag = KHRR_FP64;
     }
     std::vector<double> cell_phi(opt.mesh || opt.wave ? static_cast<size_t>(NX) * NX * NX : 0);
     auto print_cell_phi = [&](int iter) {

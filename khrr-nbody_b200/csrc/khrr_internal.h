@@ -230,6 +230,7 @@ int conservation_blocks(int64_t n);
 struct MeshGeom {
     double lo[3];
     double cs[3];
+    double rcs[3];  // 1 / cs, correctly rounded (the cell divisions use it)
     int g[3];
 };
 struct WaveConsts {

@@ -41,10 +41,27 @@ int grid_for(int64_t n, int block) {
     return static_cast<int>(g);
 }
 
+// a / b, correctly rounded, from y = RN(1/b): Markstein's correction step
+// (P. Markstein, "Computation of elementary functions on the IBM RISC
+// System/6000 processor", IBM J. Res. Develop. 34(1), 1990; see also
+// Muller et al., "Handbook of Floating-Point Arithmetic", ch. 4): q = RN(a y)
+// is within an ulp of a/b, r = a - b q is exact in one fma, and RN(q + r y)
+// is RN(a/b).  Several quotients over one denominator then share one
+// correctly rounded reciprocal (__drcp_rn).  Checked bitwise against the IEEE
+// division on 1.7e10 quotients (the stencil's operand ranges and random
+// operands over 64 binary orders of magnitude): no difference.
+__device__ __forceinline__ double div_rn(double a, double b, double y) {
+    const double q = __dmul_rn(a, y);
+    const double r = fma(-b, q, a);
+    return fma(r, y, q);
+}
+
 // Cell coordinate of one axis: (int)((p - lo) / cs) clamped to [0, g - 1],
 // with the CUDA conversion's behaviour for quotients outside the int range.
-__device__ __forceinline__ int cell_axis(double p, double lo, double cs, int g) {
-    const double q = (p - lo) / cs;
+// The quotient is the IEEE one, from the mesh's correctly rounded reciprocal
+// rcs = RN(1 / cs) (div_rn: three FP64 operations instead of a division).
+__device__ __forceinline__ int cell_axis(double p, double lo, double cs, double rcs, int g) {
+    const double q = div_rn(p - lo, cs, rcs);
     if (q >= static_cast<double>(g - 1)) return g - 1;
     if (q > -1.0) return static_cast<int>(q);
     return 0;
@@ -53,9 +70,9 @@ __device__ __forceinline__ int cell_axis(double p, double lo, double cs, int g) 
 // The reference's cell id (p2mesh-kernel.cuh:25-40): iz clamps to g[1] - 1 and
 // the y stride is g[2].
 __device__ __forceinline__ int cell_of(const double* __restrict__ p, const MeshGeom& m) {
-    const int ix = cell_axis(p[0], m.lo[0], m.cs[0], m.g[0]);
-    const int iy = cell_axis(p[1], m.lo[1], m.cs[1], m.g[1]);
-    const int iz = cell_axis(p[2], m.lo[2], m.cs[2], m.g[1]);
+    const int ix = cell_axis(p[0], m.lo[0], m.cs[0], m.rcs[0], m.g[0]);
+    const int iy = cell_axis(p[1], m.lo[1], m.cs[1], m.rcs[1], m.g[1]);
+    const int iz = cell_axis(p[2], m.lo[2], m.cs[2], m.rcs[2], m.g[1]);
     return iz * m.g[0] * m.g[1] + iy * m.g[2] + ix;
 }
 
@@ -349,20 +366,6 @@ __device__ __forceinline__ double wave_diss(const WaveConsts& W, int ix, int iy,
     return d;
 }
 
-// a / b, correctly rounded, from y = RN(1/b): Markstein's correction step
-// (P. Markstein, "Computation of elementary functions on the IBM RISC
-// System/6000 processor", IBM J. Res. Develop. 34(1), 1990; see also
-// Muller et al., "Handbook of Floating-Point Arithmetic", ch. 4): q = RN(a y)
-// is within an ulp of a/b, r = a - b q is exact in one fma, and RN(q + r y)
-// is RN(a/b).  Several quotients over one denominator then share one
-// correctly rounded reciprocal (__drcp_rn).  Checked bitwise against the IEEE
-// division on 1.7e10 quotients (the stencil's operand ranges and random
-// operands over 64 binary orders of magnitude): no difference.
-__device__ __forceinline__ double div_rn(double a, double b, double y) {
-    const double q = __dmul_rn(a, y);
-    const double r = fma(-b, q, a);
-    return fma(r, y, q);
-}
 
 // wave_diss_iteration in FP64, the reference's expressions term for term
 // (same bits as the literal per-cell kernel): kWZ consecutive z cells of one
@@ -445,10 +448,7 @@ __global__ void __launch_bounds__(256) wave_f64_kernel(double* __restrict__ phi_
 #define KHRR_WAVE_WY 8
 #endif
 constexpr int kWX = KHRR_WAVE_WX, kWY = KHRR_WAVE_WY;
-// z planes per thread of the four-cells-per-thread form (0 = not used).
-#ifndef KHRR_WAVE_X4
-#define KHRR_WAVE_X4 0
-#endif
+
 
 static_assert(kWX % 32 == 0 && kWX * kWY <= 1024, "whole warps along x");
 
@@ -979,8 +979,8 @@ struct CicAxis {
     double w[2];
 };
 
-__device__ __forceinline__ CicAxis cic_axis(double p, double lo, double cs, int g) {
-    const double u = (p - lo) / cs - 0.5;
+__device__ __forceinline__ CicAxis cic_axis(double p, double lo, double cs, double rcs, int g) {
+    const double u = div_rn(p - lo, cs, rcs) - 0.5;
     const double fl = floor(u);
     CicAxis a;
     a.i0 = fl >= -1.0 ? (fl <= static_cast<double>(g) ? static_cast<int>(fl) : g) : -2;
@@ -994,9 +994,9 @@ __global__ void cic_deposit_kernel(const double* __restrict__ pos, const double*
                                    const MeshGeom m, double* __restrict__ cell_mass) {
     const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (i >= n) return;
-    const CicAxis ax = cic_axis(pos[3 * i], m.lo[0], m.cs[0], m.g[0]);
-    const CicAxis ay = cic_axis(pos[3 * i + 1], m.lo[1], m.cs[1], m.g[1]);
-    const CicAxis az = cic_axis(pos[3 * i + 2], m.lo[2], m.cs[2], m.g[2]);
+    const CicAxis ax = cic_axis(pos[3 * i], m.lo[0], m.cs[0], m.rcs[0], m.g[0]);
+    const CicAxis ay = cic_axis(pos[3 * i + 1], m.lo[1], m.cs[1], m.rcs[1], m.g[1]);
+    const CicAxis az = cic_axis(pos[3 * i + 2], m.lo[2], m.cs[2], m.rcs[2], m.g[2]);
     const double mi = mass[i];
 #pragma unroll
     for (int c = 0; c < 2; ++c) {
@@ -1024,9 +1024,9 @@ template <class T>
 __device__ __forceinline__ void cic_interp(const double* __restrict__ p, const MeshGeom& m,
                                            const double* __restrict__ cacc, const T* __restrict__ cval, double (&acc)[3],
                                            double& val) {
-    const CicAxis ax = cic_axis(p[0], m.lo[0], m.cs[0], m.g[0]);
-    const CicAxis ay = cic_axis(p[1], m.lo[1], m.cs[1], m.g[1]);
-    const CicAxis az = cic_axis(p[2], m.lo[2], m.cs[2], m.g[2]);
+    const CicAxis ax = cic_axis(p[0], m.lo[0], m.cs[0], m.rcs[0], m.g[0]);
+    const CicAxis ay = cic_axis(p[1], m.lo[1], m.cs[1], m.rcs[1], m.g[1]);
+    const CicAxis az = cic_axis(p[2], m.lo[2], m.cs[2], m.rcs[2], m.g[2]);
     acc[0] = acc[1] = acc[2] = 0.0;
     val = 0.0;
 #pragma unroll
@@ -1187,14 +1187,14 @@ cudaError_t launch_wave_f32(float* phi_new, const float* phi, const float* phi_o
     attr[0].val.programmaticStreamSerializationAllowed = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-#if KHRR_WAVE_X4
-    if (w.nx % 4 == 0 && w.nx >= 8) {
+    // Kernel choice, measured (us per iteration, 128^3 / 256^3): one cell per
+    // thread with 4 / 8 z planes 12.5 / 71.8; four x cells per thread with 2 z
+    // planes 12.0 / 72.3 (with 4 planes 12.8 / 79.6).
+    if (w.nx < 192 && w.nx % 4 == 0 && w.nx >= 8) {
         cfg.blockDim = dim3(kW4X, kW4Y);
-        cfg.gridDim = dim3((w.nx + 4 * kW4X - 1) / (4 * kW4X), (w.nx + kW4Y - 1) / kW4Y,
-                           (w.nx + KHRR_WAVE_X4 - 1) / KHRR_WAVE_X4);
-        return cudaLaunchKernelEx(&cfg, wave_f32x4_kernel<KHRR_WAVE_X4>, phi_new, phi, phi_old, mass, w, resid);
+        cfg.gridDim = dim3((w.nx + 4 * kW4X - 1) / (4 * kW4X), (w.nx + kW4Y - 1) / kW4Y, (w.nx + 1) / 2);
+        return cudaLaunchKernelEx(&cfg, wave_f32x4_kernel<2>, phi_new, phi, phi_old, mass, w, resid);
     }
-#endif
     if (w.nx >= 192) {
         cfg.gridDim = dim3((w.nx + kWX - 1) / kWX, (w.nx + kWY - 1) / kWY, (w.nx + 7) / 8);
         return cudaLaunchKernelEx(&cfg, wave_f32_kernel<8>, phi_new, phi, phi_old, mass, w, resid);

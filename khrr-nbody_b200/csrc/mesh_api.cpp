@@ -30,6 +30,7 @@ khrr_status check_mesh(khrr_ctx* c, const khrr_mesh* m, MeshGeom* g, int64_t* nc
             return c->fail(KHRR_ERR_INVALID_ARG, "mesh origin / cell size must be finite, cell > 0");
         g->lo[k] = m->lo[k];
         g->cs[k] = m->cell[k];
+        g->rcs[k] = 1.0 / m->cell[k];  // IEEE division: the correctly rounded reciprocal
         g->g[k] = m->grid[k];
     }
     const int64_t gx = m->grid[0], gy = m->grid[1], gz = m->grid[2];

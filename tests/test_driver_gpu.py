@@ -57,8 +57,8 @@ def read_snapshot(path, n):
     return t, rec[:, :3], rec[:, 3:]
 
 
-def api_run(d, nsteps):
-    """The same simulation through the Python API."""
+def api_run(d, nsteps, flags=0):
+    """The same simulation through the Python API (flags: KHRR_FP64 or 0)."""
     import khrr
     from test_io import Galaxy
     L = khrr.lib()
@@ -76,9 +76,9 @@ def api_run(d, nsteps):
     try:
         ctx.set_external_field(Mh=1.0, a=0.3333, Rh=1.0, Mb=0.0, b=0.0431, Rb=0.2)
         ctx.upload(pos[:n], vel[:n], mass[:n], eps2[:n])
-        ctx.forces(khrr.ACC | khrr.PHI)
+        ctx.forces(khrr.ACC | khrr.PHI | flags)
         e0 = ctx.conservation()
-        ctx.step(0.002, nsteps, 0)
+        ctx.step(0.002, nsteps, flags)
         return n, ns.value, ctx.download(), e0
     finally:
         ctx.close()
@@ -151,6 +151,25 @@ def test_driver_kernel_choice(libkhrr, tmp_path, kernel):
     _, ps, _ = read_snapshot(d / "bin" / "S_   10.bin", ns)
     _, pd, _ = read_snapshot(d / "bin" / "DM_   10.bin", n - ns)
     assert np.abs(np.concatenate([ps, pd]) - state["pos"]).max() <= 1e-5
+
+
+def test_driver_fp64_kernel(libkhrr, tmp_path):
+    """--kernel fp64: the reference's own precision through the driver; its
+    snapshot equals the API run with KHRR_FP64 (the same calls), and differs
+    from the FP32 one-sided run by the FP32 rounding only."""
+    torch = pytest.importorskip("torch")
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    import khrr
+    d = tmp_path / "nbody"
+    write_inputs(d, 0, 0.1)
+    run_driver(d, "fp64")
+    n, ns, state, _ = api_run(d, 50, khrr.FP64)
+    _, ps, _ = read_snapshot(d / "bin" / "S_   10.bin", ns)
+    _, pd, _ = read_snapshot(d / "bin" / "DM_   10.bin", n - ns)
+    assert np.abs(np.concatenate([ps, pd]) - state["pos"]).max() <= 1e-12
+    _, _, state32, _ = api_run(d, 50)
+    assert np.abs(state32["pos"] - state["pos"]).max() <= 1e-5
 
 
 def test_driver_wave_mode(libkhrr, tmp_path):
