@@ -106,6 +106,11 @@ static_assert(JT % 64 == 0 && JT == kPad, "tiles are whole sub-chunk pairs and p
 #define KHRR_PAIR_UNROLL 2
 #endif
 constexpr int kSUnroll = KHRR_PAIR_UNROLL;
+// Tiles per fold of the acceleration-only variants' i-side partials.
+#ifndef KHRR_PAIR_FOLD
+#define KHRR_PAIR_FOLD 2
+#endif
+constexpr int kFoldEvery = KHRR_PAIR_FOLD;
 constexpr int kSUnrollPhi = 1;
 
 constexpr unsigned kUnif = 1;   // every body has the same softening: no h array
@@ -329,7 +334,7 @@ __global__ void __launch_bounds__(NT, (pair_min_blocks<F>())) pair_kernel(const 
             // Fold the i-side partials (times the tile mass when it was factored
             // out) into the running sums: every tile, or every second tile, at
             // the item's end and before a tile of another mass.
-            const bool fold = !kFoldPairs || (t & 1) || t + 1 == ntiles ||
+            const bool fold = !kFoldPairs || (t % kFoldEvery) == kFoldEvery - 1 || t + 1 == ntiles ||
                               (BMASS && a.tile_mass[jt0 / JT + 1] != mt);
             if (fold) {
 #pragma unroll
