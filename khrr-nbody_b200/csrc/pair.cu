@@ -45,10 +45,10 @@
 // mass (and no ghosts) the masses are factored out of both sums; otherwise
 // m_j and m_i enter per pair (2 more multiplies).
 //
-// Accuracy: the i-side partials (two halves of 64 terms per tile, over one or
-// two tiles) fold into compensated (hi + lo) running sums kept in shared
-// memory; a reaction partial is a sum of 1024 terms in three levels (8 i
-// bodies, 32 lanes, 4 warps).
+// Accuracy: the i-side partials (two halves of 64 terms per tile, over up to
+// eight tiles with accelerations only, one with the potential) fold into
+// compensated (hi + lo) running sums kept in shared memory; a reaction partial
+// is a sum of 1024 terms in three levels (8 i bodies, 32 lanes, 4 warps).
 #include <cstdint>
 
 #include "async_copy.cuh"
@@ -106,9 +106,13 @@ static_assert(JT % 64 == 0 && JT == kPad, "tiles are whole sub-chunk pairs and p
 #define KHRR_PAIR_UNROLL 2
 #endif
 constexpr int kSUnroll = KHRR_PAIR_UNROLL;
-// Tiles per fold of the acceleration-only variants' i-side partials.
+// Tiles per fold of the acceleration-only variants' i-side partials,
+// measured at 786k bodies (ms per pass; relative RMS error vs FP64 on 8192
+// targets at 786k / 2.1M): 2: 149.7-150.3, 3.64e-8 / 6.44e-8; 8: 148.3,
+// 3.76e-8 / 6.48e-8; 32: 148.0, 4.77e-8 / 6.78e-8; 256 (item ends only):
+// 147.9, 2.26e-7 / 1.54e-7.
 #ifndef KHRR_PAIR_FOLD
-#define KHRR_PAIR_FOLD 2
+#define KHRR_PAIR_FOLD 8
 #endif
 constexpr int kFoldEvery = KHRR_PAIR_FOLD;
 constexpr int kSUnrollPhi = 1;
@@ -307,10 +311,11 @@ __global__ void __launch_bounds__(NT, (pair_min_blocks<F>())) pair_kernel(const 
         }
         const float mI = BMASS ? a.tile_mass[w.i_begin / JT] : 1.f;
 
-        // i-side partials since the last fold: folded every second tile in the
-        // acceleration-only variants (149.6 ms per pass at 786k against 151.2
-        // ms folding every tile), every tile where the potential adds to the
-        // registers live across tiles (172.3 against 171.0 ms).
+        // i-side partials since the last fold: folded every kFoldEvery-th tile
+        // in the acceleration-only variants (every tile: 151.2 ms per pass at
+        // 786k, every second 149.6-150.3, every eighth 148.3), every tile where
+        // the potential adds to the registers live across tiles (172.3 against
+        // 171.0 ms).
         constexpr bool kFoldPairs = !PHI;
         float2 ai[NC][K];
 #pragma unroll
