@@ -27,13 +27,19 @@
 namespace khrr {
 namespace {
 
-constexpr int NT = 128;  // threads per CTA
-constexpr int K = 4;     // i bodies per thread
-constexpr int JT = 128;  // j bodies per shared-memory tile
-static_assert(NT * K == kF64ITile && JT == kPad, "tile shapes");
+#ifndef KHRR_F64_NT
+#define KHRR_F64_NT 128
+#endif
+constexpr int NT = KHRR_F64_NT;   // threads per CTA
+constexpr int K = kF64ITile / NT;  // i bodies per thread
+constexpr int JT = 128;            // j bodies per shared-memory tile
+constexpr int FP = (JT + NT - 1) / NT;  // j bodies each thread stages per tile
+static_assert(NT * K == kF64ITile && JT == kPad && (JT % NT == 0 || NT % JT == 0), "tile shapes");
+
+constexpr int kMinCtas = NT >= 128 ? 512 / NT : 4;  // resident CTAs per SM the registers aim at
 
 template <bool ACC, bool PHI>
-__global__ void __launch_bounds__(NT, 4) fp64_force_kernel(const F64Args a) {
+__global__ void __launch_bounds__(NT, kMinCtas) fp64_force_kernel(const F64Args a) {
     __shared__ double sx[2][JT], sy[2][JT], sz[2][JT], sm[2][JT], sh[2][JT];
     __shared__ int s_item;
     const int tid = threadIdx.x;
@@ -57,26 +63,36 @@ __global__ void __launch_bounds__(NT, 4) fp64_force_kernel(const F64Args a) {
         }
 
         const int ntiles = (w.j_end - w.j_begin) / JT;
-        // Register copy of the next tile's body tid.
-        auto fetch = [&](int t, double& x, double& y, double& z, double& m, double& h) {
-            const int64_t j = w.j_begin + static_cast<int64_t>(t) * JT + tid;
-            x = a.pos[3 * j];
-            y = a.pos[3 * j + 1];
-            z = a.pos[3 * j + 2];
-            m = a.mass[j];
-            h = 0.5 * a.eps2[j];
+        // Register copy of the next tile's bodies tid, tid + NT, ... (< JT).
+        double nx[FP], ny[FP], nz[FP], nm[FP], nh[FP];
+        auto fetch = [&](int t) {
+#pragma unroll
+            for (int q = 0; q < FP; ++q) {
+                const int jj = tid + q * NT;
+                if (jj >= JT) break;
+                const int64_t j = w.j_begin + static_cast<int64_t>(t) * JT + jj;
+                nx[q] = a.pos[3 * j];
+                ny[q] = a.pos[3 * j + 1];
+                nz[q] = a.pos[3 * j + 2];
+                nm[q] = a.mass[j];
+                nh[q] = 0.5 * a.eps2[j];
+            }
         };
-        double nx, ny, nz, nm, nh;
-        fetch(0, nx, ny, nz, nm, nh);
+        fetch(0);
         for (int t = 0; t < ntiles; ++t) {
             const int b = t & 1;
-            sx[b][tid] = nx;
-            sy[b][tid] = ny;
-            sz[b][tid] = nz;
-            sm[b][tid] = nm;
-            sh[b][tid] = nh;
+#pragma unroll
+            for (int q = 0; q < FP; ++q) {
+                const int jj = tid + q * NT;
+                if (jj >= JT) break;
+                sx[b][jj] = nx[q];
+                sy[b][jj] = ny[q];
+                sz[b][jj] = nz[q];
+                sm[b][jj] = nm[q];
+                sh[b][jj] = nh[q];
+            }
             __syncthreads();
-            if (t + 1 < ntiles) fetch(t + 1, nx, ny, nz, nm, nh);
+            if (t + 1 < ntiles) fetch(t + 1);
 #pragma unroll 2
             for (int jj = 0; jj < JT; ++jj) {
                 const double xj = sx[b][jj], yj = sy[b][jj], zj = sz[b][jj], mj = sm[b][jj], hj = sh[b][jj];
