@@ -361,7 +361,11 @@ khrr_status khrr_set_external_field(khrr_ctx* ctx, const khrr_field_params* p);
 /* Uploads n bodies: pos, vel (n x 3, AoS), mass and eps2 (n).  Systems are
  * independent (no mutual gravity): nsys >= 1 ranges given by sys_offsets
  * (nsys + 1 increasing offsets, first 0, last n); sys_offsets NULL = one
- * system.  Resets acc/phi to zero (call khrr_forces for a(t0)). */
+ * system.  Resets acc/phi to zero (call khrr_forces for a(t0)).  Every eps2
+ * must be > 0 (KHRR_ERR_INVALID_ARG otherwise).  The arrays are checked
+ * while their copies to the device are in flight, so an upload that fails
+ * after its argument checks leaves the context without state: entry points
+ * that need one return KHRR_ERR_STATE until the next successful upload. */
 khrr_status khrr_upload_state(khrr_ctx* ctx, int64_t n, const double* pos, const double* vel,
                               const double* mass, const double* eps2, int nsys,
                               const int64_t* sys_offsets);

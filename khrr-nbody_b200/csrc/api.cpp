@@ -19,6 +19,7 @@
 #include <cstring>
 #include <map>
 #include <string>
+#include <thread>
 #include <tuple>
 #include <vector>
 
@@ -34,6 +35,67 @@ using namespace khrr;
 namespace {
 
 int64_t round_up(int64_t v, int64_t m) { return (v + m - 1) / m * m; }
+
+// One 128-body tile of the caller's arrays (a system's tiles start at its
+// first body; its last one may be partial): whether every softening is
+// positive and equal to eps2[0], whether every mass equals the tile's first,
+// the smallest h = eps2 / 2 and the sum of |m|.
+struct TileScan {
+    int64_t begin, end;
+    int sys;
+    bool pos_eps, same_eps, same_mass;
+    double hmin, msum;
+};
+
+void scan_tile(const double* mass, const double* eps2, double e0, TileScan& t) {
+    const double m0 = mass[t.begin];
+    bool pos = true, same_e = true, same_m = true;
+    double h = 1e300, s[4] = {0.0, 0.0, 0.0, 0.0};
+    for (int64_t i = t.begin; i < t.end; ++i) {
+        const double e = eps2[i], m = mass[i];
+        pos &= e > 0.0;
+        same_e &= e == e0;
+        same_m &= m == m0;
+        h = std::min(h, e);
+        s[(i - t.begin) & 3] += std::fabs(m);  // four running sums, added pairwise
+    }
+    t.pos_eps = pos;
+    t.same_eps = same_e;
+    t.same_mass = same_m;
+    t.hmin = 0.5 * h;
+    t.msum = (s[0] + s[1]) + (s[2] + s[3]);
+}
+
+// All tiles of an upload.  The tiles are independent, so a large upload
+// splits them over host threads; each tile's result is the same whatever the
+// split.
+std::vector<TileScan> scan_state_tiles(const double* mass, const double* eps2, const std::vector<int64_t>& off) {
+    std::vector<TileScan> tiles;
+    const int nsys = static_cast<int>(off.size()) - 1;
+    tiles.reserve(static_cast<size_t>(off[nsys] / kPad + nsys));
+    for (int k = 0; k < nsys; ++k)
+        for (int64_t b = off[k]; b < off[k + 1]; b += kPad)
+            tiles.push_back(TileScan{b, std::min(b + kPad, off[k + 1]), k, false, false, false, 0.0, 0.0});
+    const double e0 = eps2[0];
+    const unsigned hw = std::thread::hardware_concurrency();
+    const int nthreads = off[nsys] < (int64_t(1) << 17) ? 1 : static_cast<int>(std::clamp(hw, 1u, 8u));
+    const size_t per = (tiles.size() + nthreads - 1) / nthreads;
+    auto work = [&](int r) {
+        const size_t t1 = std::min(tiles.size(), (r + 1) * per);
+        for (size_t t = r * per; t < t1; ++t) scan_tile(mass, eps2, e0, tiles[t]);
+    };
+    std::vector<std::thread> pool;
+    int started = 1;
+    try {
+        for (; started < nthreads; ++started) pool.emplace_back(work, started);
+    } catch (...) {
+        // No more threads: the ranges not started run here.
+    }
+    for (int r = started; r < nthreads; ++r) work(r);
+    work(0);
+    for (std::thread& th : pool) th.join();
+    return tiles;
+}
 
 }  // namespace
 
@@ -709,46 +771,25 @@ khrr_status khrr_upload_state(khrr_ctx* c, int64_t n, const double* pos, const d
     if (off[0] != 0 || off[nsys] != n) return c->fail(KHRR_ERR_INVALID_ARG, "system offsets must span [0, n]");
     for (int k = 0; k < nsys; ++k)
         if (off[k + 1] <= off[k]) return c->fail(KHRR_ERR_INVALID_ARG, "system %d is empty", k);
-    // One pass over the bodies: every softening positive, whether they are
-    // all equal, and per system its total |mass| and smallest h = eps2 / 2 and
-    // per 128-body tile of it the smallest h (the fixed-point scales below).
-    bool uniform_new = true;
-    std::vector<double> sys_msum(static_cast<size_t>(nsys), 0.0), sys_hmin(static_cast<size_t>(nsys), 1e300);
-    std::vector<double> tile_hmin;
-    tile_hmin.reserve(static_cast<size_t>(n / kPad + nsys));
-    for (int k = 0; k < nsys; ++k) {
-        double msum = 0.0, hsys = 1e300;
-        for (int64_t b = off[k]; b < off[k + 1]; b += kPad) {
-            const int64_t e_end = std::min(b + kPad, off[k + 1]);
-            double ht = 1e300;
-            for (int64_t i = b; i < e_end; ++i) {
-                const double e = eps2[i];
-                if (!(e > 0.0)) return c->fail(KHRR_ERR_INVALID_ARG, "eps2[%lld] must be > 0", (long long)i);
-                uniform_new = uniform_new && e == eps2[0];
-                ht = std::min(ht, 0.5 * e);
-                msum += std::fabs(mass[i]);
-            }
-            hsys = std::min(hsys, ht);
-            tile_hmin.push_back(ht);
-        }
-        sys_msum[k] = msum;
-        sys_hmin[k] = hsys;
-    }
-    cudaSetDevice(c->device);
-    // Same layout as the current state: plans and captured graphs stay valid.
-    const bool same_layout = c->has_state && c->off == off && c->uniform == uniform_new &&
-                             c->h_uniform == static_cast<float>(0.5 * eps2[0]);
-    c->off.assign(off.begin(), off.end());
-    c->cnt.resize(nsys);
-    c->poff.resize(nsys + 1);
+    std::vector<int64_t> cnt(static_cast<size_t>(nsys)), poff(static_cast<size_t>(nsys) + 1);
     int64_t p = 0;
     for (int k = 0; k < nsys; ++k) {
-        c->cnt[k] = off[k + 1] - off[k];
-        c->poff[k] = p;
-        p += round_up(c->cnt[k], kPad);
+        cnt[k] = off[k + 1] - off[k];
+        poff[k] = p;
+        p += round_up(cnt[k], kPad);
     }
-    c->poff[nsys] = p;
+    poff[nsys] = p;
     if (p > (int64_t(1) << 30)) return c->fail(KHRR_ERR_INVALID_ARG, "too many bodies");
+    cudaSetDevice(c->device);
+    const bool same_offsets = c->has_state && c->off == off;
+    // From here on the device arrays are rewritten: whatever the outcome, the
+    // previous state is gone, and a failed upload leaves the context without
+    // state.
+    c->has_state = false;
+    c->predicted = false;
+    c->off = off;
+    c->cnt = cnt;
+    c->poff = poff;
     c->n = n;
     c->npad = p;
     const size_t np = static_cast<size_t>(p);
@@ -758,6 +799,8 @@ khrr_status khrr_upload_state(khrr_ctx* c, int64_t n, const double* pos, const d
     for (DevBuf<double>* b : {&c->mass, &c->eps2, &c->phi})
         if ((st = c->cuda(b->ensure(np), "alloc state")) != KHRR_OK) return st;
     if ((st = c->cuda(c->shadow_buf.ensure(5 * np), "alloc shadow")) != KHRR_OK) return st;
+    if ((st = c->cuda(c->tile_mass.ensure(np / kPad), "alloc tile masses")) != KHRR_OK) return st;
+    if ((st = c->cuda(c->fx_scale.ensure(np / kPad), "alloc tile scales")) != KHRR_OK) return st;
     cudaStream_t s = c->stream;
     for (DevBuf<double>* b : {&c->pos, &c->vel, &c->acc, &c->post, &c->velt, &c->acct})
         cudaMemsetAsync(b->p, 0, 3 * np * sizeof(double), s);
@@ -766,57 +809,17 @@ khrr_status khrr_upload_state(khrr_ctx* c, int64_t n, const double* pos, const d
     // bodies' values are copied straight from the caller's array below.
     std::vector<double> ghost_eps2(np - static_cast<size_t>(n));
     for (int k = 0, g = 0; k < nsys; ++k) {
-        const int64_t pad = c->poff[k + 1] - c->poff[k] - c->cnt[k];
+        const int64_t pad = poff[k + 1] - poff[k] - cnt[k];
         std::fill(ghost_eps2.begin() + g, ghost_eps2.begin() + g + pad, eps2[off[k]]);
         g += static_cast<int>(pad);
     }
-    c->uniform = uniform_new;
-    c->h_uniform = static_cast<float>(0.5 * eps2[0]);
-    // One mass per 128-body tile (and no ghosts) lets the kernel factor the
-    // mass out of each tile sum; the reference's layouts have it (component
-    // counts are multiples of 1024).
-    std::vector<float> tm(np / kPad, 0.0f);
-    bool tile_uniform = true;
-    for (int k = 0; k < nsys && tile_uniform; ++k) {
-        if (c->cnt[k] % kPad) tile_uniform = false;
-        for (int64_t b = 0; b < c->cnt[k] && tile_uniform; b += kPad) {
-            const double m0 = mass[off[k] + b];
-            for (int64_t q = 1; q < kPad; ++q)
-                if (mass[off[k] + b + q] != m0) tile_uniform = false;
-            tm[(c->poff[k] + b) / kPad] = static_cast<float>(m0);
-        }
-    }
-    if (tile_uniform != c->tile_uniform_mass) c->drop_graphs();
-    c->tile_uniform_mass = tile_uniform;
-    // The pair kernel's blocks: with one mass per tile, runs of equal-mass
-    // tiles cut at 1024 bodies (one mass per block: the block-mass form);
-    // otherwise 1024-body blocks.
-    PairBlocks blocks = tile_uniform ? pair_blocks_by_mass(c->poff, tm) : pair_blocks_fixed(c->poff);
-    if (tile_uniform != c->block_uniform_mass || blocks != c->pair_blocks) {
-        c->plan_batched.valid = false;
-        c->drop_graphs();
-    }
-    c->block_uniform_mass = tile_uniform;
-    c->pair_blocks = std::move(blocks);
-    if ((st = c->cuda(c->tile_mass.ensure(tm.size()), "alloc tile masses")) != KHRR_OK) return st;
-    // Scales of the pair kernel's fixed-point sums per 128-body tile, from the
-    // tile's smallest h = eps2 / 2, its system's smallest h and total |mass|
-    // (real bodies; ghosts carry the system's first softening and no sums).
-    c->fx_scales.assign(tm.size(), FxScale{1.0, 1.0, 1.0, 1.0});
-    for (int k = 0, t = 0; k < nsys; ++k)
-        for (int64_t b = 0; b < c->cnt[k]; b += kPad, ++t)
-            c->fx_scales[(c->poff[k] + b) / kPad] = fx_scale(tile_hmin[t], sys_hmin[k], sys_msum[k]);
-    if ((st = c->cuda(c->fx_scale.ensure(tm.size()), "alloc tile scales")) != KHRR_OK) return st;
-    if ((st = c->cuda(cudaMemcpyAsync(c->fx_scale.p, c->fx_scales.data(), tm.size() * sizeof(FxScale),
-                                      cudaMemcpyHostToDevice, s),
-                      "upload")) != KHRR_OK)
-        return st;
-    st = c->cuda(cudaMemcpyAsync(c->tile_mass.p, tm.data(), tm.size() * sizeof(float), cudaMemcpyHostToDevice, s),
-                 "upload");
+    // The copies first: the scan of the caller's masses and softenings below
+    // runs on the host while they are in flight.
+    st = KHRR_OK;
     for (int k = 0, g = 0; k < nsys && st == KHRR_OK; ++k) {
-        const size_t o = static_cast<size_t>(off[k]), q = static_cast<size_t>(c->poff[k]);
-        const size_t m = static_cast<size_t>(c->cnt[k]);
-        const size_t pad = static_cast<size_t>(c->poff[k + 1]) - q - m;
+        const size_t o = static_cast<size_t>(off[k]), q = static_cast<size_t>(poff[k]);
+        const size_t m = static_cast<size_t>(cnt[k]);
+        const size_t pad = static_cast<size_t>(poff[k + 1]) - q - m;
         st = c->cuda(cudaMemcpyAsync(c->eps2.p + q, eps2 + o, m * sizeof(double), cudaMemcpyHostToDevice, s), "upload");
         if (st == KHRR_OK && pad)
             st = c->cuda(cudaMemcpyAsync(c->eps2.p + q + m, ghost_eps2.data() + g, pad * sizeof(double),
@@ -830,11 +833,69 @@ khrr_status khrr_upload_state(khrr_ctx* c, int64_t n, const double* pos, const d
         if (st == KHRR_OK)
             st = c->cuda(cudaMemcpyAsync(c->mass.p + q, mass + o, m * sizeof(double), cudaMemcpyHostToDevice, s), "upload");
     }
-    if (st != KHRR_OK) return st;
-    if ((st = c->cuda(launch_pack(c->pos.p, c->mass.p, c->eps2.p, c->npad, c->npad, c->shadow(), s),
-                      "pack")) != KHRR_OK)
+    if (st != KHRR_OK) {
+        cudaStreamSynchronize(s);  // no copy may still read the caller's arrays
         return st;
-    if ((st = c->cuda(cudaStreamSynchronize(s), "upload sync")) != KHRR_OK) return st;
+    }
+    const std::vector<TileScan> tiles = scan_state_tiles(mass, eps2, off);
+    for (size_t t = 0; t < tiles.size(); ++t) {
+        if (tiles[t].pos_eps) continue;
+        cudaStreamSynchronize(s);
+        for (int64_t i = tiles[t].begin; i < tiles[t].end; ++i)
+            if (!(eps2[i] > 0.0)) return c->fail(KHRR_ERR_INVALID_ARG, "eps2[%lld] must be > 0", (long long)i);
+    }
+    // Per system its total |mass| (tile sums in tile order) and smallest
+    // h = eps2 / 2; per padded 128-body tile the first mass; whether every
+    // softening equals eps2[0] and whether every tile has one mass (and no
+    // ghosts).
+    bool uniform_new = true, tile_uniform = true;
+    std::vector<double> sys_msum(static_cast<size_t>(nsys), 0.0), sys_hmin(static_cast<size_t>(nsys), 1e300);
+    std::vector<float> tm(np / kPad, 0.0f);
+    for (const TileScan& t : tiles) {
+        uniform_new = uniform_new && t.same_eps;
+        tile_uniform = tile_uniform && t.same_mass && t.end - t.begin == kPad;
+        sys_msum[t.sys] += t.msum;
+        sys_hmin[t.sys] = std::min(sys_hmin[t.sys], t.hmin);
+        tm[(poff[t.sys] + t.begin - off[t.sys]) / kPad] = static_cast<float>(mass[t.begin]);
+    }
+    const bool same_layout = same_offsets && c->uniform == uniform_new &&
+                             c->h_uniform == static_cast<float>(0.5 * eps2[0]);
+    c->uniform = uniform_new;
+    c->h_uniform = static_cast<float>(0.5 * eps2[0]);
+    // One mass per 128-body tile (and no ghosts) lets the kernel factor the
+    // mass out of each tile sum; the reference's layouts have it (component
+    // counts are multiples of 1024).
+    if (tile_uniform != c->tile_uniform_mass) c->drop_graphs();
+    c->tile_uniform_mass = tile_uniform;
+    // The pair kernel's blocks: with one mass per tile, runs of equal-mass
+    // tiles cut at 1024 bodies (one mass per block: the block-mass form);
+    // otherwise 1024-body blocks.
+    PairBlocks blocks = tile_uniform ? pair_blocks_by_mass(poff, tm) : pair_blocks_fixed(poff);
+    if (tile_uniform != c->block_uniform_mass || blocks != c->pair_blocks) {
+        c->plan_batched.valid = false;
+        c->drop_graphs();
+    }
+    c->block_uniform_mass = tile_uniform;
+    c->pair_blocks = std::move(blocks);
+    // Scales of the pair kernel's fixed-point sums per 128-body tile, from the
+    // tile's smallest h = eps2 / 2, its system's smallest h and total |mass|
+    // (real bodies; ghosts carry the system's first softening and no sums).
+    c->fx_scales.assign(tm.size(), FxScale{1.0, 1.0, 1.0, 1.0});
+    for (const TileScan& t : tiles)
+        c->fx_scales[(poff[t.sys] + t.begin - off[t.sys]) / kPad] =
+            fx_scale(t.hmin, sys_hmin[t.sys], sys_msum[t.sys]);
+    st = c->cuda(cudaMemcpyAsync(c->fx_scale.p, c->fx_scales.data(), tm.size() * sizeof(FxScale),
+                                 cudaMemcpyHostToDevice, s),
+                 "upload");
+    if (st == KHRR_OK)
+        st = c->cuda(cudaMemcpyAsync(c->tile_mass.p, tm.data(), tm.size() * sizeof(float), cudaMemcpyHostToDevice, s),
+                     "upload");
+    if (st == KHRR_OK)
+        st = c->cuda(launch_pack(c->pos.p, c->mass.p, c->eps2.p, c->npad, c->npad, c->shadow(), s), "pack");
+    // The host vectors above are sources of the copies: wait for them either way.
+    const khrr_status sync = c->cuda(cudaStreamSynchronize(s), "upload sync");
+    if (st != KHRR_OK) return st;
+    if (sync != KHRR_OK) return sync;
     if (!same_layout) {
         c->plan_batched.valid = false;
         c->plan_plain.valid = false;
@@ -842,7 +903,6 @@ khrr_status khrr_upload_state(khrr_ctx* c, int64_t n, const double* pos, const d
         c->drop_graphs();
     }
     c->has_state = true;
-    c->predicted = false;
     return KHRR_OK;
 }
 

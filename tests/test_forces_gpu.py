@@ -374,3 +374,48 @@ def test_empty_inputs_are_no_ops(ctx, torch_cuda):
     ctx.apply_cells_to_particles(p, one.data_ptr(), p, one.data_ptr(), ints.data_ptr(), 0)
     ctx.synchronize()
     assert bool((sentinel == 7.0).all()) and bool((one == 1.0).all()) and bool((ints == 5).all())
+
+
+def test_upload_checks_softenings_and_fails_without_state(ctx, oracle):
+    """A softening <= 0 is refused with its index, also when it sits in a late
+    tile of a large upload (the per-tile check runs on several host threads
+    above 131,072 bodies) and whether it is zero or NaN; the failed upload
+    leaves no state behind (KHRR_ERR_STATE until the next upload), and the
+    next upload of the same arrays gives the same forces as before."""
+    import khrr
+    pos, vel, mass, eps2 = galaxy(1000, 2001, seed=71, eps_d=0.006)
+    ctx.upload(pos, vel, mass, eps2)
+    ctx.forces(khrr.ACC)
+    good = ctx.download()["acc"]
+    for bad_index, bad in ((2500, 0.0), (17, float("nan"))):
+        e = eps2.copy()
+        e[bad_index] = bad
+        with pytest.raises(khrr.KhrrError, match=f"eps2\\[{bad_index}\\]") as info:
+            ctx.upload(pos, vel, mass, e)
+        assert info.value.status == 1
+        with pytest.raises(khrr.KhrrError) as info:
+            ctx.forces(khrr.ACC)
+        assert info.value.status == 6
+    ctx.upload(pos, vel, mass, eps2)
+    ctx.forces(khrr.ACC)
+    assert np.array_equal(ctx.download()["acc"], good)
+
+    # 200,000 bodies in three ragged systems (threaded scan), bad softening near the end
+    big = [galaxy(20000, 40001, seed=72), galaxy(30000, 50000, seed=73, eps_s=0.003), galaxy(20000, 39999, seed=74)]
+    P = np.concatenate([b[0] for b in big])
+    V = np.concatenate([b[1] for b in big])
+    M = np.concatenate([b[2] for b in big])
+    E = np.concatenate([b[3] for b in big])
+    off = np.cumsum([0] + [len(b[2]) for b in big])
+    e = E.copy()
+    e[len(E) - 3] = -1.0
+    with pytest.raises(khrr.KhrrError, match=f"eps2\\[{len(E) - 3}\\]"):
+        ctx.upload(P, V, M, e, offsets=off)
+    ctx.upload(P, V, M, E, offsets=off)
+    ctx.forces(khrr.ACC | khrr.PHI)
+    out = ctx.download()
+    k = 1  # the middle system against the FP64 oracle on a sample of its bodies
+    s = slice(off[k], off[k + 1])
+    idx = np.arange(0, off[k + 1] - off[k], 97)
+    assert rel_rms(out["acc"][s][idx], oracle.accel_f64(P[s], M[s], E[s], targets=idx)) <= 1e-6
+    assert rel_rms(out["phi"][s][idx], oracle.phi_f64(P[s], M[s], E[s], targets=idx)) <= 1e-6
