@@ -123,7 +123,7 @@ khrr_status khrr_ctx::check_device_flag() {
     if (e != cudaSuccess) return cuda(e, "device error flag");
     if (flag & kErrTimeout) {
         cudaMemsetAsync(errflag.p, 0, sizeof(unsigned), stream);
-        return fail(KHRR_ERR_TIMEOUT, "a kernel gave up waiting for an asynchronous copy (bounded wait)");
+        return fail(KHRR_ERR_TIMEOUT, "a kernel gave up a bounded wait (an asynchronous copy or a neighbour plane)");
     }
     return KHRR_OK;
 }

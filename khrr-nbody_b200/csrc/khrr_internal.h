@@ -309,7 +309,19 @@ struct WaveMaps {
     CUtensorMap tile[4], tile_mass;  // 32 x 8 boxes: phi^{n-1} and mass (one-step kernel)
     bool ok = false;
     bool two_step = false;           // pairs of iterations through the two-step kernel
+    // The shared-memory-resident kernel (nx = 128): its nx + 1 plane counters.
+    bool resident = false;
+    unsigned* sync = nullptr;
 };
+// Whether the shared-memory-resident FP32 stencil runs for this mesh edge on
+// the current device (nx = 128, one 197 KB CTA per plane, all co-resident).
+bool wave_resident_available(int nx);
+// k FP32 iterations of the ring in one cooperative launch with the field
+// resident in shared memory, bit-identical to k launch_wave_f32 iterations and
+// leaving the ring in the state enqueue_wave_f32 leaves it; sync: nx + 1
+// counters (zeroed here); bounded waits report into err.
+cudaError_t launch_wave_resident(float* ring, int64_t cells, const float* mass, const WaveF32& w, int k, int st,
+                                 double* resid, unsigned* sync, unsigned* err, cudaStream_t s);
 // One FP32 iteration fed by tensor copies (wave1_tma_kernel), bit-identical
 // to launch_wave_f32.
 cudaError_t launch_wave1_tma(float* phi_new, const CUtensorMap& phi, const CUtensorMap& phi_old,
@@ -321,9 +333,10 @@ cudaError_t launch_wave1_tma(float* phi_new, const CUtensorMap& phi, const CUten
 cudaError_t launch_wave2_tma(float* out1, float* out2, const CUtensorMap& phi, const CUtensorMap& phi_old,
                              const CUtensorMap& mass, const WaveF32& w, double* resid, unsigned* err, cudaStream_t s);
 // Enqueues k FP32 iterations on the ring (4 buffers of cells floats) from
-// state st; resid (may be NULL) is reduced by the last one.  With maps (ok)
-// the pairs run through the tensor-copy kernel, whose bounded waits report
-// into err.
+// state st; resid (may be NULL) is reduced by the last one.  With maps
+// (resident, nx = 128) and err, all k run in one shared-memory-resident
+// launch; else with maps (ok) the pairs run through the tensor-copy kernel.
+// Bounded waits of both report into err.
 cudaError_t enqueue_wave_f32(float* ring, int64_t cells, const float* mass, const WaveF32& w, int k, int st,
                              double* resid, cudaStream_t s, const WaveMaps* maps = nullptr, unsigned* err = nullptr);
 cudaError_t launch_acc_field(double* cell_acc, double* cell_acc_abs, const double* phi, int nx, double dx,

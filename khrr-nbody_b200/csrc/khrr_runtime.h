@@ -110,6 +110,7 @@ struct MeshSolver {
     DevBuf<int2> pci;                           // npad
     DevBuf<double4> part;                       // npad: {acc, -phi} per body
     WaveMaps maps;                              // tensor maps of phi32 / mass32
+    DevBuf<unsigned> sync;                      // nx + 1 plane counters of the resident stencil
     DevBuf<unsigned char> ns;                   // npad: 1 for real bodies, 0 for ghosts
     std::vector<int64_t> layout_poff, layout_cnt;  // the layout pci/part/ns were sized for
     int rot = kRingStart;                       // ring state: 4 * (phi^{n-1} buffer) + phi^n buffer
@@ -181,6 +182,7 @@ struct khrr_ctx {
     int wave_nx = 0;
     int wave_rot = khrr::kRingStart;                     // ring state: 4 * (phi^{n-1} buffer) + phi^n buffer
     khrr::WaveMaps wave_maps;                            // tensor maps of wave_phi / wave_mass
+    khrr::DevBuf<unsigned> wave_sync;                    // nx + 1 plane counters of the resident stencil
     bool wave_warm = false;
     std::map<std::pair<int, int>, khrr::StepGraph> wave_graphs;  // (chunk, rotation)
 

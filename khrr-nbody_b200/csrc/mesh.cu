@@ -929,6 +929,237 @@ __global__ void __launch_bounds__((kW1Consumers + 1) * 32) wave1_tma_kernel(floa
     }
 }
 
+// k FP32 iterations in one launch with the field resident in shared memory
+// (nx = 128: the 128^3 mesh of the two-galaxy encounter).  CTA z owns plane z
+// for the whole launch: phi^n of the plane in shared memory (two buffers,
+// alternating by iteration), phi^{n-1} and the mass term in registers, the
+// sponge factor w = 1/(1 + Q) of every cell in shared memory.  A warp covers
+// one 128-cell row, four consecutive x cells per lane (16-byte shared and
+// global accesses; x neighbours from the float4 and by shuffles).  Per
+// iteration a CTA reads only its two neighbours' planes phi^n (z - 1, z + 1)
+// from global memory (L2), and writes its new plane to the ring buffer the
+// one-launch-per-iteration path would write, so the ring ends in the same
+// state.  Planes are exchanged through per-plane counters: after iteration t
+// a CTA sets flag[z] = t + 1 (release); before iteration t (t >= 1) it waits
+// for flag[z - 1] and flag[z + 1] >= t.  That wait also keeps every CTA at
+// most one iteration ahead of its neighbours, so a ring buffer is overwritten
+// only once both neighbours have finished the iteration that read it (it
+// holds phi^{t-2} or older when iteration t writes phi^{t+1}).  Every wait is
+// bounded (2 s of wall time); a CTA that gives up sets err (kErrTimeout) and
+// flag[nx] (abort), and every other wait ends on that flag.  The grid is one
+// CTA per plane, launched cooperatively so all of them are resident.  Per
+// cell the arithmetic is wave_f32_kernel's, in its order, so the bits are
+// the same; the residual of the last iteration is summed per warp and added
+// with one FP64 atomic pair per warp (its last bits depend on the order).
+//
+// Measured on the encounter's mesh (CUDA events): 7.1 us per iteration in a
+// 1000-iteration solve against 10.4 us with one launch per iteration, the
+// Wave-mode step (507 iterations) 3.64 against 4.17 ms.  1024 threads (16
+// cells each, 64 registers): 7.3 us; one cell per thread instead of four
+// (16 cells each): 7.6 us.  Timing-only copies of the one-cell form put the
+// cost in the exchange through L2: 6.6 us without the neighbour waits, 3.7
+// us without the neighbour-plane loads as well.
+constexpr int kRzNX = 128;                                // mesh edge
+#ifndef KHRR_WAVE_RZ_THREADS
+#define KHRR_WAVE_RZ_THREADS 512
+#endif
+constexpr int kRzThreads = KHRR_WAVE_RZ_THREADS;
+constexpr int kRzRows = kRzThreads / 32;                  // rows per pass (a warp = one 128-cell row)
+constexpr int kRzPasses = kRzNX / kRzRows;                // passes per plane
+constexpr int kRzCells = 4 * kRzPasses;                   // cells per thread
+constexpr int kRzPlane = kRzNX * kRzNX;
+constexpr size_t kRzSmem = (3 * static_cast<size_t>(kRzPlane) + kRzNX) * sizeof(float);  // 197,120 B
+static_assert(kRzNX == 4 * 32 && kRzNX % kRzRows == 0, "a warp covers a row, four cells per lane");
+
+__device__ __forceinline__ unsigned ld_acquire_gpu(const unsigned* p) {
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ void st_release_gpu(unsigned* p, unsigned v) {
+    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// Free buffers f0 < f1 of the four-buffer ring besides o and c.
+__device__ __forceinline__ void ring_free_dev(int o, int c, int& f0, int& f1) {
+    int f[2], n = 0;
+#pragma unroll
+    for (int b = 0; b < 4; ++b)
+        if (b != o && b != c && n < 2) f[n++] = b;
+    f0 = f[0];
+    f1 = f[1];
+}
+
+__global__ void __launch_bounds__(kRzThreads, 1) wave_resident_kernel(float* __restrict__ ring, int64_t cz,
+                                                                      const float* __restrict__ mass,
+                                                                      const WaveF32 W, int k, int st,
+                                                                      double* __restrict__ resid,
+                                                                      unsigned* __restrict__ flag,
+                                                                      unsigned* __restrict__ err) {
+    extern __shared__ __align__(16) float rz_smem[];
+    float* sphi = rz_smem;                  // [2][plane]: phi^n by iteration parity
+    float* sw = rz_smem + 2 * kRzPlane;     // [plane]: w = 1 / (1 + Q)
+    float* ssy = sw + kRzPlane;             // [nx]: the y sponge table
+    const int z = blockIdx.x, tid = threadIdx.x;
+    const int lane = tid & 31, iy0 = tid >> 5;
+    const int x0 = 4 * lane;  // the lane's cells x0 .. x0 + 3 of each of its rows
+    const bool zface = z == 0 || z == kRzNX - 1;
+    const int64_t zoff = static_cast<int64_t>(z) * kRzPlane;
+    float sxb[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) sxb[j] = W.diss_base + W.sx[x0 + j];
+    const float szz = W.sz[z];
+    int old = st / 4, cur = st % 4;
+    if (tid < kRzNX) ssy[tid] = W.sy[tid];
+
+    float po[kRzCells], msw[kRzCells];  // phi^{n-1}; mass times S w
+#pragma unroll
+    for (int p = 0; p < kRzPasses; ++p) {
+        const int iy = iy0 + kRzRows * p, q = iy * kRzNX + x0;
+        const float4 m4 = *reinterpret_cast<const float4*>(mass + zoff + q);
+        const float4 o4 = *reinterpret_cast<const float4*>(ring + old * cz + zoff + q);
+        const float4 c4 = *reinterpret_cast<const float4*>(ring + cur * cz + zoff + q);
+        const float mj[4] = {m4.x, m4.y, m4.z, m4.w}, oj[4] = {o4.x, o4.y, o4.z, o4.w};
+        float wj[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const float sxy = sxb[j] + W.sy[iy];
+            const float diss = sxy + szz;
+            const float Q = diss * W.cdt_half;
+            wj[j] = __frcp_rn(1.0f + Q);
+            msw[4 * p + j] = mj[j] * (W.S * wj[j]);
+            po[4 * p + j] = oj[j];
+        }
+        *reinterpret_cast<float4*>(sw + q) = make_float4(wj[0], wj[1], wj[2], wj[3]);
+        *reinterpret_cast<float4*>(sphi + q) = c4;
+    }
+    double d2 = 0.0, n2 = 0.0;
+    const int pairs = k / 2;
+    int pending = 0;
+    __shared__ int s_abort;
+    for (int t = 0; t < k; ++t) {
+        // This iteration's output buffer, as enqueue_wave_f32 sequences them:
+        // pairs write the two free buffers f0 then f1, an odd last one f0.
+        int ob;
+        if (t < 2 * pairs && (t & 1)) {
+            ob = pending;
+        } else {
+            int f0, f1;
+            ring_free_dev(old, cur, f0, f1);
+            ob = f0;
+            pending = f1;
+        }
+        if (tid == 0) {
+            int abort = 0;
+            if (t > 0) {
+                // Both counters in flight together; the abort flag and the
+                // clock only every 64th poll.  A face plane has one
+                // neighbour: its own counter (already >= t) stands in.
+                const unsigned* fa = flag + (z > 0 ? z - 1 : z);
+                const unsigned* fb = flag + (z < kRzNX - 1 ? z + 1 : z);
+                const unsigned need = static_cast<unsigned>(t);
+                unsigned a = ld_acquire_gpu(fa), b = ld_acquire_gpu(fb);
+                if (a < need || b < need) {
+                    const uint64_t t0 = global_ns();
+                    for (unsigned spin = 1;; ++spin) {
+                        a = ld_acquire_gpu(fa);
+                        b = ld_acquire_gpu(fb);
+                        if (a >= need && b >= need) break;
+                        if ((spin & 63u) == 0u) {
+                            if (ld_acquire_gpu(flag + kRzNX) != 0u) {
+                                abort = 1;
+                                break;
+                            }
+                            if (global_ns() - t0 > 2000000000ull) {
+                                atomicOr(err, kErrTimeout);
+                                st_release_gpu(flag + kRzNX, 1u);
+                                abort = 1;
+                                break;
+                            }
+                        }
+                    }
+                }
+            }
+            s_abort = abort;
+        }
+        __syncthreads();
+        if (s_abort) return;  // uniform across the CTA; no barrier follows
+        const float* rd = sphi + (t & 1) * kRzPlane;
+        float* wr = sphi + ((t + 1) & 1) * kRzPlane;
+        // z neighbours (face planes read none)
+        const float* zm = ring + cur * cz + (zface ? zoff : zoff - kRzPlane);
+        const float* zp = ring + cur * cz + (zface ? zoff : zoff + kRzPlane);
+        float* out_g = ring + ob * cz + zoff;
+        const bool last = t == k - 1 && resid != nullptr;
+        // Every load is unconditional (neighbour rows clamped into the plane,
+        // face cells discard the value), so the loads of all the thread's
+        // rows can be in flight together.  x neighbours come from the row's
+        // float4 and, across lanes, by shuffles.
+#pragma unroll
+        for (int p = 0; p < kRzPasses; ++p) {
+            const int iy = iy0 + kRzRows * p, q = iy * kRzNX + x0;
+            const int qym = iy > 0 ? q - kRzNX : q, qyp = iy < kRzNX - 1 ? q + kRzNX : q;
+            const float4 c4 = *reinterpret_cast<const float4*>(rd + q);
+            const float4 ym4 = *reinterpret_cast<const float4*>(rd + qym);
+            const float4 yp4 = *reinterpret_cast<const float4*>(rd + qyp);
+            const float4 w4 = *reinterpret_cast<const float4*>(sw + q);
+            const float4 zm4 = __ldcg(reinterpret_cast<const float4*>(zm + q));
+            const float4 zp4 = __ldcg(reinterpret_cast<const float4*>(zp + q));
+            float left = __shfl_up_sync(0xffffffffu, c4.w, 1);
+            float right = __shfl_down_sync(0xffffffffu, c4.x, 1);
+            if (lane == 0) left = c4.x;    // x = 0 is a face
+            if (lane == 31) right = c4.w;  // x = nx - 1 is a face
+            const float cj[4] = {c4.x, c4.y, c4.z, c4.w};
+            const float xm[4] = {left, c4.x, c4.y, c4.z}, xp[4] = {c4.y, c4.z, c4.w, right};
+            const float ym[4] = {ym4.x, ym4.y, ym4.z, ym4.w}, yp[4] = {yp4.x, yp4.y, yp4.z, yp4.w};
+            const float zmj[4] = {zm4.x, zm4.y, zm4.z, zm4.w}, zpj[4] = {zp4.x, zp4.y, zp4.z, zp4.w};
+            const float wj[4] = {w4.x, w4.y, w4.z, w4.w};
+            const bool yface = zface || iy == 0 || iy == kRzNX - 1;
+            const float sy = ssy[iy];
+            float oj[4];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const int u = 4 * p + j;
+                const float nb = ((xm[j] + xp[j]) + (ym[j] + yp[j])) + (zmj[j] + zpj[j]);
+                const float sxy = sxb[j] + sy;
+                const float diss = sxy + szz;
+                const float Q = diss * W.cdt_half;
+                const float w = wj[j];
+                const float val = fmaf(nb, W.K * w, fmaf(cj[j], W.A * w, fmaf(po[u], (Q - 1.0f) * w, msw[u])));
+                const bool face = yface || (lane == 0 && j == 0) || (lane == 31 && j == 3);
+                oj[j] = face ? 0.0f : val;
+                if (last) {
+                    const double dd = static_cast<double>(oj[j]) - static_cast<double>(cj[j]);
+                    d2 += dd * dd;
+                    n2 += static_cast<double>(oj[j]) * static_cast<double>(oj[j]);
+                }
+                po[u] = cj[j];
+            }
+            const float4 o4 = make_float4(oj[0], oj[1], oj[2], oj[3]);
+            *reinterpret_cast<float4*>(wr + q) = o4;
+            *reinterpret_cast<float4*>(out_g + q) = o4;
+        }
+        __syncthreads();  // the plane is written (shared and global); rd is free
+        // The barrier orders the CTA's stores before thread 0's release.
+        if (tid == 0) st_release_gpu(flag + z, static_cast<unsigned>(t + 1));
+        old = cur;
+        cur = ob;
+    }
+    if (resid) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            d2 += __shfl_xor_sync(0xffffffffu, d2, o);
+            n2 += __shfl_xor_sync(0xffffffffu, n2, o);
+        }
+        if ((tid & 31) == 0) {
+            atomicAdd(&resid[0], d2);
+            atomicAdd(&resid[1], n2);
+        }
+    }
+}
+
+
 // acc_field (p2mesh-kernel.cuh:169-225) with a 3-D launch over the mesh.
 __global__ void acc_field_kernel(double* __restrict__ cell_acc, double* __restrict__ cell_acc_abs,
                                  const double* __restrict__ phi, int NX, double DX) {
@@ -1203,9 +1434,47 @@ cudaError_t launch_wave_f32(float* phi_new, const float* phi, const float* phi_o
     return cudaLaunchKernelEx(&cfg, wave_f32_kernel<4>, phi_new, phi, phi_old, mass, w, resid);
 }
 
+bool wave_resident_available(int nx) {
+    if (nx != kRzNX) return false;
+    static const bool ok = [] {
+        int dev = 0, sms = 0, coop = 0, occ = 0;
+        if (cudaGetDevice(&dev) != cudaSuccess ||
+            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+            cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev) != cudaSuccess || !coop)
+            return false;
+        if (cudaFuncSetAttribute(wave_resident_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 static_cast<int>(kRzSmem)) != cudaSuccess ||
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, wave_resident_kernel, kRzThreads, kRzSmem) !=
+                cudaSuccess)
+            return false;
+        return occ >= 1 && static_cast<int64_t>(occ) * sms >= kRzNX;
+    }();
+    return ok;
+}
+
+cudaError_t launch_wave_resident(float* ring, int64_t cells, const float* mass, const WaveF32& w, int k, int st,
+                                 double* resid, unsigned* sync, unsigned* err, cudaStream_t s) {
+    if (k < 1) return cudaSuccess;
+    cudaError_t e = cudaMemsetAsync(sync, 0, (kRzNX + 1) * sizeof(unsigned), s);
+    if (e != cudaSuccess) return e;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(kRzNX);
+    cfg.blockDim = dim3(kRzThreads);
+    cfg.dynamicSmemBytes = kRzSmem;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, wave_resident_kernel, ring, cells, mass, w, k, st, resid, sync, err);
+}
+
 cudaError_t enqueue_wave_f32(float* ring, int64_t cells, const float* mass, const WaveF32& w, int k, int st,
                              double* resid, cudaStream_t s, const WaveMaps* maps, unsigned* err) {
     const size_t cz = static_cast<size_t>(cells);
+    if (maps && maps->resident && maps->sync && err && w.nx == kRzNX)
+        return launch_wave_resident(ring, cells, mass, w, k, st, resid, maps->sync, err, s);
     const bool tma = maps && maps->ok && err;
     // One iteration: buffer `out` from phi^n in `cur` and phi^{n-1} in `old`.
     auto single = [&](int old, int cur, int out, double* r) {

@@ -118,8 +118,12 @@ bool make_box_map(CUtensorMap* m, const float* base, int nx, unsigned bx, unsign
 // measured fastest on the 128^3 mesh (10.4 us per iteration against 16.4 and
 // 13.1) and within noise of both on 256^3.  The tensor-copy kernels need
 // 16-byte row strides (nx % 4 == 0) and a mesh at least one box wide.
-void make_wave_maps(WaveMaps* w, float* ring, const float* mass, int nx) {
+void make_wave_maps(WaveMaps* w, float* ring, const float* mass, int nx, unsigned* sync) {
     w->ok = false;
+    // The shared-memory-resident stencil (nx = 128) unless KHRR_WAVE_RESIDENT=0.
+    const char* r = std::getenv("KHRR_WAVE_RESIDENT");
+    w->sync = sync;
+    w->resident = sync && !(r && std::atoi(r) == 0) && wave_resident_available(nx);
     const char* e = std::getenv("KHRR_WAVE_TMA");
     const int mode = e ? std::atoi(e) : 0;
     if ((mode != 1 && mode != 2) || nx % 4 != 0 || nx < 40) return;
@@ -343,6 +347,7 @@ khrr_status khrr_wave_solve(khrr_ctx* c, const khrr_wave_params* p, double tol, 
         if ((st = c->cuda(c->wave_mass.ensure(cz), "alloc")) != KHRR_OK) return st;
         if ((st = c->cuda(c->wave_tab.ensure(3 * static_cast<size_t>(nx)), "alloc")) != KHRR_OK) return st;
         if ((st = c->cuda(c->wave_resid.ensure(2), "alloc")) != KHRR_OK) return st;
+        if ((st = c->cuda(c->wave_sync.ensure(static_cast<size_t>(nx) + 1), "alloc")) != KHRR_OK) return st;
         c->wave_nx = p->nx;
         c->wave_warm = false;
     }
@@ -357,7 +362,7 @@ khrr_status khrr_wave_solve(khrr_ctx* c, const khrr_wave_params* p, double tol, 
         c->wave_rot = kRingStart;
     }
     const WaveF32 w = wave_f32(p, c->wave_tab.p);
-    make_wave_maps(&c->wave_maps, c->wave_phi.p, c->wave_mass.p, p->nx);
+    make_wave_maps(&c->wave_maps, c->wave_phi.p, c->wave_mass.p, p->nx, c->wave_sync.p);
     // Graph of one chunk of `check_every` iterations starting at a ring state;
     // the last iteration of the chunk reduces the residual.
     auto chunk_graph = [&](int k, int rot, StepGraph** out) -> khrr_status {
@@ -518,7 +523,8 @@ khrr_status khrr_set_mesh_solver(khrr_ctx* c, const khrr_mesh_solver* p) {
                                           c->stream),
                           "upload")) != KHRR_OK)
             return st;
-        make_wave_maps(&M.maps, M.phi32.p, M.mass32.p, nx);
+        if ((st = c->cuda(M.sync.ensure(static_cast<size_t>(nx) + 1), "alloc")) != KHRR_OK) return st;
+        make_wave_maps(&M.maps, M.phi32.p, M.mass32.p, nx, M.sync.p);
     }
     M.cfg = *p;
     M.geom = g;

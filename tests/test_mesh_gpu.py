@@ -285,3 +285,54 @@ def test_fp64_wave_iteration_bit_exact_on_random_fields(ctx, torch_cuda, oracle,
         prev, cur = cur, oracle.wave_iter_f64(Wo, cur, prev, mass)
     ctx.synchronize()
     assert np.array_equal(bufs[(3 + 1) % 3].cpu().numpy(), cur)
+
+
+@pytest.mark.parametrize("max_iter,check_every", [(7, 3), (6, 6), (1, 1), (4, 2)])
+def test_resident_stencil_128_bit_exact(ctx, oracle, max_iter, check_every):
+    """The shared-memory-resident FP32 stencil (128^3: one CTA per z plane,
+    all iterations of a chunk in one cooperative launch, neighbour planes
+    exchanged through counters): the field equals the oracle's FP32
+    restatement bit for bit, for odd and even chunks and single iterations,
+    and the residual of the last iteration matches the FP64 norm of the
+    oracle's last step."""
+    import khrr
+    pos, vel, mass, eps2 = galaxy_state(8192, 16384, 19)
+    nx, L = 128, 4.0
+    dx = 2 * L / nx
+    ctx.upload(pos, vel, mass, eps2)
+    b = ctx.bin((-L,) * 3, (dx,) * 3, (nx, nx, nx))
+    W = khrr.WaveParams.make(nx, dx)
+    it, res, phi = ctx.wave_solve(W, tol=0.0, max_iter=max_iter, check_every=check_every, cold=True)
+    assert it == max_iter
+    Wo = oracle.wave_params(nx, dx)
+    m32 = b["cell_mass"].astype(np.float32)
+    prev, cur = np.zeros(nx ** 3, np.float32), np.zeros(nx ** 3, np.float32)
+    for _ in range(max_iter):
+        prev, cur = cur, oracle.wave_iter_f32(Wo, cur, prev, m32)
+    assert np.array_equal(phi, cur)
+    d = cur.astype(np.float64) - prev.astype(np.float64)
+    want = np.sqrt((d * d).sum() / (cur.astype(np.float64) ** 2).sum())
+    assert abs(res - want) <= 1e-12 * want
+
+
+def test_resident_stencil_matches_per_iteration_launches(ctx, monkeypatch):
+    """Long runs at 128^3 (warm continuation over several calls, chunks of 50
+    with residual checks): the resident kernel and one launch per iteration
+    (KHRR_WAVE_RESIDENT=0) give the same field bits and residuals."""
+    import khrr
+    pos, vel, mass, eps2 = galaxy_state(8192, 16384, 20)
+    nx, L = 128, 4.0
+    dx = 2 * L / nx
+    ctx.upload(pos, vel, mass, eps2)
+    ctx.bin((-L,) * 3, (dx,) * 3, (nx, nx, nx))
+    W = khrr.WaveParams.make(nx, dx)
+    runs = {}
+    for mode in ("1", "0"):
+        monkeypatch.setenv("KHRR_WAVE_RESIDENT", mode)
+        out = [ctx.wave_solve(W, tol=0.0, max_iter=101, check_every=50, cold=True)]
+        out.append(ctx.wave_solve(W, tol=0.0, max_iter=203, check_every=50))
+        runs[mode] = out
+    for (i1, r1, p1), (i0, r0, p0) in zip(runs["1"], runs["0"]):
+        assert i1 == i0
+        assert np.array_equal(p1, p0)
+        assert abs(r1 - r0) <= 1e-12 * r0

@@ -157,6 +157,33 @@ def test_mesh_steps_match_oracle(ctx, torch_cuda, oracle, cic, fp64):
     assert np.isfinite(st["acc"]).all()
 
 
+def test_mesh_steps_resident_stencil_128(ctx, torch_cuda, monkeypatch):
+    """Wave-mode steps on the encounter's 128^3 mesh (CIC, FP32 stencil): with
+    the shared-memory-resident stencil (all iterations of a force evaluation
+    in one launch) the trajectory, accelerations and potentials equal those
+    of one launch per iteration (KHRR_WAVE_RESIDENT=0) bit for bit; odd
+    iteration counts per step exercise the ring's single-iteration tail."""
+    import khrr
+    pos, vel, mass, eps2 = galaxy(8192, 16384, 37)
+    nx, dx, dt = 128, 0.0625, 0.002
+    W = khrr.WaveParams.make(nx, dx)
+    out = {}
+    for mode in ("1", "0"):
+        monkeypatch.setenv("KHRR_WAVE_RESIDENT", mode)
+        ctx.upload(pos, vel, mass, eps2)
+        ctx.set_mesh_solver(W, assign=khrr.ASSIGN_CIC, fp64=False, iters_per_step=37, setup_iters=101)
+        try:
+            ctx.forces(khrr.ACC | khrr.PHI | khrr.MESH)
+            ctx.step(dt, 2, khrr.MESH)
+            ctx.step(dt, 1, khrr.MESH | khrr.PHI)
+            out[mode] = ctx.download()
+        finally:
+            ctx.set_mesh_solver(None)
+    for key in ("pos", "vel", "acc", "phi"):
+        assert np.array_equal(out["1"][key], out["0"][key]), key
+    assert np.isfinite(out["1"]["acc"]).all()
+
+
 def test_mesh_solver_rejects_bad_use(ctx, torch_cuda):
     import khrr
     pos, vel, mass, eps2 = galaxy(256, 256, 36)
