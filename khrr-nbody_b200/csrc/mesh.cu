@@ -930,46 +930,61 @@ __global__ void __launch_bounds__((kW1Consumers + 1) * 32) wave1_tma_kernel(floa
 }
 
 // k FP32 iterations in one launch with the field resident in shared memory
-// (nx = 128: the 128^3 mesh of the two-galaxy encounter).  CTA z owns plane z
-// for the whole launch: phi^n of the plane in shared memory (two buffers,
+// (nx = 128: the 128^3 mesh of the two-galaxy encounter).  The mesh is cut
+// into 128 bricks of 128 (x) x 16 (y) x 8 (z) cells, one CTA each, for the
+// whole launch: phi^n of the brick in shared memory (two buffers,
 // alternating by iteration), phi^{n-1} and the mass term in registers, the
-// sponge factor w = 1/(1 + Q) of every cell in shared memory.  A warp covers
-// one 128-cell row, four consecutive x cells per lane (16-byte shared and
-// global accesses; x neighbours from the float4 and by shuffles).  Per
-// iteration a CTA reads only its two neighbours' planes phi^n (z - 1, z + 1)
-// from global memory (L2), and writes its new plane to the ring buffer the
-// one-launch-per-iteration path would write, so the ring ends in the same
-// state.  Planes are exchanged through per-plane counters: after iteration t
-// a CTA sets flag[z] = t + 1 (release); before iteration t (t >= 1) it waits
-// for flag[z - 1] and flag[z + 1] >= t.  That wait also keeps every CTA at
-// most one iteration ahead of its neighbours, so a ring buffer is overwritten
-// only once both neighbours have finished the iteration that read it (it
-// holds phi^{t-2} or older when iteration t writes phi^{t+1}).  Every wait is
-// bounded (2 s of wall time); a CTA that gives up sets err (kErrTimeout) and
-// flag[nx] (abort), and every other wait ends on that flag.  The grid is one
-// CTA per plane, launched cooperatively so all of them are resident.  Per
-// cell the arithmetic is wave_f32_kernel's, in its order, so the bits are
-// the same; the residual of the last iteration is summed per warp and added
-// with one FP64 atomic pair per warp (its last bits depend on the order).
+// sponge factor w = 1/(1 + Q) of every cell in shared memory.  A warp owns 8
+// of the brick's 128 rows of 128 x cells, four consecutive cells per lane
+// (16-byte shared and global accesses; x neighbours from the float4 and by
+// shuffles).  An iteration first updates the brick's 84 interior rows, whose
+// neighbours all lie in the brick, while the neighbour bricks finish the
+// previous iteration; then it waits for them, stages the 48 rows of theirs
+// that touch it (y - 1, y + 1, z - 1, z + 1 faces; 24 KB) from global memory
+// into shared memory, and updates its 44 face rows, which it writes to the
+// ring buffer the one-launch-per-iteration path would write.  The last
+// iteration writes the whole brick, and the interior rows of phi^{k-1}
+// follow it, so the ring ends in the state of the per-iteration path (its
+// two current buffers; the other two are free).  Bricks are exchanged
+// through per-brick counters: after iteration t a CTA sets flag[b] = t + 1
+// (release); before the face rows of iteration t (t >= 1) it waits for its
+// (up to four) neighbours' flags >= t.  That wait also keeps every CTA at
+// most one iteration ahead of its neighbours, so a ring buffer's face rows
+// are overwritten only once the neighbours have finished the iteration that
+// read them (the buffer holds phi^{t-2} or older when iteration t writes
+// phi^{t+1}); interior rows are read by no other CTA.  Every wait is bounded
+// (2 s of wall time); a CTA that gives up sets err (kErrTimeout) and
+// flag[kRzBricks] (abort), and every other wait ends on that flag.  The grid
+// is one CTA per brick, launched cooperatively so all of them are resident.
+// Per cell the arithmetic is wave_f32_kernel's, in its order, so the bits
+// are the same; the residual of the last iteration is formed after the loop
+// from the two shared buffers it leaves, summed per warp and added with one
+// FP64 atomic pair per warp (its last bits depend on the order).
 //
-// Measured on the encounter's mesh (CUDA events): 7.1 us per iteration in a
-// 1000-iteration solve against 10.4 us with one launch per iteration, the
-// Wave-mode step (507 iterations) 3.64 against 4.17 ms.  1024 threads (16
-// cells each, 64 registers): 7.3 us; one cell per thread instead of four
-// (16 cells each): 7.6 us.  Timing-only copies of the one-cell form put the
-// cost in the exchange through L2: 6.6 us without the neighbour waits, 3.7
-// us without the neighbour-plane loads as well.
-constexpr int kRzNX = 128;                                // mesh edge
-#ifndef KHRR_WAVE_RZ_THREADS
-#define KHRR_WAVE_RZ_THREADS 512
-#endif
-constexpr int kRzThreads = KHRR_WAVE_RZ_THREADS;
-constexpr int kRzRows = kRzThreads / 32;                  // rows per pass (a warp = one 128-cell row)
-constexpr int kRzPasses = kRzNX / kRzRows;                // passes per plane
-constexpr int kRzCells = 4 * kRzPasses;                   // cells per thread
+// Measured on the encounter's mesh (CUDA events, same GPU, 1000-iteration
+// solve / Wave-mode step of 507 iterations): 5.6 us per iteration, 2.91 ms
+// per step, against 7.07 us / 3.39 ms for one plane per CTA (two 64 KB
+// neighbour planes read and the whole plane written per CTA and iteration)
+// and 10.4 us with one launch per iteration.  Steps on the way: bricks with
+// the face rows read straight from global memory 8.5 us (each warp's loads
+// serialised behind its z carry); halos staged in shared memory 7.2 us;
+// interior rows before the wait 6.7 us; the residual moved out of the loop
+// (no FP64 branch in it) 5.6 us.
+constexpr int kRzNX = 128;                                 // mesh edge
+constexpr int kRzBY = 16, kRzBZ = 8;                       // brick rows in y and z
+constexpr int kRzBricksY = kRzNX / kRzBY;                  // 8
+constexpr int kRzBricks = kRzBricksY * (kRzNX / kRzBZ);    // 128
+constexpr int kRzThreads = 32 * kRzBY;                     // a warp per brick row yl
+constexpr int kRzSlots = kRzBY * kRzBZ / (kRzThreads / 32);  // rows per warp (8)
+constexpr int kRzCells = 4 * kRzSlots;                     // cells per thread
 constexpr int kRzPlane = kRzNX * kRzNX;
-constexpr size_t kRzSmem = (3 * static_cast<size_t>(kRzPlane) + kRzNX) * sizeof(float);  // 197,120 B
-static_assert(kRzNX == 4 * 32 && kRzNX % kRzRows == 0, "a warp covers a row, four cells per lane");
+constexpr int kRzBrick = kRzNX * kRzBY * kRzBZ;            // 16,384 cells
+constexpr int kRzHalo = (2 * kRzBZ + 2 * kRzBY) * kRzNX;  // the neighbour rows read, 6,144 cells
+constexpr int kRzHaloVec = kRzHalo / 4;
+constexpr size_t kRzSmem = (3 * static_cast<size_t>(kRzBrick) + kRzHalo) * sizeof(float);  // 221,184 B
+static_assert(kRzHaloVec % kRzThreads == 0, "whole halo loads per thread");
+static_assert(kRzNX == 4 * 32 && kRzNX % kRzBY == 0 && kRzNX % kRzBZ == 0, "a warp covers a row, four cells per lane");
+static_assert(kRzBricks <= kRzNX, "the counters (nx + 1 words, allocated by the mesh set-up) cover the bricks and the abort flag");
 
 __device__ __forceinline__ unsigned ld_acquire_gpu(const unsigned* p) {
     unsigned v;
@@ -991,6 +1006,36 @@ __device__ __forceinline__ void ring_free_dev(int o, int c, int& f0, int& f1) {
     f1 = f[1];
 }
 
+// The brick's rows: 84 interior rows (1 <= yl <= 14, 1 <= zl <= 6), which no
+// neighbour reads and whose neighbours all lie in the brick, and 44 face rows
+// (yl in {0, 15} or zl in {0, 7}).  Warp w owns 8 rows for the whole launch:
+// slots 0-4 are interior rows w + 16 m; slot 5 is interior row 80 + (w - 12)
+// for w >= 12 and face row w for w < 12; slots 6, 7 are face rows
+// w + 16 (m + [w < 12]).  Face row f: zl = 0 for f < 16, zl = 7 for f >= 28,
+// otherwise zl = 1 + (f - 16) / 2 at yl = 0 or 15.
+static_assert(kRzBY == 16 && kRzBZ == 8 && kRzSlots == 8, "the row map below is written for 16 x 8 rows, 16 warps");
+__device__ __forceinline__ bool rz_interior_slot(int w, int i) { return i < 5 || (i == 5 && w >= 12); }
+
+__device__ __forceinline__ void rz_row(int w, int i, int& yl, int& zl) {
+    if (rz_interior_slot(w, i)) {
+        const int ii = i < 5 ? w + 16 * i : 80 + (w - 12);
+        zl = 1 + ii / 14;
+        yl = 1 + ii % 14;
+    } else {
+        const int f = w + 16 * (i - (w < 12 ? 5 : 6));
+        if (f < 16) {
+            zl = 0;
+            yl = f;
+        } else if (f >= 28) {
+            zl = kRzBZ - 1;
+            yl = f - 28;
+        } else {
+            zl = 1 + (f - 16) / 2;
+            yl = (f - 16) & 1 ? kRzBY - 1 : 0;
+        }
+    }
+}
+
 __global__ void __launch_bounds__(kRzThreads, 1) wave_resident_kernel(float* __restrict__ ring, int64_t cz,
                                                                       const float* __restrict__ mass,
                                                                       const WaveF32 W, int k, int st,
@@ -998,43 +1043,51 @@ __global__ void __launch_bounds__(kRzThreads, 1) wave_resident_kernel(float* __r
                                                                       unsigned* __restrict__ flag,
                                                                       unsigned* __restrict__ err) {
     extern __shared__ __align__(16) float rz_smem[];
-    float* sphi = rz_smem;                  // [2][plane]: phi^n by iteration parity
-    float* sw = rz_smem + 2 * kRzPlane;     // [plane]: w = 1 / (1 + Q)
-    float* ssy = sw + kRzPlane;             // [nx]: the y sponge table
-    const int z = blockIdx.x, tid = threadIdx.x;
-    const int lane = tid & 31, iy0 = tid >> 5;
+    float* sphi = rz_smem;                  // [2][brick]: phi^n by iteration parity
+    float* sw = rz_smem + 2 * kRzBrick;     // [brick]: w = 1 / (1 + Q)
+    float* shalo = sw + kRzBrick;           // [48 rows]: y halos by zl, then z halos by yl
+    const int b = blockIdx.x, by = b % kRzBricksY, bz = b / kRzBricksY;
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    const int y0 = by * kRzBY, z0 = bz * kRzBZ;
     const int x0 = 4 * lane;  // the lane's cells x0 .. x0 + 3 of each of its rows
-    const bool zface = z == 0 || z == kRzNX - 1;
-    const int64_t zoff = static_cast<int64_t>(z) * kRzPlane;
+    constexpr int kSRow = kRzBY * kRzNX;  // shared stride of zl
+    // Row (yl, zl): shared index (zl * BY + yl) * nx + x0, global index
+    // (z0 + zl) * nx^2 + (y0 + yl) * nx + x0.
+    auto sidx = [&](int yl, int zl) { return (zl * kRzBY + yl) * kRzNX + x0; };
+    auto gidx = [&](int yl, int zl) {
+        return static_cast<int64_t>(z0 + zl) * kRzPlane + static_cast<int64_t>(y0 + yl) * kRzNX + x0;
+    };
     float sxb[4];
 #pragma unroll
     for (int j = 0; j < 4; ++j) sxb[j] = W.diss_base + W.sx[x0 + j];
-    const float szz = W.sz[z];
     int old = st / 4, cur = st % 4;
-    if (tid < kRzNX) ssy[tid] = W.sy[tid];
 
-    float po[kRzCells], msw[kRzCells];  // phi^{n-1}; mass times S w
+    float po[kRzCells], msw[kRzCells];  // per slot: phi^{n-1}; mass times S w
 #pragma unroll
-    for (int p = 0; p < kRzPasses; ++p) {
-        const int iy = iy0 + kRzRows * p, q = iy * kRzNX + x0;
-        const float4 m4 = *reinterpret_cast<const float4*>(mass + zoff + q);
-        const float4 o4 = *reinterpret_cast<const float4*>(ring + old * cz + zoff + q);
-        const float4 c4 = *reinterpret_cast<const float4*>(ring + cur * cz + zoff + q);
+    for (int i = 0; i < kRzSlots; ++i) {
+        int yl, zl;
+        rz_row(wid, i, yl, zl);
+        const int s = sidx(yl, zl);
+        const int64_t g = gidx(yl, zl);
+        const float4 m4 = *reinterpret_cast<const float4*>(mass + g);
+        const float4 o4 = *reinterpret_cast<const float4*>(ring + old * cz + g);
+        const float4 c4 = *reinterpret_cast<const float4*>(ring + cur * cz + g);
         const float mj[4] = {m4.x, m4.y, m4.z, m4.w}, oj[4] = {o4.x, o4.y, o4.z, o4.w};
+        const float sy = W.sy[y0 + yl], sz = W.sz[z0 + zl];
         float wj[4];
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
-            const float sxy = sxb[j] + W.sy[iy];
-            const float diss = sxy + szz;
+            const float sxy = sxb[j] + sy;
+            const float diss = sxy + sz;
             const float Q = diss * W.cdt_half;
             wj[j] = __frcp_rn(1.0f + Q);
-            msw[4 * p + j] = mj[j] * (W.S * wj[j]);
-            po[4 * p + j] = oj[j];
+            msw[4 * i + j] = mj[j] * (W.S * wj[j]);
+            po[4 * i + j] = oj[j];
         }
-        *reinterpret_cast<float4*>(sw + q) = make_float4(wj[0], wj[1], wj[2], wj[3]);
-        *reinterpret_cast<float4*>(sphi + q) = c4;
+        *reinterpret_cast<float4*>(sw + s) = make_float4(wj[0], wj[1], wj[2], wj[3]);
+        *reinterpret_cast<float4*>(sphi + s) = c4;
     }
-    double d2 = 0.0, n2 = 0.0;
+    __syncthreads();  // the brick's phi^n and w are in shared memory
     const int pairs = k / 2;
     int pending = 0;
     __shared__ int s_abort;
@@ -1050,30 +1103,91 @@ __global__ void __launch_bounds__(kRzThreads, 1) wave_resident_kernel(float* __r
             ob = f0;
             pending = f1;
         }
+        const float* rd = sphi + (t & 1) * kRzBrick;
+        float* wr = sphi + ((t + 1) & 1) * kRzBrick;
+        float* out_g = ring + ob * cz;
+        const bool last = t == k - 1;
+        // One row: every load from shared memory and unconditional (the
+        // neighbour row is in the brick or in the staged halo: a warp-uniform
+        // address choice; face cells discard the value).
+        auto row = [&](int i) {
+            int yl, zl;
+            rz_row(wid, i, yl, zl);
+            const int y = y0 + yl, z = z0 + zl;
+            const int s = sidx(yl, zl);
+            const float* pzm = zl > 0 ? rd + s - kSRow : shalo + (2 * kRzBZ + yl) * kRzNX + x0;
+            const float* pzp = zl < kRzBZ - 1 ? rd + s + kSRow : shalo + (2 * kRzBZ + kRzBY + yl) * kRzNX + x0;
+            const float* pym = yl > 0 ? rd + s - kRzNX : shalo + zl * kRzNX + x0;
+            const float* pyp = yl < kRzBY - 1 ? rd + s + kRzNX : shalo + (kRzBZ + zl) * kRzNX + x0;
+            const float4 c4 = *reinterpret_cast<const float4*>(rd + s);
+            const float4 zm4 = *reinterpret_cast<const float4*>(pzm);
+            const float4 zp4 = *reinterpret_cast<const float4*>(pzp);
+            const float4 ym4 = *reinterpret_cast<const float4*>(pym);
+            const float4 yp4 = *reinterpret_cast<const float4*>(pyp);
+            const float4 w4 = *reinterpret_cast<const float4*>(sw + s);
+            float left = __shfl_up_sync(0xffffffffu, c4.w, 1);
+            float right = __shfl_down_sync(0xffffffffu, c4.x, 1);
+            if (lane == 0) left = c4.x;    // x = 0 is a face
+            if (lane == 31) right = c4.w;  // x = nx - 1 is a face
+            const float cj[4] = {c4.x, c4.y, c4.z, c4.w};
+            const float xm[4] = {left, c4.x, c4.y, c4.z}, xp[4] = {c4.y, c4.z, c4.w, right};
+            const float ym[4] = {ym4.x, ym4.y, ym4.z, ym4.w}, yp[4] = {yp4.x, yp4.y, yp4.z, yp4.w};
+            const float zmj[4] = {zm4.x, zm4.y, zm4.z, zm4.w}, zpj[4] = {zp4.x, zp4.y, zp4.z, zp4.w};
+            const float wj[4] = {w4.x, w4.y, w4.z, w4.w};
+            const bool rface = y == 0 || y == kRzNX - 1 || z == 0 || z == kRzNX - 1;
+            const float sy = __ldg(W.sy + y), sz = __ldg(W.sz + z);
+            float oj[4];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const int u = 4 * i + j;
+                const float nb = ((xm[j] + xp[j]) + (ym[j] + yp[j])) + (zmj[j] + zpj[j]);
+                const float sxy = sxb[j] + sy;
+                const float diss = sxy + sz;
+                const float Q = diss * W.cdt_half;
+                const float w = wj[j];
+                const float val = fmaf(nb, W.K * w, fmaf(cj[j], W.A * w, fmaf(po[u], (Q - 1.0f) * w, msw[u])));
+                const bool face = rface || (lane == 0 && j == 0) || (lane == 31 && j == 3);
+                oj[j] = face ? 0.0f : val;
+                po[u] = cj[j];
+            }
+            const float4 o4 = make_float4(oj[0], oj[1], oj[2], oj[3]);
+            *reinterpret_cast<float4*>(wr + s) = o4;
+            // Face rows every iteration (the neighbours read them), interior
+            // rows on the last one.
+            if (last || !rz_interior_slot(wid, i)) *reinterpret_cast<float4*>(out_g + gidx(yl, zl)) = o4;
+        };
+        // Interior rows first: they need nothing from the neighbours, so they
+        // run while the neighbours finish the previous iteration.
+#pragma unroll
+        for (int i = 0; i < kRzSlots; ++i)
+            if (rz_interior_slot(wid, i)) row(i);
         if (tid == 0) {
             int abort = 0;
             if (t > 0) {
-                // Both counters in flight together; the abort flag and the
-                // clock only every 64th poll.  A face plane has one
-                // neighbour: its own counter (already >= t) stands in.
-                const unsigned* fa = flag + (z > 0 ? z - 1 : z);
-                const unsigned* fb = flag + (z < kRzNX - 1 ? z + 1 : z);
+                // All counters in flight together; the abort flag and the
+                // clock only every 64th poll.  A missing neighbour (a mesh
+                // face) is stood in for by the brick's own counter (>= t).
+                const unsigned* fn[4] = {flag + (by > 0 ? b - 1 : b), flag + (by < kRzBricksY - 1 ? b + 1 : b),
+                                         flag + (bz > 0 ? b - kRzBricksY : b),
+                                         flag + (z0 + kRzBZ < kRzNX ? b + kRzBricksY : b)};
                 const unsigned need = static_cast<unsigned>(t);
-                unsigned a = ld_acquire_gpu(fa), b = ld_acquire_gpu(fb);
-                if (a < need || b < need) {
+                auto ready = [&]() {
+                    const unsigned a0 = ld_acquire_gpu(fn[0]), a1 = ld_acquire_gpu(fn[1]);
+                    const unsigned a2 = ld_acquire_gpu(fn[2]), a3 = ld_acquire_gpu(fn[3]);
+                    return a0 >= need && a1 >= need && a2 >= need && a3 >= need;
+                };
+                if (!ready()) {
                     const uint64_t t0 = global_ns();
                     for (unsigned spin = 1;; ++spin) {
-                        a = ld_acquire_gpu(fa);
-                        b = ld_acquire_gpu(fb);
-                        if (a >= need && b >= need) break;
+                        if (ready()) break;
                         if ((spin & 63u) == 0u) {
-                            if (ld_acquire_gpu(flag + kRzNX) != 0u) {
+                            if (ld_acquire_gpu(flag + kRzBricks) != 0u) {
                                 abort = 1;
                                 break;
                             }
                             if (global_ns() - t0 > 2000000000ull) {
                                 atomicOr(err, kErrTimeout);
-                                st_release_gpu(flag + kRzNX, 1u);
+                                st_release_gpu(flag + kRzBricks, 1u);
                                 abort = 1;
                                 break;
                             }
@@ -1085,74 +1199,81 @@ __global__ void __launch_bounds__(kRzThreads, 1) wave_resident_kernel(float* __r
         }
         __syncthreads();
         if (s_abort) return;  // uniform across the CTA; no barrier follows
-        const float* rd = sphi + (t & 1) * kRzPlane;
-        float* wr = sphi + ((t + 1) & 1) * kRzPlane;
-        // z neighbours (face planes read none)
-        const float* zm = ring + cur * cz + (zface ? zoff : zoff - kRzPlane);
-        const float* zp = ring + cur * cz + (zface ? zoff : zoff + kRzPlane);
-        float* out_g = ring + ob * cz + zoff;
-        const bool last = t == k - 1 && resid != nullptr;
-        // Every load is unconditional (neighbour rows clamped into the plane,
-        // face cells discard the value), so the loads of all the thread's
-        // rows can be in flight together.  x neighbours come from the row's
-        // float4 and, across lanes, by shuffles.
+        // The 48 rows of the neighbour bricks this brick reads, staged in
+        // shared memory: three independent 16-byte loads per thread through
+        // L2 (ld.cg: the neighbours rewrote them since this CTA last read the
+        // buffer); rows outside the mesh are zeros (only face cells, whose
+        // value is discarded, would read them).
+        const float* gcur = ring + cur * cz;
 #pragma unroll
-        for (int p = 0; p < kRzPasses; ++p) {
-            const int iy = iy0 + kRzRows * p, q = iy * kRzNX + x0;
-            const int qym = iy > 0 ? q - kRzNX : q, qyp = iy < kRzNX - 1 ? q + kRzNX : q;
-            const float4 c4 = *reinterpret_cast<const float4*>(rd + q);
-            const float4 ym4 = *reinterpret_cast<const float4*>(rd + qym);
-            const float4 yp4 = *reinterpret_cast<const float4*>(rd + qyp);
-            const float4 w4 = *reinterpret_cast<const float4*>(sw + q);
-            const float4 zm4 = __ldcg(reinterpret_cast<const float4*>(zm + q));
-            const float4 zp4 = __ldcg(reinterpret_cast<const float4*>(zp + q));
-            float left = __shfl_up_sync(0xffffffffu, c4.w, 1);
-            float right = __shfl_down_sync(0xffffffffu, c4.x, 1);
-            if (lane == 0) left = c4.x;    // x = 0 is a face
-            if (lane == 31) right = c4.w;  // x = nx - 1 is a face
-            const float cj[4] = {c4.x, c4.y, c4.z, c4.w};
-            const float xm[4] = {left, c4.x, c4.y, c4.z}, xp[4] = {c4.y, c4.z, c4.w, right};
-            const float ym[4] = {ym4.x, ym4.y, ym4.z, ym4.w}, yp[4] = {yp4.x, yp4.y, yp4.z, yp4.w};
-            const float zmj[4] = {zm4.x, zm4.y, zm4.z, zm4.w}, zpj[4] = {zp4.x, zp4.y, zp4.z, zp4.w};
-            const float wj[4] = {w4.x, w4.y, w4.z, w4.w};
-            const bool yface = zface || iy == 0 || iy == kRzNX - 1;
-            const float sy = ssy[iy];
-            float oj[4];
-#pragma unroll
-            for (int j = 0; j < 4; ++j) {
-                const int u = 4 * p + j;
-                const float nb = ((xm[j] + xp[j]) + (ym[j] + yp[j])) + (zmj[j] + zpj[j]);
-                const float sxy = sxb[j] + sy;
-                const float diss = sxy + szz;
-                const float Q = diss * W.cdt_half;
-                const float w = wj[j];
-                const float val = fmaf(nb, W.K * w, fmaf(cj[j], W.A * w, fmaf(po[u], (Q - 1.0f) * w, msw[u])));
-                const bool face = yface || (lane == 0 && j == 0) || (lane == 31 && j == 3);
-                oj[j] = face ? 0.0f : val;
-                if (last) {
-                    const double dd = static_cast<double>(oj[j]) - static_cast<double>(cj[j]);
-                    d2 += dd * dd;
-                    n2 += static_cast<double>(oj[j]) * static_cast<double>(oj[j]);
-                }
-                po[u] = cj[j];
+        for (int r = 0; r < kRzHaloVec / kRzThreads; ++r) {
+            const int q = tid + r * kRzThreads, hr = q >> 5, hx = 4 * (q & 31);
+            int gy, gz;
+            if (hr < 2 * kRzBZ) {  // y halos: rows (y0 - 1 | y0 + BY, z0 + zl)
+                gy = hr < kRzBZ ? y0 - 1 : y0 + kRzBY;
+                gz = z0 + (hr % kRzBZ);
+            } else {  // z halos: rows (y0 + yl, z0 - 1 | z0 + BZ)
+                const int h = hr - 2 * kRzBZ;
+                gy = y0 + (h % kRzBY);
+                gz = h < kRzBY ? z0 - 1 : z0 + kRzBZ;
             }
-            const float4 o4 = make_float4(oj[0], oj[1], oj[2], oj[3]);
-            *reinterpret_cast<float4*>(wr + q) = o4;
-            *reinterpret_cast<float4*>(out_g + q) = o4;
+            float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (gy >= 0 && gy < kRzNX && gz >= 0 && gz < kRzNX)
+                v = __ldcg(reinterpret_cast<const float4*>(gcur + static_cast<int64_t>(gz) * kRzPlane +
+                                                           static_cast<int64_t>(gy) * kRzNX + hx));
+            *reinterpret_cast<float4*>(shalo + hr * kRzNX + hx) = v;
         }
-        __syncthreads();  // the plane is written (shared and global); rd is free
+        __syncthreads();
+#pragma unroll
+        for (int i = 0; i < kRzSlots; ++i)
+            if (!rz_interior_slot(wid, i)) row(i);
+        __syncthreads();  // the brick is written (shared and global); rd and the halo are free
         // The barrier orders the CTA's stores before thread 0's release.
-        if (tid == 0) st_release_gpu(flag + z, static_cast<unsigned>(t + 1));
+        if (tid == 0) st_release_gpu(flag + b, static_cast<unsigned>(t + 1));
         old = cur;
         cur = ob;
     }
+    // phi^{k-1} (now in po) of the interior rows, which no neighbour reads:
+    // its face rows were written by iteration k - 2 (for k = 1 the buffer is
+    // the input, whole).
+    if (k >= 2) {
+        float* og = ring + old * cz;
+#pragma unroll
+        for (int i = 0; i < kRzSlots; ++i) {
+            if (!rz_interior_slot(wid, i)) continue;
+            int yl, zl;
+            rz_row(wid, i, yl, zl);
+            *reinterpret_cast<float4*>(og + gidx(yl, zl)) =
+                make_float4(po[4 * i], po[4 * i + 1], po[4 * i + 2], po[4 * i + 3]);
+        }
+    }
     if (resid) {
+        // The residual of the last iteration from the two shared buffers it
+        // leaves: phi^k (written) and phi^{k-1} (read).
+        const float* pk = sphi + (k & 1) * kRzBrick;
+        const float* pk1 = sphi + ((k - 1) & 1) * kRzBrick;
+        double d2 = 0.0, n2 = 0.0;
+#pragma unroll
+        for (int i = 0; i < kRzSlots; ++i) {
+            int yl, zl;
+            rz_row(wid, i, yl, zl);
+            const int s = sidx(yl, zl);
+            const float4 a4 = *reinterpret_cast<const float4*>(pk + s);
+            const float4 c4 = *reinterpret_cast<const float4*>(pk1 + s);
+            const float aj[4] = {a4.x, a4.y, a4.z, a4.w}, cj[4] = {c4.x, c4.y, c4.z, c4.w};
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const double dd = static_cast<double>(aj[j]) - static_cast<double>(cj[j]);
+                d2 += dd * dd;
+                n2 += static_cast<double>(aj[j]) * static_cast<double>(aj[j]);
+            }
+        }
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) {
             d2 += __shfl_xor_sync(0xffffffffu, d2, o);
             n2 += __shfl_xor_sync(0xffffffffu, n2, o);
         }
-        if ((tid & 31) == 0) {
+        if (lane == 0) {
             atomicAdd(&resid[0], d2);
             atomicAdd(&resid[1], n2);
         }
@@ -1447,7 +1568,7 @@ bool wave_resident_available(int nx) {
             cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, wave_resident_kernel, kRzThreads, kRzSmem) !=
                 cudaSuccess)
             return false;
-        return occ >= 1 && static_cast<int64_t>(occ) * sms >= kRzNX;
+        return occ >= 1 && static_cast<int64_t>(occ) * sms >= kRzBricks;
     }();
     return ok;
 }
@@ -1455,10 +1576,10 @@ bool wave_resident_available(int nx) {
 cudaError_t launch_wave_resident(float* ring, int64_t cells, const float* mass, const WaveF32& w, int k, int st,
                                  double* resid, unsigned* sync, unsigned* err, cudaStream_t s) {
     if (k < 1) return cudaSuccess;
-    cudaError_t e = cudaMemsetAsync(sync, 0, (kRzNX + 1) * sizeof(unsigned), s);
+    cudaError_t e = cudaMemsetAsync(sync, 0, (kRzBricks + 1) * sizeof(unsigned), s);
     if (e != cudaSuccess) return e;
     cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(kRzNX);
+    cfg.gridDim = dim3(kRzBricks);
     cfg.blockDim = dim3(kRzThreads);
     cfg.dynamicSmemBytes = kRzSmem;
     cfg.stream = s;
