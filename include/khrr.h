@@ -406,6 +406,14 @@ khrr_status khrr_autotune(khrr_ctx* ctx, const char* cache_path);
 khrr_status khrr_enable_timing(khrr_ctx* ctx, int enable);
 khrr_status khrr_force_timing(khrr_ctx* ctx, double* ms, int64_t* launches,
                               double* interactions);
+/* Device time of the last khrr_bin, khrr_bin_cell_phi or khrr_sort_by_cell
+ * made with timing enabled: the milliseconds between CUDA events recorded on
+ * the context's stream before the call's first kernel and after its last one,
+ * so neither the downloads to the caller's buffers nor the host-side
+ * synchronisation that ends the call are included.  (No reference
+ * counterpart: the reference times nothing on the mesh path.)  Returns
+ * KHRR_ERR_STATE when no such call was timed. */
+khrr_status khrr_call_timing(khrr_ctx* ctx, double* ms);
 /* Pair interactions one force pass computes on the uploaded state
  * (sum over systems of n_k^2, j = i counted as the reference does). */
 khrr_status khrr_pair_count(khrr_ctx* ctx, double* pairs);

@@ -627,6 +627,22 @@ khrr_status khrr_ctx::timing_pair(cudaEvent_t* e0, cudaEvent_t* e1) {
     return KHRR_OK;
 }
 
+khrr_status khrr_ctx::call_start() {
+    call_timed = false;
+    if (!timing) return KHRR_OK;
+    khrr_status st;
+    if (!call0 && (st = cuda(cudaEventCreate(&call0), "event create")) != KHRR_OK) return st;
+    if (!call1 && (st = cuda(cudaEventCreate(&call1), "event create")) != KHRR_OK) return st;
+    return cuda(cudaEventRecord(call0, stream), "event");
+}
+
+khrr_status khrr_ctx::call_stop() {
+    if (!timing || !call0 || !call1) return KHRR_OK;
+    khrr_status st = cuda(cudaEventRecord(call1, stream), "event");
+    if (st == KHRR_OK) call_timed = true;
+    return st;
+}
+
 khrr_status khrr_ctx::force_mode(int flags, int* mode) {
     const bool plain = (flags & KHRR_PLAIN) != 0, f64 = (flags & KHRR_FP64) != 0;
     if (plain && f64) return fail(KHRR_ERR_INVALID_ARG, "KHRR_PLAIN and KHRR_FP64 exclude each other");
@@ -712,6 +728,8 @@ void khrr_destroy(khrr_ctx* c) {
         cudaEventDestroy(e.first);
         cudaEventDestroy(e.second);
     }
+    if (c->call0) cudaEventDestroy(c->call0);
+    if (c->call1) cudaEventDestroy(c->call1);
     if (c->ph0) cudaEventDestroy(c->ph0);
     if (c->ph1) cudaEventDestroy(c->ph1);
     if (c->own) cudaStreamDestroy(c->own);
@@ -1115,6 +1133,18 @@ khrr_status khrr_enable_timing(khrr_ctx* c, int enable) {
     c->ev_used = 0;
     c->timed_launches = 0;
     c->timed_pairs = 0.0;
+    return KHRR_OK;
+}
+
+khrr_status khrr_call_timing(khrr_ctx* c, double* ms) {
+    if (!c || !ms) return KHRR_ERR_INVALID_ARG;
+    if (!c->call_timed)
+        return c->fail(KHRR_ERR_STATE, "no timed call (enable timing, then khrr_bin, khrr_bin_cell_phi or khrr_sort_by_cell)");
+    khrr_status st = c->cuda(cudaEventSynchronize(c->call1), "synchronize");
+    if (st != KHRR_OK) return st;
+    float t = 0.0f;
+    if ((st = c->cuda(cudaEventElapsedTime(&t, c->call0, c->call1), "elapsed")) != KHRR_OK) return st;
+    *ms = t;
     return KHRR_OK;
 }
 

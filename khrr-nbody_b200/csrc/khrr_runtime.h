@@ -196,6 +196,10 @@ struct khrr_ctx {
     size_t ev_used = 0;
     int64_t timed_launches = 0;
     double timed_pairs = 0.0;
+    // Device time of the last synchronising mesh call (khrr_call_timing):
+    // events before its first and after its last kernel.
+    cudaEvent_t call0 = nullptr, call1 = nullptr;
+    bool call_timed = false;
     std::map<const void*, int> occupancy;
 
     khrr_status fail(khrr_status s, const char* fmt, ...);
@@ -218,6 +222,8 @@ struct khrr_ctx {
     khrr_status enqueue_step(double dt, int mode, bool phi_now, bool compat);
     khrr_status get_step_graph(double dt, int mode, bool phi_now, bool compat, khrr::StepGraph** out);
     khrr_status timing_pair(cudaEvent_t* e0, cudaEvent_t* e1);
+    khrr_status call_start();  // with timing on: event before the call's first kernel
+    khrr_status call_stop();   // with timing on: event after its last kernel
     double pairs_per_pass() const;
     khrr_status force_mode(int flags, int* mode);  // KHRR_PLAIN / KHRR_FP64 -> ForceMode
     // Mesh-force solver (mesh_api.cpp).

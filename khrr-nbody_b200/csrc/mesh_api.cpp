@@ -245,6 +245,7 @@ khrr_status khrr_bin(khrr_ctx* c, const khrr_mesh* mesh, int* cell_id, int* id_i
         if ((st = c->cuda(b->ensure(static_cast<size_t>(C)), "alloc")) != KHRR_OK) return st;
     if ((st = c->cuda(c->maxpbc.ensure(static_cast<size_t>(scan_block_count(C))), "alloc")) != KHRR_OK) return st;
     if ((st = c->cuda(c->cell_mass.ensure(static_cast<size_t>(C)), "alloc")) != KHRR_OK) return st;
+    if ((st = c->call_start()) != KHRR_OK) return st;
     cudaMemsetAsync(c->mcount.p, 0, static_cast<size_t>(C) * sizeof(int), s);
     cudaMemsetAsync(c->cell_mass.p, 0, static_cast<size_t>(C) * sizeof(double), s);
     // Every system's real bodies go to the one mesh (ghosts stay out).
@@ -259,6 +260,7 @@ khrr_status khrr_bin(khrr_ctx* c, const khrr_mesh* mesh, int* cell_id, int* id_i
     if ((st = c->cuda(launch_scan(c->mcount.p, false, C, c->maxpbc.p, c->mstart.p, false, c->mscan.p, s), "scan")) !=
         KHRR_OK)
         return st;
+    if ((st = c->call_stop()) != KHRR_OK) return st;
     c->mesh = g;
     c->ncells = C;
     c->has_bin = true;
@@ -306,6 +308,7 @@ khrr_status khrr_bin_cell_phi(khrr_ctx* c, int reset, double* cell_phi) {
     const size_t C = static_cast<size_t>(c->ncells);
     khrr_status st;
     cudaStream_t s = c->stream;
+    if ((st = c->call_start()) != KHRR_OK) return st;
     if (reset || c->cell_phi_cells != c->ncells) {  // a new mesh starts from zero
         if ((st = c->cuda(c->cell_phi.ensure(C), "alloc")) != KHRR_OK) return st;
         cudaMemsetAsync(c->cell_phi.p, 0, C * sizeof(double), s);
@@ -317,6 +320,7 @@ khrr_status khrr_bin_cell_phi(khrr_ctx* c, int reset, double* cell_phi) {
                           "cell phi")) != KHRR_OK)
             return st;
     }
+    if ((st = c->call_stop()) != KHRR_OK) return st;
     if (cell_phi &&
         (st = c->cuda(cudaMemcpyAsync(cell_phi, c->cell_phi.p, C * sizeof(double), cudaMemcpyDeviceToHost, s),
                       "download")) != KHRR_OK)
@@ -475,11 +479,13 @@ khrr_status khrr_sort_by_cell(khrr_ctx* c, int* order) {
     if (c->n > 0x7fffffffLL) return c->fail(KHRR_ERR_INVALID_ARG, "more bodies than int32 indices");
     khrr_status st;
     if ((st = c->cuda(c->morder.ensure(static_cast<size_t>(c->n)), "alloc")) != KHRR_OK) return st;
+    if ((st = c->call_start()) != KHRR_OK) return st;
     for (size_t k = 0; k < c->cnt.size(); ++k)
         if ((st = c->cuda(launch_scatter_order(c->pci.p + c->poff[k], c->mstart.p, c->cnt[k],
                                                static_cast<int>(c->off[k]), c->morder.p, c->stream),
                           "scatter")) != KHRR_OK)
             return st;
+    if ((st = c->call_stop()) != KHRR_OK) return st;
     if (order && (st = c->cuda(cudaMemcpyAsync(order, c->morder.p, static_cast<size_t>(c->n) * sizeof(int),
                                                cudaMemcpyDeviceToHost, c->stream),
                                "download")) != KHRR_OK)

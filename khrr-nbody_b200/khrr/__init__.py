@@ -128,6 +128,7 @@ def lib(path: pathlib.Path | str | None = None) -> C.CDLL:
         "khrr_set_tuning": ([vp, C.POINTER(Tuning)], i),
         "khrr_get_tuning": ([vp, C.POINTER(Tuning)], i),
         "khrr_autotune": ([vp, C.c_char_p], i),
+        "khrr_call_timing": ([vp, C.POINTER(C.c_double)], i),
         "khrr_enable_timing": ([vp, i], i),
         "khrr_force_timing": ([vp, C.POINTER(d), C.POINTER(i64), C.POINTER(d)], i),
         "khrr_pair_count": ([vp, C.POINTER(d)], i),
@@ -336,6 +337,13 @@ class Context:
         pairs = C.c_double()
         self._check(self.L.khrr_force_timing(self.h, C.byref(ms), C.byref(launches), C.byref(pairs)))
         return ms.value, launches.value, pairs.value
+
+    def call_timing(self) -> float:
+        """Device milliseconds of the last timed khrr_bin / khrr_bin_cell_phi /
+        khrr_sort_by_cell (timing enabled), without its downloads and host sync."""
+        ms = C.c_double()
+        self._check(self.L.khrr_call_timing(self.h, C.byref(ms)))
+        return ms.value
 
     def pair_count(self) -> float:
         p = C.c_double()

@@ -336,3 +336,36 @@ def test_resident_stencil_matches_per_iteration_launches(ctx, monkeypatch):
         assert i1 == i0
         assert np.array_equal(p1, p0)
         assert abs(r1 - r0) <= 1e-12 * r0
+
+
+def test_call_timing_of_mesh_calls(ctx):
+    """khrr_call_timing: the device time of the last timed khrr_bin /
+    khrr_sort_by_cell is positive and no longer than the call measured from
+    outside (which adds the downloads and the closing host synchronisation);
+    without a timed call it reports KHRR_ERR_STATE."""
+    import time
+    import khrr
+    pos, vel, mass, eps2 = galaxy_state(8192, 16384, 41)
+    ctx.upload(pos, vel, mass, eps2)
+    nx, L = 64, 4.0
+    ctx.enable_timing(False)
+    ctx.bin((-L,) * 3, (2 * L / nx,) * 3, (nx, nx, nx))
+    with pytest.raises(khrr.KhrrError) as e:
+        ctx.call_timing()
+    assert e.value.status == 6  # KHRR_ERR_STATE
+    ctx.enable_timing(True)
+    try:
+        t0 = time.perf_counter()
+        b = ctx.bin((-L,) * 3, (2 * L / nx,) * 3, (nx, nx, nx))
+        wall = (time.perf_counter() - t0) * 1e3
+        ms = ctx.call_timing()
+        assert 0.0 < ms <= wall
+        assert b["count"].sum() == len(mass)
+        t0 = time.perf_counter()
+        order = ctx.sort_by_cell()
+        wall = (time.perf_counter() - t0) * 1e3
+        ms2 = ctx.call_timing()
+        assert 0.0 < ms2 <= wall
+        assert np.array_equal(np.sort(order), np.arange(len(mass)))
+    finally:
+        ctx.enable_timing(False)
