@@ -429,6 +429,15 @@ khrr_status khrr_fp32_probe(khrr_ctx* ctx, double* tflops);
  * flag.  The context stays usable.  No fault, trap or unbounded loop is
  * involved. */
 khrr_status khrr_probe_bounded_wait(khrr_ctx* ctx, double seconds);
+/* The same check for the cooperative 128^3 stencil, whose CTAs wait on one
+ * another's counters: four iterations on a zero field in scratch buffers of
+ * its own, with brick 0 never publishing its counter and every wait limited
+ * to `seconds` (0 < s <= 10).  Its neighbours give up and raise the device
+ * error flag and the kernel's abort word, every other CTA's wait ends on
+ * that word, and the launch completes; the call reports KHRR_ERR_TIMEOUT and
+ * clears the flag, and the context stays usable.  KHRR_ERR_UNSUPPORTED where
+ * the resident stencil cannot run (it needs 128 co-resident 221 KB CTAs). */
+khrr_status khrr_probe_resident_wave(khrr_ctx* ctx, double seconds);
 
 #ifdef __cplusplus
 }

@@ -309,19 +309,24 @@ struct WaveMaps {
     CUtensorMap tile[4], tile_mass;  // 32 x 8 boxes: phi^{n-1} and mass (one-step kernel)
     bool ok = false;
     bool two_step = false;           // pairs of iterations through the two-step kernel
-    // The shared-memory-resident kernel (nx = 128): its nx + 1 plane counters.
+    // The shared-memory-resident kernel (nx = 128): nx + 1 words for its 128
+    // brick counters and abort word.
     bool resident = false;
     unsigned* sync = nullptr;
 };
 // Whether the shared-memory-resident FP32 stencil runs for this mesh edge on
-// the current device (nx = 128, one 197 KB CTA per plane, all co-resident).
+// the current device (nx = 128, one 221 KB CTA per 128 x 16 x 8 brick, all
+// co-resident).
 bool wave_resident_available(int nx);
 // k FP32 iterations of the ring in one cooperative launch with the field
 // resident in shared memory, bit-identical to k launch_wave_f32 iterations and
 // leaving the ring in the state enqueue_wave_f32 leaves it; sync: nx + 1
-// counters (zeroed here); bounded waits report into err.
+// counters (zeroed here); bounded waits (limit_ns each) report into err.
+// withhold: a brick that never publishes its counter (the failure probe;
+// -1 otherwise).
 cudaError_t launch_wave_resident(float* ring, int64_t cells, const float* mass, const WaveF32& w, int k, int st,
-                                 double* resid, unsigned* sync, unsigned* err, cudaStream_t s);
+                                 double* resid, unsigned* sync, unsigned* err, cudaStream_t s,
+                                 unsigned long long limit_ns = 2000000000ull, int withhold = -1);
 // One FP32 iteration fed by tensor copies (wave1_tma_kernel), bit-identical
 // to launch_wave_f32.
 cudaError_t launch_wave1_tma(float* phi_new, const CUtensorMap& phi, const CUtensorMap& phi_old,

@@ -1041,7 +1041,8 @@ __global__ void __launch_bounds__(kRzThreads, 1) wave_resident_kernel(float* __r
                                                                       const WaveF32 W, int k, int st,
                                                                       double* __restrict__ resid,
                                                                       unsigned* __restrict__ flag,
-                                                                      unsigned* __restrict__ err) {
+                                                                      unsigned* __restrict__ err,
+                                                                      unsigned long long limit_ns, int withhold) {
     extern __shared__ __align__(16) float rz_smem[];
     float* sphi = rz_smem;                  // [2][brick]: phi^n by iteration parity
     float* sw = rz_smem + 2 * kRzBrick;     // [brick]: w = 1 / (1 + Q)
@@ -1185,7 +1186,7 @@ __global__ void __launch_bounds__(kRzThreads, 1) wave_resident_kernel(float* __r
                                 abort = 1;
                                 break;
                             }
-                            if (global_ns() - t0 > 2000000000ull) {
+                            if (global_ns() - t0 > limit_ns) {
                                 atomicOr(err, kErrTimeout);
                                 st_release_gpu(flag + kRzBricks, 1u);
                                 abort = 1;
@@ -1229,7 +1230,9 @@ __global__ void __launch_bounds__(kRzThreads, 1) wave_resident_kernel(float* __r
             if (!rz_interior_slot(wid, i)) row(i);
         __syncthreads();  // the brick is written (shared and global); rd and the halo are free
         // The barrier orders the CTA's stores before thread 0's release.
-        if (tid == 0) st_release_gpu(flag + b, static_cast<unsigned>(t + 1));
+        // (withhold: the failure probe's brick that never publishes, so its
+        // neighbours' waits run out; -1 in every solve)
+        if (tid == 0 && b != withhold) st_release_gpu(flag + b, static_cast<unsigned>(t + 1));
         old = cur;
         cur = ob;
     }
@@ -1574,7 +1577,8 @@ bool wave_resident_available(int nx) {
 }
 
 cudaError_t launch_wave_resident(float* ring, int64_t cells, const float* mass, const WaveF32& w, int k, int st,
-                                 double* resid, unsigned* sync, unsigned* err, cudaStream_t s) {
+                                 double* resid, unsigned* sync, unsigned* err, cudaStream_t s,
+                                 unsigned long long limit_ns, int withhold) {
     if (k < 1) return cudaSuccess;
     cudaError_t e = cudaMemsetAsync(sync, 0, (kRzBricks + 1) * sizeof(unsigned), s);
     if (e != cudaSuccess) return e;
@@ -1588,7 +1592,8 @@ cudaError_t launch_wave_resident(float* ring, int64_t cells, const float* mass, 
     attr[0].val.cooperative = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    return cudaLaunchKernelEx(&cfg, wave_resident_kernel, ring, cells, mass, w, k, st, resid, sync, err);
+    return cudaLaunchKernelEx(&cfg, wave_resident_kernel, ring, cells, mass, w, k, st, resid, sync, err, limit_ns,
+                              withhold);
 }
 
 cudaError_t enqueue_wave_f32(float* ring, int64_t cells, const float* mass, const WaveF32& w, int k, int st,

@@ -446,6 +446,40 @@ khrr_status check_cubic(khrr_ctx* c, const khrr_mesh* m, MeshGeom* g, int64_t* n
 
 }  // namespace
 
+khrr_status khrr_probe_resident_wave(khrr_ctx* c, double seconds) {
+    khrr::NvtxRange nvtx_range("khrr_probe_resident_wave");
+    if (!c) return KHRR_ERR_INVALID_ARG;
+    if (!(seconds > 0.0) || seconds > 10.0) return c->fail(KHRR_ERR_INVALID_ARG, "seconds must be in (0, 10]");
+    constexpr int nx = 128;
+    if (!wave_resident_available(nx))
+        return c->fail(KHRR_ERR_UNSUPPORTED, "the resident 128^3 stencil does not run on this device");
+    khrr_status st = c->check_device_flag();  // report (and clear) anything raised earlier first
+    if (st != KHRR_OK) return st;
+    // A zero field on scratch buffers of the probe's own (the context's
+    // solver state is not touched), four iterations, brick 0 withholding
+    // its counter.
+    const size_t cz = static_cast<size_t>(nx) * nx * nx;
+    DevBuf<float> ring, mass, tab;
+    DevBuf<unsigned> sync;
+    if ((st = c->cuda(ring.ensure(4 * cz), "alloc")) != KHRR_OK || (st = c->cuda(mass.ensure(cz), "alloc")) != KHRR_OK ||
+        (st = c->cuda(tab.ensure(3 * nx), "alloc")) != KHRR_OK || (st = c->cuda(sync.ensure(nx + 1), "alloc")) != KHRR_OK)
+        return st;
+    cudaStream_t s = c->stream;
+    cudaMemsetAsync(ring.p, 0, 4 * cz * sizeof(float), s);
+    cudaMemsetAsync(mass.p, 0, cz * sizeof(float), s);
+    cudaMemsetAsync(tab.p, 0, 3 * nx * sizeof(float), s);
+    WaveF32 w{};
+    w.nx = nx;
+    w.sx = tab.p;
+    w.sy = tab.p + nx;
+    w.sz = tab.p + 2 * nx;
+    if ((st = c->cuda(launch_wave_resident(ring.p, static_cast<int64_t>(cz), mass.p, w, 4, 1, nullptr, sync.p,
+                                           c->errflag.p, s, static_cast<unsigned long long>(seconds * 1e9), 0),
+                      "resident wave probe")) != KHRR_OK)
+        return st;
+    return c->check_device_flag();  // synchronises before the scratch is freed
+}
+
 khrr_status khrr_cic_deposit(khrr_ctx* c, const double* pos, const double* mass, int64_t n, const khrr_mesh* mesh,
                              double* cell_mass) {
     khrr::NvtxRange nvtx_range("khrr_cic_deposit");

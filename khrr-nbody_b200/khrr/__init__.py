@@ -146,6 +146,7 @@ def lib(path: pathlib.Path | str | None = None) -> C.CDLL:
         "khrr_bin_cell_phi": ([vp, i, vp], i),
         "khrr_accel_noalloc": ([vp, vp, vp, vp, vp, i64, i, vp], i),
         "khrr_probe_bounded_wait": ([vp, d], i),
+        "khrr_probe_resident_wave": ([vp, d], i),
         "khrr_cic_deposit": ([vp, vp, vp, i64, C.POINTER(Mesh), vp], i),
         "khrr_cic_gather": ([vp, vp, i64, C.POINTER(Mesh), vp, vp, vp, vp], i),
         "khrr_sort_by_cell": ([vp, vp], i),
@@ -419,6 +420,11 @@ class Context:
         """Status of the library's bounded-wait failure path (KHRR_ERR_TIMEOUT
         = 5 when it works); raises nothing."""
         return int(self.L.khrr_probe_bounded_wait(self.h, float(seconds)))
+
+    def probe_resident_wave(self, seconds=0.2) -> int:
+        """khrr_probe_resident_wave: the cooperative 128^3 stencil with one brick
+        withholding its counter; returns the status (KHRR_ERR_TIMEOUT expected)."""
+        return int(self.L.khrr_probe_resident_wave(self.h, float(seconds)))
 
     def mesh_solver_phi(self, nx):
         out = np.empty(nx ** 3)

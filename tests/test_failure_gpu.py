@@ -63,3 +63,36 @@ def test_probe_rejects_bad_limits(ctx):
     import khrr
     assert khrr.STATUS[ctx.probe_bounded_wait(0.0)] == "KHRR_ERR_INVALID_ARG"
     assert khrr.STATUS[ctx.probe_bounded_wait(60.0)] == "KHRR_ERR_INVALID_ARG"
+
+
+def test_resident_stencil_wait_times_out_and_context_recovers(ctx):
+    """The cooperative 128^3 stencil's CTAs wait on one another's counters:
+    with one brick withholding its counter, its neighbours' bounded waits give
+    up, the abort word ends every other wait, the call reports
+    KHRR_ERR_TIMEOUT, and the next resident wave solve on the same context
+    equals one on a fresh context bit for bit."""
+    import khrr
+    t0 = time.perf_counter()
+    st = ctx.probe_resident_wave(0.25)
+    dt = time.perf_counter() - t0
+    if khrr.STATUS[st] == "KHRR_ERR_UNSUPPORTED":
+        pytest.skip("the resident stencil does not run on this device")
+    assert khrr.STATUS[st] == "KHRR_ERR_TIMEOUT"
+    assert 0.25 <= dt < 5.0
+    assert khrr.STATUS[ctx.probe_resident_wave(0.0)] == "KHRR_ERR_INVALID_ARG"
+    pos, vel, mass, eps2 = galaxy()
+    nx, L = 128, 4.0
+    W = khrr.WaveParams.make(nx, 2 * L / nx)
+    out = []
+    for c in (ctx, khrr.Context(0)):
+        try:
+            c.upload(pos, vel, mass, eps2)
+            c.bin((-L,) * 3, (2 * L / nx,) * 3, (nx, nx, nx))
+            out.append(c.wave_solve(W, tol=0.0, max_iter=60, check_every=30, cold=True))
+        finally:
+            if c is not ctx:
+                c.close()
+    (i1, r1, p1), (i2, r2, p2) = out
+    assert i1 == i2 == 60
+    assert np.array_equal(p1, p2)
+    assert r1 == r2 or abs(r1 - r2) <= 1e-12 * r2
