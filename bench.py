@@ -847,29 +847,40 @@ def run_khrr(args):
     # single-GPU run only: under torchrun the other ranks would wait for them
     # at the closing barrier, past the process group's timeout.
     single = rank == 0 and world == 1
+    leg_s = {}  # wall seconds of each leg outside the timed region
+
+    def leg(name, fn):
+        t0 = time.perf_counter()
+        out = fn()
+        leg_s[name] = round(time.perf_counter() - t0, 1)
+        return out
     # the precision contract at this size: FP32 (tuned kernel) vs FP64 runs
     drift64 = None
     if single and args.drift_steps > 0:
-        drift64 = drift_vs_fp64_leg(khrr, ctx, torch, pos, vel, mass, eps2, args.drift_steps,
-                                    fp64_steps=min(args.drift_fp64_steps, args.drift_steps))
+        drift64 = leg("drift_vs_fp64", lambda: drift_vs_fp64_leg(
+            khrr, ctx, torch, pos, vel, mass, eps2, args.drift_steps,
+            fp64_steps=min(args.drift_fp64_steps, args.drift_steps)))
     ens = None
     if not args.no_ensemble and single:
-        ens = ensemble_leg(khrr, local, torch)
+        ens = leg("ensemble", lambda: ensemble_leg(khrr, local, torch))
     mesh = None
     if not args.no_mesh and single:
-        mesh = mesh_leg(khrr, local, torch, float(peaks.get("hbm_gbs", 6650.0)), args.mesh_max_iter)
+        mesh = leg("mesh", lambda: mesh_leg(khrr, local, torch, float(peaks.get("hbm_gbs", 6650.0)),
+                                            args.mesh_max_iter))
     ctx.close()
     configs = None
     if not args.no_configs and single:
-        configs = {"config0": config0_leg(khrr, local, torch, run_cpu=not args.no_cpu_baseline),
+        configs = {"config0": leg("config0", lambda: config0_leg(khrr, local, torch,
+                                                                 run_cpu=not args.no_cpu_baseline)),
                    "config1": "this line: value, roofline, acc_rel_rms_vs_fp64, drift_vs_fp64",
-                   "config2": config2_leg(khrr, local, torch),
+                   "config2": leg("config2", lambda: config2_leg(khrr, local, torch)),
                    "config3": "ensemble",
-                   "config4": config4_leg(khrr, local, torch)}
+                   "config4": leg("config4", lambda: config4_leg(khrr, local, torch))}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        rate, cores, kind, sample, _ = cpu_reference_sample(pos, vel, mass, eps2, 15.0, np.random.default_rng(5))
+        rate, cores, kind, sample, _ = leg("cpu_baseline", lambda: cpu_reference_sample(
+            pos, vel, mass, eps2, 15.0, np.random.default_rng(5)))
         cpu = {"value": rate / 1e9, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample}
 
     if dist:
@@ -920,6 +931,7 @@ def run_khrr(args):
         "ensemble": ens,
         "mesh": mesh,
         "configs": configs,
+        "leg_seconds": leg_s,
     }
     print(json.dumps(line), flush=True)
     return 0
