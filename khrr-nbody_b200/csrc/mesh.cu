@@ -28,6 +28,7 @@
 
 #include "async_copy.cuh"
 #include "khrr_internal.h"
+#include "wave_bricks.h"
 
 namespace khrr {
 namespace {
@@ -970,21 +971,8 @@ __global__ void __launch_bounds__((kW1Consumers + 1) * 32) wave1_tma_kernel(floa
 // serialised behind its z carry); halos staged in shared memory 7.2 us;
 // interior rows before the wait 6.7 us; the residual moved out of the loop
 // (no FP64 branch in it) 5.6 us.
-constexpr int kRzNX = 128;                                 // mesh edge
-constexpr int kRzBY = 16, kRzBZ = 8;                       // brick rows in y and z
-constexpr int kRzBricksY = kRzNX / kRzBY;                  // 8
-constexpr int kRzBricks = kRzBricksY * (kRzNX / kRzBZ);    // 128
-constexpr int kRzThreads = 32 * kRzBY;                     // a warp per brick row yl
-constexpr int kRzSlots = kRzBY * kRzBZ / (kRzThreads / 32);  // rows per warp (8)
-constexpr int kRzCells = 4 * kRzSlots;                     // cells per thread
-constexpr int kRzPlane = kRzNX * kRzNX;
-constexpr int kRzBrick = kRzNX * kRzBY * kRzBZ;            // 16,384 cells
-constexpr int kRzHalo = (2 * kRzBZ + 2 * kRzBY) * kRzNX;  // the neighbour rows read, 6,144 cells
-constexpr int kRzHaloVec = kRzHalo / 4;
+// Brick geometry, row map and halo rows: wave_bricks.h.
 constexpr size_t kRzSmem = (3 * static_cast<size_t>(kRzBrick) + kRzHalo) * sizeof(float);  // 221,184 B
-static_assert(kRzHaloVec % kRzThreads == 0, "whole halo loads per thread");
-static_assert(kRzNX == 4 * 32 && kRzNX % kRzBY == 0 && kRzNX % kRzBZ == 0, "a warp covers a row, four cells per lane");
-static_assert(kRzBricks <= kRzNX, "the counters (nx + 1 words, allocated by the mesh set-up) cover the bricks and the abort flag");
 
 __device__ __forceinline__ unsigned ld_acquire_gpu(const unsigned* p) {
     unsigned v;
@@ -1004,36 +992,6 @@ __device__ __forceinline__ void ring_free_dev(int o, int c, int& f0, int& f1) {
         if (b != o && b != c && n < 2) f[n++] = b;
     f0 = f[0];
     f1 = f[1];
-}
-
-// The brick's rows: 84 interior rows (1 <= yl <= 14, 1 <= zl <= 6), which no
-// neighbour reads and whose neighbours all lie in the brick, and 44 face rows
-// (yl in {0, 15} or zl in {0, 7}).  Warp w owns 8 rows for the whole launch:
-// slots 0-4 are interior rows w + 16 m; slot 5 is interior row 80 + (w - 12)
-// for w >= 12 and face row w for w < 12; slots 6, 7 are face rows
-// w + 16 (m + [w < 12]).  Face row f: zl = 0 for f < 16, zl = 7 for f >= 28,
-// otherwise zl = 1 + (f - 16) / 2 at yl = 0 or 15.
-static_assert(kRzBY == 16 && kRzBZ == 8 && kRzSlots == 8, "the row map below is written for 16 x 8 rows, 16 warps");
-__device__ __forceinline__ bool rz_interior_slot(int w, int i) { return i < 5 || (i == 5 && w >= 12); }
-
-__device__ __forceinline__ void rz_row(int w, int i, int& yl, int& zl) {
-    if (rz_interior_slot(w, i)) {
-        const int ii = i < 5 ? w + 16 * i : 80 + (w - 12);
-        zl = 1 + ii / 14;
-        yl = 1 + ii % 14;
-    } else {
-        const int f = w + 16 * (i - (w < 12 ? 5 : 6));
-        if (f < 16) {
-            zl = 0;
-            yl = f;
-        } else if (f >= 28) {
-            zl = kRzBZ - 1;
-            yl = f - 28;
-        } else {
-            zl = 1 + (f - 16) / 2;
-            yl = (f - 16) & 1 ? kRzBY - 1 : 0;
-        }
-    }
 }
 
 __global__ void __launch_bounds__(kRzThreads, 1) wave_resident_kernel(float* __restrict__ ring, int64_t cz,
@@ -1116,10 +1074,10 @@ __global__ void __launch_bounds__(kRzThreads, 1) wave_resident_kernel(float* __r
             rz_row(wid, i, yl, zl);
             const int y = y0 + yl, z = z0 + zl;
             const int s = sidx(yl, zl);
-            const float* pzm = zl > 0 ? rd + s - kSRow : shalo + (2 * kRzBZ + yl) * kRzNX + x0;
-            const float* pzp = zl < kRzBZ - 1 ? rd + s + kSRow : shalo + (2 * kRzBZ + kRzBY + yl) * kRzNX + x0;
-            const float* pym = yl > 0 ? rd + s - kRzNX : shalo + zl * kRzNX + x0;
-            const float* pyp = yl < kRzBY - 1 ? rd + s + kRzNX : shalo + (kRzBZ + zl) * kRzNX + x0;
+            const float* pzm = zl > 0 ? rd + s - kSRow : shalo + rz_halo_zm(yl) * kRzNX + x0;
+            const float* pzp = zl < kRzBZ - 1 ? rd + s + kSRow : shalo + rz_halo_zp(yl) * kRzNX + x0;
+            const float* pym = yl > 0 ? rd + s - kRzNX : shalo + rz_halo_ym(zl) * kRzNX + x0;
+            const float* pyp = yl < kRzBY - 1 ? rd + s + kRzNX : shalo + rz_halo_yp(zl) * kRzNX + x0;
             const float4 c4 = *reinterpret_cast<const float4*>(rd + s);
             const float4 zm4 = *reinterpret_cast<const float4*>(pzm);
             const float4 zp4 = *reinterpret_cast<const float4*>(pzp);
@@ -1168,9 +1126,8 @@ __global__ void __launch_bounds__(kRzThreads, 1) wave_resident_kernel(float* __r
                 // All counters in flight together; the abort flag and the
                 // clock only every 64th poll.  A missing neighbour (a mesh
                 // face) is stood in for by the brick's own counter (>= t).
-                const unsigned* fn[4] = {flag + (by > 0 ? b - 1 : b), flag + (by < kRzBricksY - 1 ? b + 1 : b),
-                                         flag + (bz > 0 ? b - kRzBricksY : b),
-                                         flag + (z0 + kRzBZ < kRzNX ? b + kRzBricksY : b)};
+                const unsigned* fn[4] = {flag + rz_neighbour(b, 0), flag + rz_neighbour(b, 1),
+                                         flag + rz_neighbour(b, 2), flag + rz_neighbour(b, 3)};
                 const unsigned need = static_cast<unsigned>(t);
                 auto ready = [&]() {
                     const unsigned a0 = ld_acquire_gpu(fn[0]), a1 = ld_acquire_gpu(fn[1]);
@@ -1210,14 +1167,7 @@ __global__ void __launch_bounds__(kRzThreads, 1) wave_resident_kernel(float* __r
         for (int r = 0; r < kRzHaloVec / kRzThreads; ++r) {
             const int q = tid + r * kRzThreads, hr = q >> 5, hx = 4 * (q & 31);
             int gy, gz;
-            if (hr < 2 * kRzBZ) {  // y halos: rows (y0 - 1 | y0 + BY, z0 + zl)
-                gy = hr < kRzBZ ? y0 - 1 : y0 + kRzBY;
-                gz = z0 + (hr % kRzBZ);
-            } else {  // z halos: rows (y0 + yl, z0 - 1 | z0 + BZ)
-                const int h = hr - 2 * kRzBZ;
-                gy = y0 + (h % kRzBY);
-                gz = h < kRzBY ? z0 - 1 : z0 + kRzBZ;
-            }
+            rz_halo_source(hr, by, bz, gy, gz);
             float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
             if (gy >= 0 && gy < kRzNX && gz >= 0 && gz < kRzNX)
                 v = __ldcg(reinterpret_cast<const float4*>(gcur + static_cast<int64_t>(gz) * kRzPlane +
