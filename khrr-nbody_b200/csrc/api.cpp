@@ -15,6 +15,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdarg>
+#include <cstdlib>
 #include <cstdio>
 #include <cstring>
 #include <map>
@@ -319,22 +320,39 @@ khrr_status khrr_ctx::ensure_plan(int mode) {
     const bool plain = mode == kModePlain;
     khrr_status st;
     if (mode == kModeF64) {
-        // The FP64 kernel's queue: 512-body i tiles, 128-body j tiles, the
-        // j split that fills the last wave of its resident CTAs.
-        const int ctas = fp64_force_ctas(sm_count);
-        if (p.valid && p.ctas == ctas) return KHRR_OK;
-        plan_force_items(poff, cnt, kF64ITile, kPad, ctas, 0, false, p);
+        // The symmetric FP64 kernel on the pair plan over 1024-body blocks
+        // (one partial slot per body, FP64 atomics), or with
+        // KHRR_FP64_ONESIDED=1 the one-sided kernel's queue: 512-body i
+        // tiles, 128-body j tiles, the j split that fills the last wave of
+        // its resident CTAs.
+        const char* e = std::getenv("KHRR_FP64_ONESIDED");
+        const bool sym = !(e && std::atoi(e) == 1);
+        const int ctas = sym ? fp64_pair_ctas(sm_count) : fp64_force_ctas(sm_count);
+        if (p.valid && p.ctas == ctas && p.f64_pair == sym) return KHRR_OK;
+        if (sym) {
+            plan_pair_items(pair_blocks_fixed(poff), cnt, ctas, 0, p);
+            p.nslots = 1;
+            p.sys_split.assign(cnt.size(), 1);
+            if ((st = cuda(p.d_pair_items.ensure(p.pair_items.size()), "alloc items")) != KHRR_OK) return st;
+            if ((st = cuda(cudaMemcpyAsync(p.d_pair_items.p, p.pair_items.data(),
+                                           p.pair_items.size() * sizeof(PairItem), cudaMemcpyHostToDevice, stream),
+                           "upload items")) != KHRR_OK)
+                return st;
+        } else {
+            plan_force_items(poff, cnt, kF64ITile, kPad, ctas, 0, false, p);
+            if ((st = cuda(p.d_items.ensure(p.items.size()), "alloc items")) != KHRR_OK) return st;
+            if ((st = cuda(cudaMemcpyAsync(p.d_items.p, p.items.data(), p.items.size() * sizeof(WorkItem),
+                                           cudaMemcpyHostToDevice, stream),
+                           "upload items")) != KHRR_OK)
+                return st;
+        }
         p.pair = false;
-        p.threads = 128;
-        p.ipt = kF64ITile / 128;
+        p.f64_pair = sym;
+        p.threads = sym ? kPairBlock / 4 : 128;
+        p.ipt = sym ? 4 : kF64ITile / 128;
         p.jt = kPad;
         p.split_req = 0;
         p.ctas = ctas;
-        if ((st = cuda(p.d_items.ensure(p.items.size()), "alloc items")) != KHRR_OK) return st;
-        if ((st = cuda(cudaMemcpyAsync(p.d_items.p, p.items.data(), p.items.size() * sizeof(WorkItem),
-                                       cudaMemcpyHostToDevice, stream),
-                       "upload items")) != KHRR_OK)
-            return st;
         std::vector<unsigned char> ns(static_cast<size_t>(npad), 0);
         for (size_t k = 0; k < cnt.size(); ++k)
             std::fill(ns.begin() + poff[k], ns.begin() + poff[k] + cnt[k], static_cast<unsigned char>(p.sys_split[k]));
@@ -450,7 +468,22 @@ khrr_status khrr_ctx::enqueue_force(int mode, bool acc, bool phi, bool events, c
     // khrr_step points them at fresh timing events before each replay.
     if (events && (st = cuda(cudaEventRecordWithFlags(ph0, stream, cudaEventRecordExternal), "event")) != KHRR_OK)
         return st;
-    if (mode == kModeF64) {
+    if (mode == kModeF64 && p.f64_pair) {
+        if ((st = cuda(cudaMemsetAsync(queue.p, 0, sizeof(unsigned), stream), "queue reset")) != KHRR_OK) return st;
+        if ((st = cuda(cudaMemsetAsync(part.p, 0, sizeof(double4) * npad, stream), "sums reset")) != KHRR_OK)
+            return st;
+        F64PairArgs a{};
+        a.pos = x;
+        a.mass = mass.p;
+        a.eps2 = eps2.p;
+        a.items = p.d_pair_items.p;
+        a.n_items = static_cast<int>(p.pair_items.size());
+        a.queue = queue.p;
+        a.sums = part.p;
+        if ((st = cuda(launch_fp64_pair(a, acc, phi, std::min(a.n_items, ctas), stream), "FP64 pair kernel")) !=
+            KHRR_OK)
+            return st;
+    } else if (mode == kModeF64) {
         if ((st = cuda(cudaMemsetAsync(queue.p, 0, sizeof(unsigned), stream), "queue reset")) != KHRR_OK) return st;
         F64Args a{};
         a.pos = x;

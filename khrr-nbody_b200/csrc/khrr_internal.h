@@ -187,6 +187,19 @@ struct F64Args {
 };
 cudaError_t launch_fp64_force(const F64Args& a, bool acc, bool phi, int grid, cudaStream_t s);
 int fp64_force_ctas(int sm_count);  // resident CTAs of the FP64 kernel on the device
+// The symmetric FP64 pass on the pair kernel's plan: sums (ax, ay, az,
+// sum m/r per body, zeroed before the launch) accumulated with FP64 atomics.
+struct F64PairArgs {
+    const double* pos;      // AoS double3 [npad]
+    const double* mass;     // [npad]
+    const double* eps2;     // [npad]
+    const PairItem* items;  // plan_pair_items over 1024-body blocks
+    int n_items;
+    unsigned* queue;        // next-item counter (zeroed before each launch)
+    double4* sums;          // [npad]
+};
+cudaError_t launch_fp64_pair(const F64PairArgs& a, bool acc, bool phi, int grid, cudaStream_t s);
+int fp64_pair_ctas(int sm_count);
 
 // ---- integrate.cu -----------------------------------------------------------
 struct StepArgs {

@@ -63,8 +63,9 @@ struct ForcePlan {
     int nslots = 1;
     DevBuf<WorkItem> d_items;
     DevBuf<unsigned char> d_nsplit;
-    // The symmetric pair kernel's queue (pair plans only).
+    // The symmetric pair kernel's queue (pair plans; FP64 plans with f64_pair).
     bool pair = false;
+    bool f64_pair = false;  // FP64 plan: the symmetric FP64 kernel on pair_items
     std::vector<PairItem> pair_items;
     DevBuf<PairItem> d_pair_items;
     ForcePlan() = default;
