@@ -64,9 +64,12 @@ enum {
                                    Wave mode, instead of the direct sum          */
     KHRR_FP64 = 64              /* khrr_forces / khrr_step: the direct sum in FP64,
                                    the reference's precision (ACCEL_kernel and
-                                   PHI_kernel with real = double), at about a
-                                   quarter of the FP32 pair kernel's rate: the
-                                   comparator for accuracy and energy drift      */
+                                   PHI_kernel with real = double; each unordered
+                                   pair evaluated once, or with the environment
+                                   variable KHRR_FP64_ONESIDED=1 every ordered
+                                   pair), at about 30 % of the FP32 pair
+                                   kernel's rate: the comparator for accuracy
+                                   and energy drift                              */
 };
 
 /* Analytic halo + bulge parameters (__gr_par.ini lines 1-6); the derived
