@@ -142,14 +142,24 @@ __global__ void __launch_bounds__(NT, kMinCtas) fp64_force_kernel(const F64Args 
 // the two sides (6 fma; +2 fma for the potential).  The sums are FP64
 // throughout; their order differs from the reference's j loop (and between
 // runs, through the atomics) only at the level of FP64 rounding.
-constexpr int PNT = 256;                  // threads per CTA
+#ifndef KHRR_F64P_NT
+#define KHRR_F64P_NT 256
+#endif
+#ifndef KHRR_F64P_UNROLL
+#define KHRR_F64P_UNROLL 2
+#endif
+#ifndef KHRR_F64P_CTAS
+#define KHRR_F64P_CTAS 2
+#endif
+constexpr int PNT = KHRR_F64P_NT;         // threads per CTA
+constexpr int kF64PUnroll = KHRR_F64P_UNROLL;
 constexpr int PK = kPairBlock / PNT;      // i bodies per thread (4)
 constexpr int PJT = kPairTile;            // j bodies per tile (128)
 constexpr int PW = PNT / 32;              // warps (8)
 static_assert(PNT * PK == kPairBlock && PJT == 128 && PJT % 32 == 0 && PNT >= PJT, "pair shapes");
 
 template <bool ACC, bool PHI>
-__global__ void __launch_bounds__(PNT, 2) fp64_pair_kernel(const F64PairArgs a) {
+__global__ void __launch_bounds__(PNT, KHRR_F64P_CTAS) fp64_pair_kernel(const F64PairArgs a) {
     constexpr int NC = (ACC ? 3 : 0) + (PHI ? 1 : 0), CP = NC - 1;
     __shared__ double tx[2][PJT], ty[2][PJT], tz[2][PJT], tm[2][PJT], th[2][PJT];
     __shared__ double jw[PW][NC][PJT];
@@ -209,7 +219,7 @@ __global__ void __launch_bounds__(PNT, 2) fp64_pair_kernel(const F64PairArgs a) 
                 double r[NC];
 #pragma unroll
                 for (int c = 0; c < NC; ++c) r[c] = 0.0;
-#pragma unroll 2
+#pragma unroll kF64PUnroll
                 for (int s = 0; s < 32; ++s) {
                     const int j = c0 + ((lane + s) & 31);
                     const double xj = tx[b][j], yj = ty[b][j], zj = tz[b][j], mj = tm[b][j], hj = th[b][j];
